@@ -1,0 +1,241 @@
+"""Python binding of the B200 coupled-cluster engine (C-ABI in include/aces_b200.h).
+
+The engine is the shared library ``libacesb200.so`` built next to this file
+(``python aces-ii_b200/build.py``).  Loading fails loudly when it is absent:
+there is no CPU fallback.
+
+Typical use mirrors the reference's program flow (intprc writes the MO
+integral lists, xvcc reads them, vcc/vcc.F):
+
+    import acesb200 as ab
+    lib = ab.load()
+    lib.init(0)
+    lib.sym_init(pop, vrt)
+    ab.put_hamiltonian(lib, eps, blocks, irr_o, irr_v)   # lists 13, 10, 16, 25, 30, 233
+    res = lib.xvcc(cc_conv=7, cc_exporder=5)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .dpd import DPD, put_dense_list, get_dense_list  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libacesb200.so")
+
+ACES_OK = 0
+PREC_FP64 = 0
+PREC_BF16X3 = 1
+
+# exported C-ABI symbols (include/aces_b200.h)
+SYMBOLS = [
+    "aces_init", "aces_fin", "aces_last_error", "aces_sym_init", "aces_irpdpd",
+    "aces_isymoff", "aces_dirprd", "aces_list_touch", "aces_updmoi", "aces_inipck",
+    "aces_isytyp", "aces_list_dims", "aces_getlst", "aces_putlst", "aces_getlst_dev",
+    "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
+    "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "xvcc_run", "xlambda_run",
+    "xdens_1pdm",
+]
+
+
+class CCConfig(C.Structure):
+    """aces_cc_config (include/aces_b200.h)."""
+    _fields_ = [
+        ("cc_conv", C.c_int), ("cc_maxcyc", C.c_int), ("cc_exporder", C.c_int),
+        ("precision", C.c_int), ("triples", C.c_int), ("use_graph", C.c_int),
+        ("verbose", C.c_int), ("reserved", C.c_int),
+        ("e_ccsd", C.c_double), ("e_t4", C.c_double), ("e_st5", C.c_double),
+        ("last_residual", C.c_double), ("ncycle", C.c_int), ("converged", C.c_int),
+        ("seconds_per_iter", C.c_double), ("seconds_triples", C.c_double),
+    ]
+
+
+class AcesError(RuntimeError):
+    def __init__(self, fn, status, msg):
+        super().__init__(f"{fn} returned {status}: {msg}")
+        self.status = status
+
+
+_DP = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class Lib:
+    """Thin checked wrapper over the shared library."""
+
+    def __init__(self, path=LIBPATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} is missing: build it with `python aces-ii_b200/build.py` "
+                "(the engine has no CPU fallback)")
+        self.path = path
+        self.h = C.CDLL(path)
+        h = self.h
+        h.aces_last_error.restype = C.c_char_p
+        h.aces_list_devptr.restype = C.c_void_p
+        h.aces_list_devptr.argtypes = [C.c_int, C.c_int]
+        h.aces_reclen.restype = C.c_longlong
+        h.aces_reclen.argtypes = [C.c_char_p]
+        h.aces_getlst.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        h.aces_putlst.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        h.aces_getall.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int]
+        h.aces_putall.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int]
+        h.aces_putrec.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p]
+        h.aces_getrec.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p]
+        h.aces_sym_init.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        h.aces_xgemm.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
+                                 C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double,
+                                 C.c_void_p, C.c_int, C.c_int]
+        for fn in ("xvcc_run", "xlambda_run", "xdens_1pdm"):
+            getattr(h, fn).argtypes = [C.POINTER(CCConfig)]
+
+    def _chk(self, fn, status):
+        if status != ACES_OK:
+            raise AcesError(fn, status, self.h.aces_last_error().decode())
+        return status
+
+    def error(self):
+        return self.h.aces_last_error().decode()
+
+    # ---- runtime / symmetry -------------------------------------------------
+    def init(self, device=0):
+        self._chk("aces_init", self.h.aces_init(device))
+
+    def fin(self):
+        self._chk("aces_fin", self.h.aces_fin())
+
+    def sym_init(self, pop, vrt):
+        n = len(pop)
+        p = (C.c_int * n)(*[int(x) for x in pop])
+        v = (C.c_int * n)(*[int(x) for x in vrt])
+        self._chk("aces_sym_init", self.h.aces_sym_init(n, p, v))
+        self.nirrep = n
+        self.pop = [int(x) for x in pop]
+        self.vrt = [int(x) for x in vrt]
+
+    def irpdpd(self, irrep, typ):
+        r = self.h.aces_irpdpd(irrep, typ)
+        if r < 0:
+            raise AcesError("aces_irpdpd", r, self.error())
+        return r
+
+    def isymoff(self, irrep_q, irrep_pq, typ):
+        r = self.h.aces_isymoff(irrep_q, irrep_pq, typ)
+        if r < 0:
+            raise AcesError("aces_isymoff", r, self.error())
+        return r
+
+    # ---- lists ------------------------------------------------------------------
+    def inipck(self, irrepx, typl, typr, lst, iset=1):
+        self._chk("aces_inipck", self.h.aces_inipck(irrepx, typl, typr, lst, iset))
+
+    def list_touch(self, ncols, nrows, irrep, lst):
+        return self.h.aces_list_touch(ncols, nrows, irrep, lst, 0)
+
+    def list_dims(self, irrep, lst):
+        nc, nr = C.c_int(), C.c_int()
+        self._chk("aces_list_dims", self.h.aces_list_dims(irrep, lst, C.byref(nc), C.byref(nr)))
+        return nr.value, nc.value
+
+    def getlst(self, first, ncols, irrep, lst):
+        nr, _ = self.list_dims(irrep, lst)
+        out = np.zeros((ncols, nr))  # column-major: each row of `out` is one column
+        self._chk("aces_getlst", self.h.aces_getlst(out.ctypes.data, first, ncols, irrep, lst))
+        return out.T
+
+    def putlst(self, cols, first, irrep, lst):
+        """cols: (nrows, ncols) array; stored column-major."""
+        a = np.ascontiguousarray(np.asarray(cols, dtype=np.float64).T)
+        ncols = a.shape[0]
+        self._chk("aces_putlst", self.h.aces_putlst(a.ctypes.data, first, ncols, irrep, lst))
+
+    def putlst_raw(self, buf, first, ncols, irrep, lst):
+        """buf: contiguous float64 buffer already in column-major order."""
+        self._chk("aces_putlst", self.h.aces_putlst(buf.ctypes.data, first, ncols, irrep, lst))
+
+    def getall(self, length, irrepx, lst):
+        out = np.zeros(length)
+        self._chk("aces_getall", self.h.aces_getall(out.ctypes.data, length, irrepx, lst))
+        return out
+
+    def putall(self, vec, irrepx, lst):
+        a = np.ascontiguousarray(vec, dtype=np.float64)
+        self._chk("aces_putall", self.h.aces_putall(a.ctypes.data, a.size, irrepx, lst))
+
+    # ---- records ------------------------------------------------------------------
+    def putrec(self, label, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._chk("aces_putrec", self.h.aces_putrec(label.encode(), a.nbytes, a.ctypes.data))
+
+    def getrec(self, label, n):
+        out = np.zeros(n)
+        self._chk("aces_getrec", self.h.aces_getrec(label.encode(), out.nbytes, out.ctypes.data))
+        return out
+
+    # ---- BLAS boundary ---------------------------------------------------------------
+    def xgemm(self, transa, transb, m, n, k, alpha, A_ptr, lda, B_ptr, ldb, beta, C_ptr, ldc,
+              precision=PREC_FP64):
+        """XGEMM on device pointers (column-major, tools/xgemm.F)."""
+        self._chk("aces_xgemm", self.h.aces_xgemm(transa.encode(), transb.encode(), m, n, k,
+                                                  alpha, A_ptr, lda, B_ptr, ldb, beta, C_ptr,
+                                                  ldc, precision))
+
+    # ---- programs -----------------------------------------------------------------
+    def _run(self, fn, cfg, allow_noconv=False):
+        st = getattr(self.h, fn)(C.byref(cfg))
+        if st != ACES_OK and not (allow_noconv and st == -9):
+            raise AcesError(fn, st, self.error())
+        return cfg
+
+    def xvcc(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, triples=0,
+             use_graph=0, verbose=0, allow_noconv=False):
+        cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
+                       precision=precision, triples=triples, use_graph=use_graph,
+                       verbose=verbose)
+        return self._run("xvcc_run", cfg, allow_noconv)
+
+    def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0):
+        cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
+                       precision=precision, verbose=verbose)
+        return self._run("xlambda_run", cfg)
+
+    def xdens(self):
+        return self._run("xdens_1pdm", CCConfig())
+
+
+_lib = None
+
+
+def load(path=LIBPATH):
+    global _lib
+    if _lib is None or _lib.path != path:
+        _lib = Lib(path)
+    return _lib
+
+
+# Integral lists read by xvcc_run: list id -> (row pair type, column pair type,
+# physicists' block and the transpose taking it to [row p, row q, col r, col s]).
+INTEGRAL_LISTS = {
+    13: (14, 14, "oooo", (0, 1, 2, 3)),    # <Ij|Kl>
+    10: (14, 18, "ooov", (0, 1, 2, 3)),    # <Ij|Ka>
+    16: (13, 14, "oovv", (2, 3, 0, 1)),    # <Ab|Ij>
+    25: (11, 11, "ovov", (1, 0, 3, 2)),    # <Ai|Bj> = <iA|jB>
+    30: (13, 11, "ovvv", (3, 2, 1, 0)),    # <Ab|Ci> = <iC|bA>
+    233: (13, 13, "vvvv", (0, 1, 2, 3)),   # <Ab|Cd>
+}
+
+
+def put_hamiltonian(lib, eps, blocks, irr_o, irr_v, fock=None):
+    """Write orbital energies and the six integral lists the way the reference's
+    intprc does (intprc/clmoio.F).  ``blocks`` maps 'oooo', 'ooov', 'oovv',
+    'ovov', 'ovvv', 'vvvv' to dense physicists'-notation arrays <pq|rs>."""
+    dpd = DPD(lib, irr_o, irr_v)
+    lib.putrec("SCFEVALA", np.asarray(eps, dtype=np.float64))
+    if fock is not None:
+        lib.putrec("FOCKMAT", np.asarray(fock, dtype=np.float64))
+    for lst, (tl, tr, key, perm) in INTEGRAL_LISTS.items():
+        dense = blocks[key] if perm == (0, 1, 2, 3) else blocks[key].transpose(perm)
+        put_dense_list(lib, dpd, lst, tl, tr, dense)
+    return dpd

@@ -1,0 +1,87 @@
+// common.cuh -- shared state and helpers of the B200 CC engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/aces_b200.h"
+
+namespace acesb200 {
+
+void set_error(const char *fmt, ...);
+
+#define ACES_CUDA(call)                                                        \
+  do {                                                                         \
+    cudaError_t _e = (call);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      ::acesb200::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,         \
+                            cudaGetErrorString(_e));                           \
+      return ACES_ERR_CUDA;                                                    \
+    }                                                                          \
+  } while (0)
+
+#define ACES_TRY(call)                                                         \
+  do {                                                                         \
+    int _s = (call);                                                           \
+    if (_s != ACES_OK) return _s;                                              \
+  } while (0)
+
+// One irrep block of a list: nrows x ncols doubles, column-major, on device.
+struct ListBlock {
+  int nrows = 0;
+  int ncols = 0;
+  double *dev = nullptr;
+};
+
+// Bump allocator over large device chunks: lists live until aces_fin, like
+// the reference's single ICORE heap (acescore/aces_malloc.c).
+struct DeviceArena {
+  struct Chunk { char *base; size_t size; size_t used; };
+  std::vector<Chunk> chunks;
+  size_t chunk_bytes = size_t(256) << 20;
+  void *alloc(size_t bytes);
+  void release();
+  size_t total() const;
+};
+
+struct SymInfo {
+  int nirrep = 0;
+  int pop[8] = {0};
+  int vrt[8] = {0};
+  int irpdpd[8][22] = {{0}};     // [irrep][type]
+  int isymoff[8][8][25] = {{{0}}};  // [irp_q][irp_pq][type], 1-based
+  bool ready = false;
+};
+
+struct State {
+  std::recursive_mutex mu;
+  int device = -1;
+  SymInfo sym;
+  std::map<int, std::vector<ListBlock>> lists;  // list id -> 8 irreps
+  std::map<int, std::pair<int, int>> isytyp;    // list -> (left, right) type
+  std::map<std::string, std::vector<char>> records;
+  DeviceArena arena;
+};
+
+State &state();
+
+// pair-type description: spins and occupied/virtual character of each index
+struct PairType {
+  char p, q;       // 'O' or 'V'
+  int packing;     // 0 FULL, 1 PACK (p<q), 2 PCK2 (p<=q)
+};
+PairType pair_type(int type);   // type 1..25
+
+// Orbital count of irrep h (0-based) for 'O'/'V' (RHF: alpha == beta).
+inline int norb(const SymInfo &s, char c, int h) { return c == 'O' ? s.pop[h] : s.vrt[h]; }
+
+// 0-based pair index (within the pairs of total irrep hpq) of local orbitals
+// p (irrep hp) and q (irrep hq), or -1 when the pair is not stored
+// (p >= q in a PACK block, p > q in a PCK2 block).
+long long pair_index(const SymInfo &s, int type, int hp, int p, int hq, int q);
+
+}  // namespace acesb200

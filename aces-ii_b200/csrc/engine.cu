@@ -1,0 +1,795 @@
+// engine.cu -- closed-shell CCSD on the device: list input, the residual of
+// one xvcc iteration (vcc/vcc.F:811-1024) as NT contractions + resorts,
+// NEWT2/E4SENG, CMPENG and DIIS (vcc/dodiis0.F) without host round trips
+// except the 5 scalars of the convergence test.
+//
+// Index conventions (C order): t1[i,a]; t2[i,j,a,b] = t_{iJ}^{aB} (the
+// reference's list 46, Ab x Ij, in C1); integrals <pq|rs> as I_xxxx[p,q,r,s].
+#include <cmath>
+#include <cstring>
+#include <initializer_list>
+
+#include "engine.cuh"
+
+namespace acesb200 {
+
+static const long long kHuge = 1LL << 62;
+
+CCEngine::~CCEngine() { release(); }
+
+void CCEngine::release() {
+  DBuf *all[] = {&eo, &ev, &foo, &fvv, &fov, &offo, &offv, &fovT, &I_oooo, &I_ooov, &I_oovv,
+                 &I_ovov, &I_ovvv, &I_vvvv, &L_oovv, &LF, &LovP, &LooP, &LmeP, &I1, &I2, &IvP,
+                 &IvP2, &IX, &IX2, &WA0, &WB0, &IoP3, &IvT, &IvT2, &IooT, &LT1, &X, &Xn, &Z1,
+                 &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
+                 &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
+                 &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec};
+  for (DBuf *b : all) {
+    if (b->p) cudaFree(b->p);
+    b->p = nullptr;
+    b->n = 0;
+  }
+  for (auto &b : hx) if (b.p) cudaFree(b.p);
+  for (auto &b : he) if (b.p) cudaFree(b.p);
+  hx.clear();
+  he.clear();
+  for (auto &e : split_cache) {
+    if (e.op.hi) cudaFree(e.op.hi);
+  }
+  split_cache.clear();
+  if (split_tmpA.hi) cudaFree(split_tmpA.hi);
+  if (split_tmpB.hi) cudaFree(split_tmpB.hi);
+  split_tmpA = SplitOperand();
+  split_tmpB = SplitOperand();
+  if (st) cudaStreamDestroy(st);
+  st = 0;
+}
+
+int CCEngine::alloc(DBuf &b, size_t n) {
+  if (b.p && b.n >= n) return ACES_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.n = 0;
+  size_t bytes = (n ? n : 1) * sizeof(double);
+  if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("engine: cudaMalloc of %zu bytes failed", bytes);
+    return ACES_ERR_NOMEM;
+  }
+  b.n = n;
+  ACES_CUDA(cudaMemsetAsync(b.p, 0, bytes, st));
+  return ACES_OK;
+}
+
+int CCEngine::copy(double *dst, const double *src, size_t n) {
+  if (n) ACES_CUDA(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, st));
+  return ACES_OK;
+}
+
+int CCEngine::perm(double *out, int n0, int n1, int n2, int n3, double beta,
+                   std::initializer_list<PermTerm> terms) {
+  PermSpec s;
+  s.n[0] = n0; s.n[1] = n1; s.n[2] = n2; s.n[3] = n3;
+  s.nterms = 0;
+  s.beta = beta;
+  for (const PermTerm &t : terms) s.t[s.nterms++] = t;
+  return permute(out, s, st);
+}
+
+static PermTerm PT(const double *src, double alpha, long long s0, long long s1, long long s2,
+                   long long s3) {
+  PermTerm t;
+  t.src = src;
+  t.alpha = alpha;
+  t.s[0] = s0; t.s[1] = s1; t.s[2] = s2; t.s[3] = s3;
+  return t;
+}
+
+int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long lda, const double *B,
+                long long ldb, double beta, const CView &C, bool constA, bool constB) {
+  gemm_calls++;
+  gemm_flops += 2.0 * M * N * (double)K;
+  bool split = prec == ACES_PREC_BF16X3 && (double)M * N * K >= 1.0e7 && K >= 16;
+  if (!split) return gemm_nt_f64(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
+  auto get = [&](const double *src, long long ld, int rows, bool cst, SplitOperand &tmp,
+                 const SplitOperand **out) -> int {
+    if (cst) {
+      for (auto &e : split_cache)
+        if (e.src == src && e.op.rows == rows && e.op.k == K) { *out = &e.op; return ACES_OK; }
+      SplitEntry e;
+      e.src = src;
+      ACES_TRY(split_pack(e.op, src, ld, rows, K, st));
+      split_cache.push_back(e);
+      *out = &split_cache.back().op;
+      return ACES_OK;
+    }
+    ACES_TRY(split_pack(tmp, src, ld, rows, K, st));
+    *out = &tmp;
+    return ACES_OK;
+  };
+  const SplitOperand *a = nullptr, *b = nullptr;
+  ACES_TRY(get(A, lda, M, constA, split_tmpA, &a));
+  ACES_TRY(get(B, ldb, N, constB, split_tmpB, &b));
+  return gemm_nt_bf16x3(*a, *b, M, N, alpha, beta, C, st);
+}
+
+// ---------------------------------------------------------------------------
+// list input
+// ---------------------------------------------------------------------------
+namespace {
+struct HostMap {
+  std::vector<int> rowidx, colidx;
+  std::vector<signed char> rowsgn, colsgn;
+};
+
+void pair_table(const SymInfo &s, int type, const std::vector<int> &irr_p,
+                const std::vector<int> &loc_p, const std::vector<int> &irr_q,
+                const std::vector<int> &loc_q, std::vector<int> &idx,
+                std::vector<signed char> &sgn) {
+  int np = (int)irr_p.size(), nq = (int)irr_q.size();
+  idx.assign((size_t)np * nq, -1);
+  sgn.assign((size_t)np * nq, 0);
+  PairType t = pair_type(type);
+  for (int p = 0; p < np; ++p)
+    for (int q = 0; q < nq; ++q) {
+      int hp = irr_p[p], hq = irr_q[q], lp = loc_p[p], lq = loc_q[q];
+      long long k;
+      if (t.packing == 0) {
+        idx[(size_t)p * nq + q] = (int)pair_index(s, type, hp, lp, hq, lq);
+        sgn[(size_t)p * nq + q] = 1;
+      } else if (hp < hq || (hp == hq && lp < lq)) {
+        idx[(size_t)p * nq + q] = (int)pair_index(s, type, hp, lp, hq, lq);
+        sgn[(size_t)p * nq + q] = 1;
+      } else if (hp > hq || (hp == hq && lp > lq)) {
+        k = pair_index(s, type, hq, lq, hp, lp);
+        idx[(size_t)p * nq + q] = (int)k;
+        sgn[(size_t)p * nq + q] = t.packing == 1 ? -1 : 2;  // 2: PCK2 swapped, same value
+      }
+      // p == q in a PACK type: not stored (zero)
+    }
+}
+
+struct DevMap {
+  int *d_rowidx = nullptr, *d_colidx = nullptr;
+  signed char *d_rowsgn = nullptr, *d_colsgn = nullptr;
+  int *d_irr[4] = {nullptr, nullptr, nullptr, nullptr};
+  double **d_base = nullptr;
+  int *d_nrows = nullptr;
+  DpdMap m;
+  ~DevMap() {
+    cudaFree(d_rowidx); cudaFree(d_colidx); cudaFree(d_rowsgn); cudaFree(d_colsgn);
+    for (int k = 0; k < 4; ++k) cudaFree(d_irr[k]);
+    cudaFree(d_base); cudaFree(d_nrows);
+  }
+};
+
+template <class T>
+int upload(T **d, const std::vector<T> &h) {
+  ACES_CUDA(cudaMalloc(d, std::max<size_t>(1, h.size()) * sizeof(T)));
+  if (!h.empty()) ACES_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return ACES_OK;
+}
+
+int make_map(DevMap &dm, int list, int typeL, int typeR, const std::vector<int> &irr_o,
+             const std::vector<int> &irr_v, bool create) {
+  State &stt = state();
+  const SymInfo &s = stt.sym;
+  auto orbs = [&](char c, std::vector<int> &irr, std::vector<int> &loc) {
+    irr = c == 'O' ? irr_o : irr_v;
+    loc.resize(irr.size());
+    int cnt[8] = {0};
+    for (size_t k = 0; k < irr.size(); ++k) loc[k] = cnt[irr[k]]++;
+  };
+  PairType L = pair_type(typeL), R = pair_type(typeR);
+  std::vector<int> ip, lp, iq, lq, ir, lr, is, ls;
+  orbs(L.p, ip, lp); orbs(L.q, iq, lq); orbs(R.p, ir, lr); orbs(R.q, is, ls);
+  HostMap hm;
+  pair_table(s, typeL, ip, lp, iq, lq, hm.rowidx, hm.rowsgn);
+  pair_table(s, typeR, ir, lr, is, ls, hm.colidx, hm.colsgn);
+  if (create) ACES_TRY(aces_inipck(1, typeL, typeR, list, 1));
+  std::vector<double *> base(8, nullptr);
+  std::vector<int> nrows(8, 0);
+  for (int h = 0; h < s.nirrep; ++h) {
+    int nc = 0, nr = 0;
+    aces_list_dims(h + 1, list, &nc, &nr);
+    if (nc != s.irpdpd[h][typeR - 1] || nr != s.irpdpd[h][typeL - 1]) {
+      set_error("list %d irrep %d has %dx%d, expected %dx%d (types %d,%d)", list, h + 1, nr, nc,
+                s.irpdpd[h][typeL - 1], s.irpdpd[h][typeR - 1], typeL, typeR);
+      return ACES_ERR_NOLIST;
+    }
+    base[h] = aces_list_devptr(h + 1, list);
+    nrows[h] = nr;
+  }
+  ACES_TRY(upload(&dm.d_rowidx, hm.rowidx));
+  ACES_TRY(upload(&dm.d_colidx, hm.colidx));
+  ACES_TRY(upload(&dm.d_rowsgn, hm.rowsgn));
+  ACES_TRY(upload(&dm.d_colsgn, hm.colsgn));
+  ACES_TRY(upload(&dm.d_irr[0], ip));
+  ACES_TRY(upload(&dm.d_irr[1], iq));
+  ACES_TRY(upload(&dm.d_irr[2], ir));
+  ACES_TRY(upload(&dm.d_irr[3], is));
+  ACES_TRY(upload(&dm.d_base, base));
+  ACES_TRY(upload(&dm.d_nrows, nrows));
+  dm.m.rowidx = dm.d_rowidx; dm.m.colidx = dm.d_colidx;
+  dm.m.rowsgn = dm.d_rowsgn; dm.m.colsgn = dm.d_colsgn;
+  dm.m.irr_p = dm.d_irr[0]; dm.m.irr_q = dm.d_irr[1];
+  dm.m.irr_r = dm.d_irr[2]; dm.m.irr_s = dm.d_irr[3];
+  dm.m.base = dm.d_base; dm.m.nrows = dm.d_nrows;
+  dm.m.np = (int)ip.size(); dm.m.nq = (int)iq.size();
+  dm.m.nr = (int)ir.size(); dm.m.ns = (int)is.size();
+  return ACES_OK;
+}
+}  // namespace
+
+int CCEngine::load_from_lists() {
+  State &stt = state();
+  const SymInfo &s = stt.sym;
+  if (!s.ready) {
+    set_error("xvcc_run: symmetry not initialised (aces_sym_init)");
+    return ACES_ERR_NOSYM;
+  }
+  if (!st) ACES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  o = v = 0;
+  irr_o.clear(); irr_v.clear();
+  for (int h = 0; h < s.nirrep; ++h) {
+    for (int k = 0; k < s.pop[h]; ++k) irr_o.push_back(h);
+    for (int k = 0; k < s.vrt[h]; ++k) irr_v.push_back(h);
+    o += s.pop[h];
+    v += s.vrt[h];
+  }
+  nmo = o + v;
+  if (o == 0 || v == 0) {
+    set_error("xvcc_run: empty occupied or virtual space");
+    return ACES_ERR_ARG;
+  }
+  eps_h.assign(nmo, 0.0);
+  ACES_TRY(aces_getrec("SCFEVALA", (long long)nmo * 8, eps_h.data()));
+  std::vector<double> F((size_t)nmo * nmo, 0.0);
+  nonhf = aces_reclen("FOCKMAT") == (long long)nmo * nmo * 8;
+  if (nonhf) {
+    ACES_TRY(aces_getrec("FOCKMAT", (long long)nmo * nmo * 8, F.data()));
+    for (int p = 0; p < nmo; ++p) eps_h[p] = F[(size_t)p * nmo + p];
+  } else {
+    for (int p = 0; p < nmo; ++p) F[(size_t)p * nmo + p] = eps_h[p];
+  }
+  for (double x : eps_h)
+    if (!std::isfinite(x)) {
+      set_error("xvcc_run: non-finite orbital energy");
+      return ACES_ERR_NAN;
+    }
+  std::vector<double> hoo((size_t)o * o), hvv((size_t)v * v), hov((size_t)o * v),
+      hofo((size_t)o * o), hofv((size_t)v * v), hfovT((size_t)v * o);
+  for (int i = 0; i < o; ++i)
+    for (int j = 0; j < o; ++j) {
+      hoo[i * o + j] = F[(size_t)i * nmo + j];
+      hofo[i * o + j] = i == j ? 0.0 : F[(size_t)i * nmo + j];
+    }
+  for (int a = 0; a < v; ++a)
+    for (int b = 0; b < v; ++b) {
+      hvv[a * v + b] = F[(size_t)(o + a) * nmo + o + b];
+      hofv[a * v + b] = a == b ? 0.0 : F[(size_t)(o + a) * nmo + o + b];
+    }
+  for (int i = 0; i < o; ++i)
+    for (int a = 0; a < v; ++a) {
+      hov[i * v + a] = F[(size_t)i * nmo + o + a];
+      hfovT[a * o + i] = F[(size_t)i * nmo + o + a];
+    }
+  ACES_TRY(alloc(eo, o)); ACES_TRY(alloc(ev, v));
+  ACES_TRY(alloc(foo, (size_t)o * o)); ACES_TRY(alloc(fvv, (size_t)v * v));
+  ACES_TRY(alloc(fov, (size_t)o * v)); ACES_TRY(alloc(offo, (size_t)o * o));
+  ACES_TRY(alloc(offv, (size_t)v * v)); ACES_TRY(alloc(fovT, (size_t)o * v));
+  auto h2d = [&](DBuf &b, const std::vector<double> &h) -> int {
+    ACES_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
+    return ACES_OK;
+  };
+  std::vector<double> heo(eps_h.begin(), eps_h.begin() + o), hev(eps_h.begin() + o, eps_h.end());
+  ACES_TRY(h2d(eo, heo)); ACES_TRY(h2d(ev, hev));
+  ACES_TRY(h2d(foo, hoo)); ACES_TRY(h2d(fvv, hvv)); ACES_TRY(h2d(fov, hov));
+  ACES_TRY(h2d(offo, hofo)); ACES_TRY(h2d(offv, hofv)); ACES_TRY(h2d(fovT, hfovT));
+  ACES_CUDA(cudaStreamSynchronize(st));
+
+  const long long O = o, V = v;
+  // list 13 (14,14): <Ij|Kl>  -> I_oooo[i,j,k,l]
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 13, 14, 14, irr_o, irr_v, false));
+    ACES_TRY(alloc(I_oooo, O * O * O * O));
+    launch_gather(I_oooo.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // list 10 (14,18): <Ij|Ka>  -> I_ooov[i,j,k,a]
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 10, 14, 18, irr_o, irr_v, false));
+    ACES_TRY(alloc(I_ooov, O * O * O * V));
+    launch_gather(I_ooov.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // list 16 (13,14): <Ab|Ij> -> dense [a,b,i,j] -> I_oovv[i,j,a,b]
+  ACES_TRY(alloc(tmp4, std::max(O * O * V * V, O * V * V * V)));
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 16, 13, 14, irr_o, irr_v, false));
+    launch_gather(tmp4.p, dm.m, st);
+    ACES_TRY(alloc(I_oovv, O * O * V * V));
+    // out (i,j,a,b) <- tmp[a,b,i,j]
+    ACES_TRY(perm(I_oovv.p, o, o, v, v, 0.0, {PT(tmp4.p, 1.0, O, 1, V * O * O, O * O)}));
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // list 25 (11,11): <Ai|Bj> -> dense [a,i,b,j] = <ai|bj>; I_ovov[m,b,j,e] = <mb|je> = <bm|ej> = d[b,m,e,j]
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 25, 11, 11, irr_o, irr_v, false));
+    launch_gather(tmp4.p, dm.m, st);
+    ACES_TRY(alloc(I_ovov, O * O * V * V));
+    // d strides: [a,i,b,j] -> a: O*V*O, i: V*O, b: O, j: 1 ; out (m,b,j,e) = d[b,m,e,j]
+    ACES_TRY(perm(I_ovov.p, o, v, o, v, 0.0,
+                  {PT(tmp4.p, 1.0, V * O, O * V * O, 1, O)}));
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // list 30 (13,11): <Ab|Ci> -> dense [a,b,c,i]; I_ovvv[m,a,e,f] = <ma|ef> = <fe|am> = d[f,e,a,m]
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 30, 13, 11, irr_o, irr_v, false));
+    launch_gather(tmp4.p, dm.m, st);
+    ACES_TRY(alloc(I_ovvv, O * V * V * V));
+    // d strides [a,b,c,i]: a: V*V*O, b: V*O, c: O, i: 1; out (m,a,e,f) = d[f,e,a,m]
+    ACES_TRY(perm(I_ovvv.p, o, v, v, v, 0.0, {PT(tmp4.p, 1.0, 1, O, V * O, V * V * O)}));
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // list 233 (13,13): <Ab|Cd> -> I_vvvv[a,b,c,d]
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 233, 13, 13, irr_o, irr_v, false));
+    ACES_TRY(alloc(I_vvvv, V * V * V * V));
+    launch_gather(I_vvvv.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  return ACES_OK;
+}
+
+// ---------------------------------------------------------------------------
+// iteration-independent resorted integrals
+// ---------------------------------------------------------------------------
+int CCEngine::setup_intermediates() {
+  const long long O = o, V = v;
+  const long long OV = O * V, OOVV = O * O * V * V, OVVV = O * V * V * V, OOOV = O * O * O * V;
+  // strides of the base arrays
+  // I_oovv[m,n,e,f]: (O*V*V, V*V, V, 1); I_ovvv[m,a,e,f]: (V*V*V, V*V, V, 1)
+  // I_ooov[m,n,i,e]: (O*O*V, O*V, V, 1); I_ovov[m,b,j,e]: (V*O*V, O*V, V, 1)
+  const long long so[4] = {O * V * V, V * V, V, 1};
+  const long long sv[4] = {V * V * V, V * V, V, 1};
+  const long long s3[4] = {O * O * V, O * V, V, 1};
+  const long long sj[4] = {V * O * V, O * V, V, 1};
+  ACES_TRY(alloc(L_oovv, OOVV));
+  ACES_TRY(perm(L_oovv.p, o, o, v, v, 0.0,
+                {PT(I_oovv.p, 2.0, so[0], so[1], so[2], so[3]),
+                 PT(I_oovv.p, -1.0, so[0], so[1], so[3], so[2])}));
+  // LF[a,e,m,f] = 2 I_ovvv[m,a,f,e] - I_ovvv[m,a,e,f]
+  ACES_TRY(alloc(LF, OVVV));
+  ACES_TRY(perm(LF.p, v, v, o, v, 0.0,
+                {PT(I_ovvv.p, 2.0, sv[1], sv[3], sv[0], sv[2]),
+                 PT(I_ovvv.p, -1.0, sv[1], sv[2], sv[0], sv[3])}));
+  // LovP[e,m,n,f] = L_oovv[m,n,e,f]
+  ACES_TRY(alloc(LovP, OOVV));
+  ACES_TRY(perm(LovP.p, v, o, o, v, 0.0, {PT(L_oovv.p, 1.0, so[2], so[0], so[1], so[3])}));
+  // LooP[m,i,n,e] = 2 I_ooov[m,n,i,e] - I_ooov[n,m,i,e]
+  ACES_TRY(alloc(LooP, OOOV));
+  ACES_TRY(perm(LooP.p, o, o, o, v, 0.0,
+                {PT(I_ooov.p, 2.0, s3[0], s3[2], s3[1], s3[3]),
+                 PT(I_ooov.p, -1.0, s3[1], s3[2], s3[0], s3[3])}));
+  // LmeP[m,e,n,f] = L_oovv[m,n,e,f]
+  ACES_TRY(alloc(LmeP, OOVV));
+  ACES_TRY(perm(LmeP.p, o, v, o, v, 0.0, {PT(L_oovv.p, 1.0, so[0], so[2], so[1], so[3])}));
+  // I1[m,e,n,f] = I_oovv[m,n,e,f];  I2[m,e,n,f] = I_oovv[m,n,f,e]
+  ACES_TRY(alloc(I1, OOVV));
+  ACES_TRY(perm(I1.p, o, v, o, v, 0.0, {PT(I_oovv.p, 1.0, so[0], so[2], so[1], so[3])}));
+  ACES_TRY(alloc(I2, OOVV));
+  ACES_TRY(perm(I2.p, o, v, o, v, 0.0, {PT(I_oovv.p, 1.0, so[0], so[3], so[1], so[2])}));
+  // IvP[b,m,e,f] = I_ovvv[m,b,e,f]; IvP2[b,m,e,f] = I_ovvv[m,b,f,e]
+  ACES_TRY(alloc(IvP, OVVV));
+  ACES_TRY(perm(IvP.p, v, o, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[1], sv[0], sv[2], sv[3])}));
+  ACES_TRY(alloc(IvP2, OVVV));
+  ACES_TRY(perm(IvP2.p, v, o, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[1], sv[0], sv[3], sv[2])}));
+  // IX[j,m,e,n] = I_ooov[n,m,j,e]; IX2[j,m,e,n] = I_ooov[m,n,j,e]
+  ACES_TRY(alloc(IX, OOOV));
+  ACES_TRY(perm(IX.p, o, o, v, o, 0.0, {PT(I_ooov.p, 1.0, s3[2], s3[1], s3[3], s3[0])}));
+  ACES_TRY(alloc(IX2, OOOV));
+  ACES_TRY(perm(IX2.p, o, o, v, o, 0.0, {PT(I_ooov.p, 1.0, s3[2], s3[0], s3[3], s3[1])}));
+  // WA0[j,b,m,e] = <mb|ej> = I_oovv[m,j,e,b];  WB0[j,b,m,e] = -<mb|je> = -I_ovov[m,b,j,e]
+  ACES_TRY(alloc(WA0, OOVV));
+  ACES_TRY(perm(WA0.p, o, v, o, v, 0.0, {PT(I_oovv.p, 1.0, so[1], so[3], so[0], so[2])}));
+  ACES_TRY(alloc(WB0, OOVV));
+  ACES_TRY(perm(WB0.p, o, v, o, v, 0.0, {PT(I_ovov.p, -1.0, sj[2], sj[1], sj[0], sj[3])}));
+  // IoP3[i,j,b,m] = I_ooov[i,j,m,b]
+  ACES_TRY(alloc(IoP3, OOOV));
+  ACES_TRY(perm(IoP3.p, o, o, v, o, 0.0, {PT(I_ooov.p, 1.0, s3[0], s3[1], s3[3], s3[2])}));
+  // IvT[j,a,b,e] = I_ovvv[j,e,b,a]; IvT2[a,m,e,f] = I_ovvv[m,a,e,f]
+  ACES_TRY(alloc(IvT, OVVV));
+  ACES_TRY(perm(IvT.p, o, v, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[0], sv[3], sv[2], sv[1])}));
+  ACES_TRY(alloc(IvT2, OVVV));
+  ACES_TRY(perm(IvT2.p, v, o, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[1], sv[0], sv[2], sv[3])}));
+  // IooT[i,m,n,e] = I_ooov[m,n,i,e]
+  ACES_TRY(alloc(IooT, OOOV));
+  ACES_TRY(perm(IooT.p, o, o, o, v, 0.0, {PT(I_ooov.p, 1.0, s3[2], s3[0], s3[1], s3[3])}));
+  // LT1[i,a,n,f] = 2<na|fi> - <na|if> = 2 I_oovv[n,i,f,a] - I_ovov[n,a,i,f]
+  ACES_TRY(alloc(LT1, OOVV));
+  ACES_TRY(perm(LT1.p, o, v, o, v, 0.0,
+                {PT(I_oovv.p, 2.0, so[1], so[3], so[0], so[2]),
+                 PT(I_ovov.p, -1.0, sj[2], sj[1], sj[0], sj[3])}));
+  // working storage
+  ACES_TRY(alloc(X, OV + OOVV));
+  ACES_TRY(alloc(Xn, OV + OOVV));
+  ACES_TRY(alloc(Z1, OV));
+  ACES_TRY(alloc(Z2, OOVV));
+  DBuf *big[] = {&tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P,
+                 &Y1, &Y2, &XnP, &WA, &WB, &XP};
+  for (DBuf *b : big) ACES_TRY(alloc(*b, OOVV));
+  ACES_TRY(alloc(ZT, OOOV));
+  ACES_TRY(alloc(Xmn, O * O * O * O));
+  ACES_TRY(alloc(Wmnij, O * O * O * O));
+  ACES_TRY(alloc(WmnT, O * O * O * O));
+  ACES_TRY(alloc(t1T, OV));
+  ACES_TRY(alloc(Fae, V * V)); ACES_TRY(alloc(Fp, V * V));
+  ACES_TRY(alloc(Fmi, O * O)); ACES_TRY(alloc(Fpp, O * O));
+  ACES_TRY(alloc(FmiT, O * O)); ACES_TRY(alloc(FppT, O * O));
+  ACES_TRY(alloc(Fme, OV)); ACES_TRY(alloc(FmeT, OV));
+  ACES_TRY(alloc(scratch, 592 * 32));
+  ACES_TRY(alloc(dev_small, 64 + 25 * 25 + 32));
+  ACES_TRY(alloc(Bmat, 25 * 25));
+  ACES_CUDA(cudaStreamSynchronize(st));
+  // tmp4 is no longer needed
+  if (tmp4.p) { cudaFree(tmp4.p); tmp4.p = nullptr; tmp4.n = 0; }
+  return ACES_OK;
+}
+
+int CCEngine::mp2_guess() {
+  // T2 = <ij|ab>/D, T1 = 0 (intprc FORMT2)
+  ACES_CUDA(cudaMemsetAsync(Z1.p, 0, (size_t)o * v * 8, st));
+  launch_newt(t2(), I_oovv.p, t1(), Z1.p, eo.p, ev.p, o, v, st);
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the residual of one CCSD iteration: Z1, Z2 from X = [t1 | t2]
+// ---------------------------------------------------------------------------
+int CCEngine::residual() {
+  const long long O = o, V = v;
+  const long long OV = O * V, VV = V * V, OO = O * O, OVV = O * V * V, OOV = O * O * V;
+  double *T1 = t1(), *T2 = t2();
+  const long long st2[4] = {O * V * V, V * V, V, 1};  // t2[i,j,a,b]
+  // t1T[a,m]
+  ACES_TRY(perm(t1T.p, 1, 1, v, o, 0.0, {PT(T1, 1.0, 0, 0, 1, V)}));
+  // FTAU (libr/ftau.f)
+  launch_tau(tau.p, T2, T1, 1.0, o, v, st);
+  launch_tau(taut.p, T2, T1, 0.5, o, v, st);
+  // ---- F(ae): QUAD3 + T1RING (vcc/quad3.f, libr/t1ring.F) ----
+  ACES_TRY(copy(Fae.p, offv.p, VV));
+  ACES_TRY(G(v, v, o, -0.5, t1T.p, O, fovT.p, O, 1.0, cview_rowmajor(Fae.p, V)));
+  ACES_TRY(G(v * v, 1, o * v, 1.0, LF.p, OV, T1, OV, 1.0, cview_rowmajor(Fae.p, 1), true));
+  // tautP[a,m,n,f] = taut[m,n,a,f]
+  ACES_TRY(perm(tautP.p, v, o, o, v, 0.0, {PT(taut.p, 1.0, st2[2], st2[0], st2[1], st2[3])}));
+  ACES_TRY(G(v, v, o * o * v, -1.0, tautP.p, OOV, LovP.p, OOV, 1.0, cview_rowmajor(Fae.p, V),
+             false, true));
+  // ---- F(mi): QUAD2 + T1INW2 (vcc/quad2.f, vcc/t1inw2.f) ----
+  ACES_TRY(copy(Fmi.p, offo.p, OO));
+  ACES_TRY(G(o, o, v, 0.5, fov.p, V, T1, V, 1.0, cview_rowmajor(Fmi.p, O)));
+  ACES_TRY(G(o * o, 1, o * v, 1.0, LooP.p, OV, T1, OV, 1.0, cview_rowmajor(Fmi.p, 1), true));
+  ACES_TRY(G(o, o, o * v * v, 1.0, L_oovv.p, OVV, taut.p, OVV, 1.0, cview_rowmajor(Fmi.p, O),
+             true));
+  // ---- F(me): MAKFME (vcc/makfme.F) ----
+  ACES_TRY(copy(Fme.p, fov.p, OV));
+  ACES_TRY(G(o * v, 1, o * v, 1.0, LmeP.p, OV, T1, OV, 1.0, cview_rowmajor(Fme.p, 1), true));
+  // F'(be) = F(be) - 1/2 t(mb) F(me);  F''(mj) = F(mj) + 1/2 F(me) t(je)
+  ACES_TRY(perm(FmeT.p, 1, 1, v, o, 0.0, {PT(Fme.p, 1.0, 0, 0, 1, V)}));
+  ACES_TRY(copy(Fp.p, Fae.p, VV));
+  ACES_TRY(G(v, v, o, -0.5, t1T.p, O, FmeT.p, O, 1.0, cview_rowmajor(Fp.p, V)));
+  ACES_TRY(copy(Fpp.p, Fmi.p, OO));
+  ACES_TRY(G(o, o, v, 0.5, Fme.p, V, T1, V, 1.0, cview_rowmajor(Fpp.p, O)));
+  ACES_TRY(perm(FppT.p, 1, 1, o, o, 0.0, {PT(Fpp.p, 1.0, 0, 0, 1, O)}));
+  ACES_TRY(perm(FmiT.p, 1, 1, o, o, 0.0, {PT(Fmi.p, 1.0, 0, 0, 1, O)}));
+
+  // ---- T1 increments (INITSN, FEACONT, FMICONT, FMECONT, T1INT1, E4S) ----
+  ACES_TRY(copy(Z1.p, fov.p, OV));
+  ACES_TRY(G(o, v, v, 1.0, T1, V, Fae.p, V, 1.0, cview_rowmajor(Z1.p, V)));
+  ACES_TRY(G(o, v, o, -1.0, FmiT.p, O, t1T.p, O, 1.0, cview_rowmajor(Z1.p, V)));
+  // U[i,a,m,e] = 2 t2[i,m,a,e] - t2[m,i,a,e]
+  ACES_TRY(perm(U.p, o, v, o, v, 0.0,
+                {PT(T2, 2.0, st2[0], st2[2], st2[1], st2[3]),
+                 PT(T2, -1.0, st2[1], st2[2], st2[0], st2[3])}));
+  ACES_TRY(G(o * v, 1, o * v, 1.0, U.p, OV, Fme.p, OV, 1.0, cview_rowmajor(Z1.p, 1)));
+  ACES_TRY(G(o * v, 1, o * v, 1.0, LT1.p, OV, T1, OV, 1.0, cview_rowmajor(Z1.p, 1), true));
+  // T2T1AB1: wP[i,m,e,f] = 2 t2[i,m,f,e] - t2[i,m,e,f];  Z1[i,a] += sum IvT2[a,(mef)] wP[i,(mef)]
+  ACES_TRY(perm(wP.p, o, o, v, v, 0.0,
+                {PT(T2, 2.0, st2[0], st2[1], st2[3], st2[2]),
+                 PT(T2, -1.0, st2[0], st2[1], st2[2], st2[3])}));
+  ACES_TRY(G(v, o, o * v * v, 1.0, IvT2.p, OVV, wP.p, OVV, 1.0, cview_colmajor(Z1.p, V), true));
+  // T2T1AB2: uT[a,m,n,e] = 2 t2[m,n,a,e] - t2[n,m,a,e];  Z1[i,a] -= sum uT[a,(mne)] IooT[i,(mne)]
+  ACES_TRY(perm(uT.p, v, o, o, v, 0.0,
+                {PT(T2, 2.0, st2[2], st2[0], st2[1], st2[3]),
+                 PT(T2, -1.0, st2[2], st2[1], st2[0], st2[3])}));
+  ACES_TRY(G(v, o, o * o * v, -1.0, uT.p, OOV, IooT.p, OOV, 1.0, cview_colmajor(Z1.p, V), false,
+             true));
+
+  // ---- W(mnij) (QUAD1, T1INW2) and the hole-hole ladder (DRLAD ITYPE=1) ----
+  ACES_TRY(G(o * o * o, o, v, 1.0, I_ooov.p, V, T1, V, 0.0, cview_rowmajor(Xmn.p, O), true));
+  const long long s4[4] = {O * O * O, O * O, O, 1};
+  ACES_TRY(perm(Wmnij.p, o, o, o, o, 0.0,
+                {PT(I_oooo.p, 1.0, s4[0], s4[1], s4[2], s4[3]),
+                 PT(Xmn.p, 1.0, s4[0], s4[1], s4[2], s4[3]),
+                 PT(Xmn.p, 1.0, s4[1], s4[0], s4[3], s4[2])}));
+  ACES_TRY(G(o * o, o * o, v * v, 1.0, I_oovv.p, VV, tau.p, VV, 1.0,
+             cview_rowmajor(Wmnij.p, OO), true));
+  ACES_TRY(perm(WmnT.p, 1, 1, o * o, o * o, 0.0, {PT(Wmnij.p, 1.0, 0, 0, 1, OO)}));
+  // INITIN: Z2 <- <ij|ab>
+  ACES_TRY(copy(Z2.p, I_oovv.p, (size_t)OO * VV));
+  // tauT[a,b,m,n] = tau[m,n,a,b]
+  ACES_TRY(perm(tauT.p, v, v, o, o, 0.0, {PT(tau.p, 1.0, st2[2], st2[3], st2[0], st2[1])}));
+  ACES_TRY(G(v * v, o * o, o * o, 1.0, tauT.p, OO, WmnT.p, OO, 1.0, cview_colmajor(Z2.p, VV)));
+  // ---- particle-particle ladder (DRLAD ITYPE=6, vcc/ladab1.F:61) ----
+  ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0, cview_colmajor(Z2.p, VV),
+             true));
+
+  // ---- W(mbej) ABAB and ABBA (DWMBEJ, T1RING), layout W[j,b,m,e] ----
+  ACES_TRY(copy(WA.p, WA0.p, (size_t)OO * VV));
+  ACES_TRY(G(o, o * v * v, v, 1.0, T1, V, IvP.p, V, 1.0, cview_rowmajor(WA.p, OVV), false, true));
+  CView vWn{WA.p, kHuge, 0, OV, OV, OVV, 1};
+  ACES_TRY(G(v, o * o * v, o, -1.0, t1T.p, O, IX.p, O, 1.0, vWn, false, true));
+  // Y2[j,b,n,f] = t2[n,j,f,b];  XnP[j,b,n,f] = 1/2 t2[j,n,f,b] + t1[j,f] t1[n,b]; Y1 = Y2 - XnP
+  ACES_TRY(perm(Y2.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[1], st2[3], st2[0], st2[2])}));
+  ACES_TRY(perm(XnP.p, o, v, o, v, 0.0, {PT(T2, 0.5, st2[0], st2[3], st2[1], st2[2])}));
+  // + t1[j,f] t1[n,b]: rank-1 per (j,b,n,f) -> GEMM over a unit K: A[(j),f]... use outer product
+  {
+    // XnP[(j,b),(n,f)] += t1[j,f] t1[n,b] : as C[(j,n,f? )] is awkward; do it as K=1 products
+    // C[m=(j,f), n=(n,b)] = t1[j,f] * t1[n,b] mapped to XnP[j,b,n,f]
+    CView vx{XnP.p, V, OVV, 1, V, V, OV};
+    ACES_TRY(gemm_nt_f64(o * v, o * v, 1, 1.0, T1, 1, T1, 1, 1.0, vx, st));
+  }
+  ACES_TRY(perm(Y1.p, o, v, o, v, 0.0,
+                {PT(Y2.p, 1.0, OVV, OV, V, 1), PT(XnP.p, -1.0, OVV, OV, V, 1)}));
+  ACES_TRY(G(o * v, o * v, o * v, 1.0, Y1.p, OV, I1.p, OV, 1.0, cview_rowmajor(WA.p, OV), false,
+             true));
+  ACES_TRY(G(o * v, o * v, o * v, -0.5, Y2.p, OV, I2.p, OV, 1.0, cview_rowmajor(WA.p, OV), false,
+             true));
+  ACES_TRY(copy(WB.p, WB0.p, (size_t)OO * VV));
+  ACES_TRY(G(o, o * v * v, v, -1.0, T1, V, IvP2.p, V, 1.0, cview_rowmajor(WB.p, OVV), false, true));
+  CView vWn2{WB.p, kHuge, 0, OV, OV, OVV, 1};
+  ACES_TRY(G(v, o * o * v, o, 1.0, t1T.p, O, IX2.p, O, 1.0, vWn2, false, true));
+  ACES_TRY(G(o * v, o * v, o * v, 1.0, XnP.p, OV, I2.p, OV, 1.0, cview_rowmajor(WB.p, OV), false,
+             true));
+
+  // ---- terms symmetrised by P(ia,jb), accumulated in XP[i,j,a,b] ----
+  // FEACONT (vcc/feacont.f)
+  ACES_TRY(G(o * o * v, v, v, 1.0, T2, V, Fp.p, V, 0.0, cview_rowmajor(XP.p, V)));
+  // FMICONT (vcc/fmicont.f): t2P[i,a,b,m] = t2[i,m,a,b]
+  ACES_TRY(perm(t2P.p, o, v, v, o, 0.0, {PT(T2, 1.0, st2[0], st2[2], st2[3], st2[1])}));
+  CView vfm{XP.p, VV, OVV, 1, kHuge, 0, VV};
+  ACES_TRY(G(o * v * v, o, o, -1.0, t2P.p, O, FppT.p, O, 1.0, vfm));
+  // ZT[i,j,b,m] = <mb|ij> + sum_ef <mb|ef> tau(ij,ef) + sum_e <mb|ej> t(ie) + sum_e <mb|ie> t(je)
+  // (T1INT2A, T1INW1, T12INT2), then XP -= sum_m t(ma) ZT[(ijb), m]
+  ACES_TRY(copy(ZT.p, IoP3.p, (size_t)OOV * O));
+  CView vz1{ZT.p, V, 1, O, kHuge, 0, V * O};
+  ACES_TRY(G(o * v, o * o, v * v, 1.0, I_ovvv.p, VV, tau.p, VV, 1.0, vz1, true));
+  ACES_TRY(G(o * v * o, o, v, 1.0, WA0.p, V, T1, V, 1.0, cview_colmajor(ZT.p, OOV), true));
+  CView vz3{ZT.p, V * O, OOV, 1, kHuge, 0, V * O};
+  ACES_TRY(G(o * v * o, o, v, -1.0, WB0.p, V, T1, V, 1.0, vz3, true));
+  CView vxp{XP.p, V, VV, 1, kHuge, 0, V};
+  ACES_TRY(G(o * o * v, v, o, -1.0, ZT.p, O, t1T.p, O, 1.0, vxp));
+  // T1INT2B (vcc/t1int2b.f)
+  ACES_TRY(G(o, o * v * v, v, 1.0, T1, V, IvT.p, V, 1.0, cview_rowmajor(XP.p, OVV), false, true));
+  // ring (DRRNG/RNGDRV, vcc/rngdrv.f): Tp[i,a,m,e] = t2[i,m,a,e]; Tpp[j,a,m,e] = t2[j,m,e,a]
+  ACES_TRY(perm(Tp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[2], st2[1], st2[3])}));
+  ACES_TRY(perm(Tpp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[3], st2[1], st2[2])}));
+  CView vr1{XP.p, V, OVV, V, V, VV, 1};
+  ACES_TRY(G(o * v, o * v, o * v, 1.0, U.p, OV, WA.p, OV, 1.0, vr1));
+  ACES_TRY(G(o * v, o * v, o * v, 1.0, Tp.p, OV, WB.p, OV, 1.0, vr1));
+  CView vr3{XP.p, V, VV, V, V, OVV, 1};
+  ACES_TRY(G(o * v, o * v, o * v, 1.0, Tpp.p, OV, WB.p, OV, 1.0, vr3));
+  // Z2 += XP + XP^T(ia<->jb) (SUMSYM / SUMRNG)
+  ACES_TRY(perm(Z2.p, o, o, v, v, 1.0,
+                {PT(XP.p, 1.0, st2[0], st2[1], st2[2], st2[3]),
+                 PT(XP.p, 1.0, st2[1], st2[0], st2[3], st2[2])}));
+  return ACES_OK;
+}
+
+// One CC cycle: residual, Jacobi update, energy, DIIS (vcc/vcc.F:797-1087).
+int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, double *dres,
+                        bool *extrap) {
+  const long long len = (long long)o * v + (long long)o * o * v * v;
+  ACES_TRY(residual());
+  launch_newt(t2n(), Z2.p, t1n(), Z1.p, eo.p, ev.p, o, v, st);
+  double *d = dev_small.p;  // [0..2] energy, [3] res, [4] dres, [8..32] dots, [40..64] coef
+  launch_energy(d, t2n(), t1n(), I_oovv.p, fov.p, o, v, scratch.p, st);
+  int ndimr = icycle < exporder ? icycle : exporder;
+  int idimr = (icycle - 1) % exporder;
+  if ((int)hx.size() < exporder) {
+    hx.resize(exporder);
+    he.resize(exporder);
+  }
+  if (!hx[idimr].p) {
+    ACES_TRY(alloc(hx[idimr], len));
+    ACES_TRY(alloc(he[idimr], len));
+  }
+  ACES_TRY(copy(hx[idimr].p, X.p, len));
+  launch_diff(he[idimr].p, Xn.p, X.p, len, st);
+  launch_absmax(d + 3, he[idimr].p, o, v, scratch.p, st);
+  std::vector<const double *> hp(ndimr);
+  for (int k = 0; k < ndimr; ++k) hp[k] = he[k].p;
+  ACES_TRY(launch_diis_dots(d + 8, he[idimr].p, hp.data(), ndimr, o, v, scratch.p, st));
+  double hd[40];
+  ACES_CUDA(cudaMemcpyAsync(hd, d, 40 * 8, cudaMemcpyDeviceToHost, st));
+  ACES_CUDA(cudaStreamSynchronize(st));
+  e3[0] = hd[1];  // E_AA (printed alpha-alpha part)
+  e3[1] = hd[0];  // E_AB
+  e3[2] = 2.0 * hd[1] + hd[0] + hd[2];
+  *res = hd[3];
+  if (Bh.size() != 625) Bh.assign(625, 0.0);
+  for (int k = 0; k < ndimr; ++k) {
+    Bh[k * 25 + idimr] = hd[8 + k];
+    Bh[idimr * 25 + k] = hd[8 + k];
+  }
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(e3[k])) {
+      set_error("non-finite CC energy at cycle %d", icycle);
+      return ACES_ERR_NAN;
+    }
+  ACES_CUDA(cudaMemcpyAsync(Bmat.p, Bh.data(), 625 * 8, cudaMemcpyHostToDevice, st));
+  int *status = reinterpret_cast<int *>(d + 36);
+  launch_diis_solve(d + 40, status, Bmat.p, ndimr, st);
+  // DIIS residual dvec = sum_i c_i e_i (vcc/dodiis0.F:131-146)
+  std::vector<const double *> pe(ndimr);
+  for (int k = 0; k < ndimr; ++k) pe[k] = he[k].p;
+  ACES_TRY(alloc(dvec, len));
+  launch_lincomb(dvec.p, nullptr, d + 40, pe.data(), ndimr, len, st);
+  launch_absmax(d + 4, dvec.p, o, v, scratch.p, st);
+  int hstat = 0;
+  ACES_CUDA(cudaMemcpyAsync(&hstat, status, 4, cudaMemcpyDeviceToHost, st));
+  ACES_CUDA(cudaMemcpyAsync(dres, d + 4, 8, cudaMemcpyDeviceToHost, st));
+  ACES_CUDA(cudaStreamSynchronize(st));
+  if (hstat) {
+    set_error("DIIS bordered system singular at cycle %d", icycle);
+    return ACES_ERR_SINGULAR;
+  }
+  *extrap = ndimr >= 2;
+  return ACES_OK;
+}
+
+// accept the new amplitudes: extrapolated (DIIS) or plain Jacobi (DRMOVE)
+static int accept(CCEngine &E, bool extrap, int ndimr) {
+  const long long len = (long long)E.o * E.v + (long long)E.o * E.o * E.v * E.v;
+  if (extrap) {
+    std::vector<const double *> px(ndimr);
+    for (int k = 0; k < ndimr; ++k) px[k] = E.hx[k].p;
+    launch_lincomb(E.X.p, E.dvec.p, E.dev_small.p + 40, px.data(), ndimr, len, E.st);
+  } else {
+    ACES_TRY(E.copy(E.X.p, E.Xn.p, len));
+  }
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+int CCEngine::write_back() {
+  const long long O = o, V = v;
+  const SymInfo &s = state().sym;
+  // T2(AB) -> list 46 (13,14): dense [a,b,i,j] = t2[i,j,a,b]
+  DBuf tmp;
+  ACES_TRY(alloc(tmp, O * O * V * V));
+  const long long st2[4] = {O * V * V, V * V, V, 1};
+  ACES_TRY(perm(tmp.p, v, v, o, o, 0.0, {PT(t2(), 1.0, st2[2], st2[3], st2[0], st2[1])}));
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 46, 13, 14, irr_o, irr_v, true));
+    launch_scatter(tmp.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // T2(AA) -> list 44 (1,3): dense [a,b,i,j] = t2[i,j,a,b] - t2[i,j,b,a]
+  ACES_TRY(perm(tmp.p, v, v, o, o, 0.0,
+                {PT(t2(), 1.0, st2[2], st2[3], st2[0], st2[1]),
+                 PT(t2(), -1.0, st2[3], st2[2], st2[0], st2[1])}));
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 44, 1, 3, irr_o, irr_v, true));
+    launch_scatter(tmp.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // T1 -> list 90 irrep 1, a single column over (a,i) pairs of type 9
+  {
+    int n9 = s.irpdpd[0][8];
+    ACES_TRY(aces_list_touch(1, n9, 1, 90, 0));
+    std::vector<double> h1((size_t)o * v), col((size_t)n9, 0.0);
+    ACES_CUDA(cudaMemcpy(h1.data(), t1(), h1.size() * 8, cudaMemcpyDeviceToHost));
+    std::vector<int> lo(o), lv(v);
+    int cnt[8] = {0};
+    for (int i = 0; i < o; ++i) lo[i] = cnt[irr_o[i]]++;
+    for (int k = 0; k < 8; ++k) cnt[k] = 0;
+    for (int a = 0; a < v; ++a) lv[a] = cnt[irr_v[a]]++;
+    for (int i = 0; i < o; ++i)
+      for (int a = 0; a < v; ++a)
+        if (irr_o[i] == irr_v[a])
+          col[pair_index(s, 9, irr_v[a], lv[a], irr_o[i], lo[i])] = h1[(size_t)i * v + a];
+    ACES_TRY(aces_putlst(col.data(), 1, 1, 1, 90));
+  }
+  cudaFree(tmp.p);
+  return ACES_OK;
+}
+
+static CCEngine *g_engine = nullptr;
+CCEngine *engine_instance(bool create) {
+  if (!g_engine && create) g_engine = new CCEngine();
+  return g_engine;
+}
+void engine_reset() {
+  delete g_engine;
+  g_engine = nullptr;
+}
+
+}  // namespace acesb200
+
+using namespace acesb200;
+
+extern "C" int xvcc_run(aces_cc_config *cfg) {
+  if (!cfg) return ACES_ERR_ARG;
+  State &stt = state();
+  std::lock_guard<std::recursive_mutex> lk(stt.mu);
+  if (cfg->cc_exporder < 1 || cfg->cc_exporder > 25 || cfg->cc_maxcyc < 1) {
+    set_error("xvcc_run: cc_exporder must be 1..25 and cc_maxcyc >= 1");
+    return ACES_ERR_ARG;
+  }
+  if (cfg->precision != ACES_PREC_FP64 && cfg->precision != ACES_PREC_BF16X3) return ACES_ERR_ARG;
+  engine_reset();
+  CCEngine &E = *engine_instance(true);
+  E.prec = cfg->precision;
+  ACES_TRY(E.load_from_lists());
+  ACES_TRY(E.setup_intermediates());
+  ACES_TRY(E.mp2_guess());
+  const double tol = std::pow(10.0, -cfg->cc_conv);
+  cudaEvent_t ev0, ev1;
+  ACES_CUDA(cudaEventCreate(&ev0));
+  ACES_CUDA(cudaEventCreate(&ev1));
+  double e3[3] = {0, 0, 0}, res = 0, dres = 0;
+  bool converged = false;
+  int icycle = 0;
+  float ms_total = 0.f;
+  for (icycle = 1; icycle <= cfg->cc_maxcyc; ++icycle) {
+    bool extrap = false;
+    ACES_CUDA(cudaEventRecord(ev0, E.st));
+    ACES_TRY(E.iteration(icycle, cfg->cc_exporder, e3, &res, &dres, &extrap));
+    int ndimr = icycle < cfg->cc_exporder ? icycle : cfg->cc_exporder;
+    bool conv = std::fabs(res) < tol;
+    if (!conv) ACES_TRY(accept(E, extrap, ndimr));
+    ACES_CUDA(cudaEventRecord(ev1, E.st));
+    ACES_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    ms_total += ms;
+    if (cfg->verbose)
+      printf("  cycle %3d  E(corr) = %.12f  max res = % .8e  max DIIS res = % .8e  %.3f ms\n",
+             icycle, e3[2], res, dres, ms);
+    if (conv) {
+      converged = true;
+      break;
+    }
+  }
+  if (icycle > cfg->cc_maxcyc) icycle = cfg->cc_maxcyc;
+  // final energy of the accepted amplitudes (vcc/vcc.F:1101)
+  double *d = E.dev_small.p;
+  launch_energy(d, E.t2(), E.t1(), E.I_oovv.p, E.fov.p, E.o, E.v, E.scratch.p, E.st);
+  double hd[3];
+  ACES_CUDA(cudaMemcpyAsync(hd, d, 24, cudaMemcpyDeviceToHost, E.st));
+  ACES_CUDA(cudaStreamSynchronize(E.st));
+  cfg->e_ccsd = 2.0 * hd[1] + hd[0] + hd[2];
+  cfg->last_residual = res;
+  cfg->ncycle = icycle;
+  cfg->converged = converged ? 1 : 0;
+  cfg->seconds_per_iter = ms_total * 1e-3 / (icycle > 0 ? icycle : 1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  ACES_TRY(E.write_back());
+  aces_putrec("CCSDENRG", 8, &cfg->e_ccsd);
+  if (!converged) {
+    set_error("CC equations did not converge in %d cycles", cfg->cc_maxcyc);
+    return ACES_ERR_NOCONV;
+  }
+  return ACES_OK;
+}

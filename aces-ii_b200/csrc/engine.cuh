@@ -1,0 +1,86 @@
+// engine.cuh -- the closed-shell CC engine shared by xvcc_run, xlambda_run and
+// xdens_1pdm.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "gemm.cuh"
+#include "kernels.cuh"
+
+namespace acesb200 {
+
+// Dense FP64 device buffer owned by the engine.
+struct DBuf {
+  double *p = nullptr;
+  size_t n = 0;
+};
+
+class CCEngine {
+ public:
+  int o = 0, v = 0, nmo = 0;
+  int prec = ACES_PREC_FP64;
+  cudaStream_t st = 0;
+  bool nonhf = false;
+
+  // orbital data
+  std::vector<double> eps_h;       // nmo, DPD order
+  std::vector<int> irr_o, irr_v;   // orbital irreps
+  DBuf eo, ev, foo, fvv, fov, offo, offv, fovT;
+
+  // integrals (dense, physicists' notation)
+  DBuf I_oooo, I_ooov, I_oovv, I_ovov, I_ovvv, I_vvvv;
+  // precomputed resorted integrals
+  DBuf L_oovv, LF, LovP, LooP, LmeP, I1, I2, IvP, IvP2, IX, IX2, WA0, WB0, IoP3, IvT, IvT2,
+      IooT, LT1;
+
+  // amplitudes: X = [t1 | t2] contiguous
+  DBuf X, Xn, Z1, Z2;
+  double *t1() { return X.p; }
+  double *t2() { return X.p + (size_t)o * v; }
+  double *t1n() { return Xn.p; }
+  double *t2n() { return Xn.p + (size_t)o * v; }
+
+  // temporaries
+  DBuf tau, taut, tautP, tauT, U, Tp, Tpp, uT, wP, t2P, Y1, Y2, XnP, WA, WB, ZT, XP, Xmn, Wmnij,
+      WmnT, t1T, Fae, Fmi, Fme, Fp, Fpp, FmiT, FppT, FmeT, tmp4;
+  DBuf scratch, dev_small;  // reductions / DIIS scalars
+  // DIIS history
+  std::vector<DBuf> hx, he;
+  DBuf Bmat;  // 25x25 on device
+  DBuf dvec;  // DIIS residual sum_i c_i e_i
+  std::vector<double> Bh;  // host copy (kept like /diisdat1/ in vcc/dodiis0.F)
+
+  // split-precision operand cache (constant integrals)
+  struct SplitEntry { const double *src; SplitOperand op; };
+  std::vector<SplitEntry> split_cache;
+  SplitOperand split_tmpA, split_tmpB;
+
+  // statistics
+  long long gemm_calls = 0;
+  double gemm_flops = 0.0;
+
+  ~CCEngine();
+  int alloc(DBuf &b, size_t n);
+  int load_from_lists();
+  int setup_intermediates();
+  int mp2_guess();
+  int residual();   // Z1, Z2 from X
+  int iteration(int icycle, int exporder, double *e_out3, double *res, double *dres,
+                bool *extrap);
+  int write_back();
+  void release();
+
+  // contraction dispatch (FP64 DMMA or BF16x3 tcgen05)
+  int G(int M, int N, int K, double alpha, const double *A, long long lda, const double *B,
+        long long ldb, double beta, const CView &C, bool constA = false, bool constB = false);
+  int perm(double *out, int n0, int n1, int n2, int n3, double beta,
+           std::initializer_list<PermTerm> terms);
+  int copy(double *dst, const double *src, size_t n);
+};
+
+CCEngine *engine_instance(bool create);
+void engine_reset();
+
+}  // namespace acesb200

@@ -1,0 +1,57 @@
+// gemm.cuh -- contraction kernels of the CC engine.
+//
+// Every tensor contraction of the CCSD/(T)/Lambda terms is issued as an
+// "NT" product over K-contiguous operands (the reference's XGEMM calls,
+// tools/xgemm.F:10, after its SSTGEN/SYMTR resorts):
+//
+//   C[m,n] = alpha * sum_k A[m*lda + k] * B[n*ldb + k] + beta * C[m,n]
+//
+// with C addressed through a two-level view so a resorted output can be
+// written in place:
+//   &C[m,n] = p + (m / mdiv)*sm1 + (m % mdiv)*sm0 + (n / ndiv)*sn1 + (n % ndiv)*sn0
+#pragma once
+#include <cuda_runtime.h>
+
+namespace acesb200 {
+
+struct CView {
+  double *p;
+  long long mdiv, sm1, sm0;
+  long long ndiv, sn1, sn0;
+};
+
+// plain row-major C[m*ldc + n]
+inline CView cview_rowmajor(double *p, long long ldc) {
+  return CView{p, 1LL << 62, 0, ldc, 1LL << 62, 0, 1};
+}
+// column-major C[m + n*ldc]
+inline CView cview_colmajor(double *p, long long ldc) {
+  return CView{p, 1LL << 62, 0, 1, 1LL << 62, 0, ldc};
+}
+
+// FP64 tensor-core (DMMA) contraction.
+int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long lda,
+                const double *B, long long ldb, double beta, const CView &C, cudaStream_t st);
+
+// Split-precision operand: x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi),
+// stored K-contiguous and zero-padded to (rows_pad x k_pad).
+struct SplitOperand {
+  void *hi = nullptr;   // __nv_bfloat16[rows_pad * k_pad]
+  void *lo = nullptr;
+  int rows = 0, k = 0, rows_pad = 0, k_pad = 0;
+  size_t bytes() const { return (size_t)rows_pad * k_pad * 2 * 2; }
+};
+
+// rows and K padding of split operands (the tcgen05 kernel's tile sizes)
+constexpr int kSplitRowPad = 128;
+constexpr int kSplitKPad = 64;
+
+// Fill a split operand from an FP64 K-contiguous matrix (src[r*ld + k]).
+int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int k, cudaStream_t st);
+
+// BF16x3 contraction on tcgen05: A, B split operands with equal k_pad.
+// acc = A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (TMEM), C = alpha*acc + beta*C (FP64).
+int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
+                   double beta, const CView &C, cudaStream_t st);
+
+}  // namespace acesb200

@@ -1,0 +1,511 @@
+// kernels.cu -- bandwidth-bound kernels of the CC engine: resorts, FTAU,
+// NEWT2/E4SENG, CMPENG, DIIS reductions, the DIIS solve and DPD gathers.
+#include <cstdio>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace acesb200 {
+
+// ---------------------------------------------------------------------------
+// Resort: generic 4-index permute-accumulate.
+// ---------------------------------------------------------------------------
+struct PermArgs {
+  int n[4];
+  int nterms;
+  const double *src[4];
+  double alpha[4];
+  long long s[4][4];
+  double beta;
+};
+
+__global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int i3 = r % a.n[3]; r /= a.n[3];
+    int i2 = r % a.n[2]; r /= a.n[2];
+    int i1 = r % a.n[1]; r /= a.n[1];
+    int i0 = (int)r;
+    double acc = a.beta == 0.0 ? 0.0 : a.beta * out[idx];
+    for (int t = 0; t < a.nterms; ++t)
+      acc += a.alpha[t] * __ldg(a.src[t] + i0 * a.s[t][0] + i1 * a.s[t][1] + i2 * a.s[t][2] +
+                                i3 * a.s[t][3]);
+    out[idx] = acc;
+  }
+}
+
+// 32x32 shared-memory tiles over (i3, i_d) where every term reads i_d with
+// unit stride: reads coalesced along i_d, writes coalesced along i3.
+template <int D>
+__global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out, PermArgs a) {
+  __shared__ double tile[32][33];
+  const int nd = a.n[D];
+  const int t3 = (a.n[3] + 31) / 32, td = (nd + 31) / 32;
+  long long b = blockIdx.x;
+  int b3 = b % t3; b /= t3;
+  int bd = b % td; b /= td;
+  // remaining two dims (the ones that are neither 3 nor D)
+  int o0 = -1, o1 = -1;
+  for (int k = 0; k < 3; ++k)
+    if (k != D) { if (o0 < 0) o0 = k; else o1 = k; }
+  int io1 = b % a.n[o1];
+  int io0 = (int)(b / a.n[o1]);
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  double acc[4];
+  // output element (i3 = b3*32 + tx, id = bd*32 + ty + 8*k)
+  for (int k = 0; k < 4; ++k) acc[k] = 0.0;
+  for (int t = 0; t < a.nterms; ++t) {
+    __syncthreads();
+    // load: tile[id_local][i3_local] with coalesced id
+    for (int k = 0; k < 4; ++k) {
+      int l3 = ty + 8 * k;        // i3 local
+      int ld = tx;                // id local (unit stride)
+      int i3 = b3 * 32 + l3, id = bd * 32 + ld;
+      double v = 0.0;
+      if (i3 < a.n[3] && id < nd) {
+        long long off = (long long)io0 * a.s[t][o0] + (long long)io1 * a.s[t][o1] +
+                        (long long)i3 * a.s[t][3] + (long long)id * a.s[t][D];
+        v = __ldg(a.src[t] + off);
+      }
+      tile[ld][l3] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < 4; ++k) acc[k] += a.alpha[t] * tile[ty + 8 * k][tx];
+  }
+  for (int k = 0; k < 4; ++k) {
+    int i3 = b3 * 32 + tx, id = bd * 32 + ty + 8 * k;
+    if (i3 < a.n[3] && id < nd) {
+      int idx_[4];
+      idx_[3] = i3; idx_[D] = id; idx_[o0] = io0; idx_[o1] = io1;
+      long long o = (((long long)idx_[0] * a.n[1] + idx_[1]) * a.n[2] + idx_[2]) * a.n[3] + idx_[3];
+      out[o] = (a.beta == 0.0 ? 0.0 : a.beta * out[o]) + acc[k];
+    }
+  }
+}
+
+int permute(double *out, const PermSpec &spec, cudaStream_t st) {
+  PermArgs a;
+  long long total = 1;
+  for (int k = 0; k < 4; ++k) {
+    a.n[k] = spec.n[k];
+    total *= spec.n[k];
+  }
+  if (total == 0) return ACES_OK;
+  a.nterms = spec.nterms;
+  a.beta = spec.beta;
+  for (int t = 0; t < 4; ++t) {
+    a.src[t] = t < spec.nterms ? spec.t[t].src : nullptr;
+    a.alpha[t] = t < spec.nterms ? spec.t[t].alpha : 0.0;
+    for (int k = 0; k < 4; ++k) a.s[t][k] = t < spec.nterms ? spec.t[t].s[k] : 0;
+  }
+  // tiled path when the innermost output index is strided in every source and
+  // some other index has unit stride in all of them
+  int D = -1;
+  bool all_unit3 = true;
+  for (int t = 0; t < spec.nterms; ++t)
+    if (a.s[t][3] != 1) all_unit3 = false;
+  if (!all_unit3) {
+    for (int d = 0; d < 3 && D < 0; ++d) {
+      bool ok = true;
+      for (int t = 0; t < spec.nterms; ++t)
+        if (a.s[t][d] != 1) ok = false;
+      if (ok && a.n[d] >= 8) D = d;
+    }
+  }
+  if (D >= 0 && a.n[3] >= 8) {
+    long long nb = (long long)((a.n[3] + 31) / 32) * ((a.n[D] + 31) / 32);
+    for (int k = 0; k < 3; ++k)
+      if (k != D) nb *= a.n[k];
+    dim3 blk(32, 8);
+    if (D == 0) k_permute_tiled<0><<<(unsigned)nb, blk, 0, st>>>(out, a);
+    if (D == 1) k_permute_tiled<1><<<(unsigned)nb, blk, 0, st>>>(out, a);
+    if (D == 2) k_permute_tiled<2><<<(unsigned)nb, blk, 0, st>>>(out, a);
+  } else {
+    long long nb = (total + 255) / 256;
+    if (nb > 148 * 64) nb = 148 * 64;
+    k_permute_naive<<<(unsigned)nb, 256, 0, st>>>(out, a, total);
+  }
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise
+// ---------------------------------------------------------------------------
+__global__ void k_tau(double *__restrict__ tau, const double *__restrict__ t2,
+                      const double *__restrict__ t1, double c, int o, int v, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int b = r % v; r /= v;
+    int a = r % v; r /= v;
+    int j = r % o;
+    int i = (int)(r / o);
+    tau[idx] = t2[idx] + c * t1[i * v + a] * t1[j * v + b];
+  }
+}
+
+void launch_tau(double *tau, const double *t2, const double *t1, double c, int o, int v,
+                cudaStream_t st) {
+  long long total = (long long)o * o * v * v;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total);
+}
+
+__global__ void k_newt(double *__restrict__ t2n, const double *__restrict__ z2,
+                       double *__restrict__ t1n, const double *__restrict__ z1,
+                       const double *__restrict__ eo, const double *__restrict__ ev, int o, int v,
+                       long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int b = r % v; r /= v;
+    int a = r % v; r /= v;
+    int j = r % o;
+    int i = (int)(r / o);
+    long long tidx = (((long long)j * o + i) * v + b) * v + a;
+    double z = 0.5 * (z2[idx] + z2[tidx]);
+    t2n[idx] = z / (eo[i] + eo[j] - ev[a] - ev[b]);
+    if (idx < (long long)o * v) {
+      int ii = (int)(idx / v), aa = (int)(idx % v);
+      t1n[idx] = z1[idx] / (eo[ii] - ev[aa]);
+    }
+  }
+}
+
+void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, const double *eo,
+                 const double *ev, int o, int v, cudaStream_t st) {
+  long long total = (long long)o * o * v * v;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_newt<<<(unsigned)nb, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, total);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reductions (deterministic two-pass)
+// ---------------------------------------------------------------------------
+constexpr int kRedBlocks = 592;  // 4 per SM
+
+template <int N>
+__device__ void block_reduce(double (&vals)[N], double *out) {
+  __shared__ double sh[N][32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 0; k < N; ++k) {
+    double x = vals[k];
+    for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+    if (lane == 0) sh[k][wid] = x;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    for (int k = 0; k < N; ++k) {
+      double x = lane < nw ? sh[k][lane] : 0.0;
+      for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+      if (lane == 0) out[k] = x;
+    }
+  }
+}
+
+__global__ void k_energy(double *__restrict__ part, const double *__restrict__ t2,
+                         const double *__restrict__ t1, const double *__restrict__ V,
+                         const double *__restrict__ fov, int o, int v, long long total) {
+  double s[3] = {0.0, 0.0, 0.0};
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int b = r % v; r /= v;
+    int a = r % v; r /= v;
+    int j = r % o;
+    int i = (int)(r / o);
+    double tau = t2[idx] + t1[i * v + a] * t1[j * v + b];
+    double vij = V[idx];
+    double vji = V[idx - (long long)b - (long long)a * v + (long long)a + (long long)b * v];
+    s[0] += tau * vij;
+    s[1] += 0.5 * tau * (vij - vji);
+    if (idx < (long long)o * v) s[2] += 2.0 * fov[idx] * t1[idx];
+  }
+  block_reduce<3>(s, part + 3 * blockIdx.x);
+}
+
+__global__ void k_final_sum(double *out, const double *part, int nblk, int nv) {
+  // single warp per value, fixed order
+  int k = blockIdx.x;
+  double x = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += 32) x += part[(long long)b * nv + k];
+  for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+  if (threadIdx.x == 0) out[k] = x;
+}
+
+void launch_energy(double *out3, const double *t2, const double *t1, const double *voovv,
+                   const double *fov, int o, int v, double *scratch, cudaStream_t st) {
+  long long total = (long long)o * o * v * v;
+  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total);
+  k_final_sum<<<3, 32, 0, st>>>(out3, scratch, kRedBlocks, 3);
+}
+
+__global__ void k_diff(double *e, const double *a, const double *b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    e[i] = a[i] - b[i];
+}
+
+void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st) {
+  long long nb = (n + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_diff<<<(unsigned)nb, 256, 0, st>>>(e, xnew, xold, n);
+}
+
+struct HistPtrs {
+  const double *p[25];
+};
+
+// dots of e with hist[k] over T1, T2(AB) and packed T2(AA) (i<j, a<b)
+__global__ void k_diis_dots(double *__restrict__ part, const double *__restrict__ e, HistPtrs h,
+                            int nh, int o, int v) {
+  double s[25];
+  for (int k = 0; k < 25; ++k) s[k] = 0.0;
+  const long long n1 = (long long)o * v;
+  const long long n2 = (long long)o * o * v * v;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
+       idx += (long long)gridDim.x * blockDim.x) {
+    double x = e[idx];
+    bool aa = false;
+    long long tix = 0;
+    if (idx >= n1) {
+      long long r = idx - n1;
+      int b = r % v; r /= v;
+      int a = r % v; r /= v;
+      int j = r % o;
+      int i = (int)(r / o);
+      if (i < j && a < b) {
+        aa = true;
+        tix = idx + (long long)(b - a) * v + (a - b);  // (i,j,b,a)
+      }
+    }
+    double xa = aa ? x - e[tix] : 0.0;
+    for (int k = 0; k < nh; ++k) {
+      double y = h.p[k][idx];
+      double acc = x * y;
+      if (aa) acc += xa * (y - h.p[k][tix]);
+      s[k] += acc;
+    }
+  }
+  // reduce 25 values
+  __shared__ double sh[25][8];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 0; k < nh; ++k) {
+    double x = s[k];
+    for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+    if (lane == 0) sh[k][wid] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < nh) {
+    double x = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+    part[(long long)blockIdx.x * 25 + threadIdx.x] = x;
+  }
+}
+
+int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
+                     int o, int v, double *scratch, cudaStream_t st) {
+  if (nh < 1 || nh > 25) return ACES_ERR_ARG;
+  HistPtrs h;
+  for (int k = 0; k < 25; ++k) h.p[k] = k < nh ? hist[k] : nullptr;
+  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v);
+  k_final_sum<<<nh, 32, 0, st>>>(dots_out, scratch, kRedBlocks, 25);
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+// signed absmax; ties resolved towards the lower index (ISAMAX)
+__device__ inline void amax_merge(double &bv, long long &bi, double v, long long i) {
+  if (fabs(v) > fabs(bv) || (fabs(v) == fabs(bv) && i < bi)) {
+    bv = v;
+    bi = i;
+  }
+}
+
+__global__ void k_absmax(double *__restrict__ pv, long long *__restrict__ pi,
+                         const double *__restrict__ x, int o, int v) {
+  const long long n1 = (long long)o * v;
+  const long long n2 = (long long)o * o * v * v;
+  double bv = 0.0;
+  long long bi = 0x7fffffffffffffffLL;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
+       idx += (long long)gridDim.x * blockDim.x) {
+    amax_merge(bv, bi, x[idx], idx);
+    if (idx >= n1) {
+      long long r = idx - n1;
+      int b = r % v; r /= v;
+      int a = r % v; r /= v;
+      int j = r % o;
+      int i = (int)(r / o);
+      if (i < j && a < b) {
+        long long tix = idx + (long long)(b - a) * v + (a - b);
+        amax_merge(bv, bi, x[idx] - x[tix], n1 + n2 + idx);
+      }
+    }
+  }
+  for (int off = 16; off; off >>= 1) {
+    double ov = __shfl_down_sync(0xffffffff, bv, off);
+    long long oi = __shfl_down_sync(0xffffffff, bi, off);
+    amax_merge(bv, bi, ov, oi);
+  }
+  __shared__ double sv[8];
+  __shared__ long long si[8];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sv[wid] = bv; si[wid] = bi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax_merge(bv, bi, sv[w], si[w]);
+    pv[blockIdx.x] = bv;
+    pi[blockIdx.x] = bi;
+  }
+}
+
+__global__ void k_absmax_final(double *out, const double *pv, const long long *pi, int nb) {
+  double bv = 0.0;
+  long long bi = 0x7fffffffffffffffLL;
+  for (int b = 0; b < nb; ++b) amax_merge(bv, bi, pv[b], pi[b]);
+  out[0] = bv;
+}
+
+void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st) {
+  double *pv = scratch;
+  long long *pi = (long long *)(scratch + kRedBlocks);
+  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v);
+  k_absmax_final<<<1, 1, 0, st>>>(out, pv, pi, kRedBlocks);
+}
+
+// Bordered DIIS system [[0,-1..],[-1,B]] (lam,c) = (-1,0,..) by LU with
+// partial pivoting (the pivot order of LAPACK dgetf2, libr/dodiis.F:46).
+__global__ void k_diis_solve(double *coef, int *status, const double *B, int n) {
+  if (threadIdx.x != 0) return;
+  double A[26][26];
+  double rhs[26];
+  int N = n + 1;
+  for (int i = 0; i < N; ++i) {
+    rhs[i] = i == 0 ? -1.0 : 0.0;
+    for (int j = 0; j < N; ++j) {
+      if (i == 0 && j == 0) A[i][j] = 0.0;
+      else if (i == 0 || j == 0) A[i][j] = -1.0;
+      else A[i][j] = B[(i - 1) * 25 + (j - 1)];
+    }
+  }
+  int st = 0;
+  for (int k = 0; k < N; ++k) {
+    int p = k;
+    double m = fabs(A[k][k]);
+    for (int i = k + 1; i < N; ++i)
+      if (fabs(A[i][k]) > m) { m = fabs(A[i][k]); p = i; }
+    if (m == 0.0) { st = 1; break; }
+    if (p != k) {
+      for (int j = 0; j < N; ++j) { double t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t; }
+      double t = rhs[k]; rhs[k] = rhs[p]; rhs[p] = t;
+    }
+    double inv = 1.0 / A[k][k];
+    for (int i = k + 1; i < N; ++i) {
+      double l = A[i][k] * inv;
+      A[i][k] = l;
+      for (int j = k + 1; j < N; ++j) A[i][j] -= l * A[k][j];
+      rhs[i] -= l * rhs[k];
+    }
+  }
+  if (!st) {
+    for (int i = N - 1; i >= 0; --i) {
+      double x = rhs[i];
+      for (int j = i + 1; j < N; ++j) x -= A[i][j] * rhs[j];
+      rhs[i] = x / A[i][i];
+    }
+    for (int i = 0; i < n; ++i) coef[i] = rhs[i + 1];
+  }
+  status[0] = st;
+}
+
+void launch_diis_solve(double *coef_out, int *status_out, const double *B, int n, cudaStream_t st) {
+  k_diis_solve<<<1, 32, 0, st>>>(coef_out, status_out, B, n);
+}
+
+__global__ void k_lincomb(double *__restrict__ out, const double *__restrict__ base,
+                          const double *__restrict__ c, HistPtrs p, int n, long long len) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = base ? base[i] : 0.0;
+    for (int k = 0; k < n; ++k) acc += c[k] * p.p[k][i];
+    out[i] = acc;
+  }
+}
+
+void launch_lincomb(double *out, const double *base, const double *c, const double *const *p,
+                    int n, long long len, cudaStream_t st) {
+  HistPtrs a;
+  for (int k = 0; k < 25; ++k) a.p[k] = k < n ? p[k] : nullptr;
+  long long nb = (len + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_lincomb<<<(unsigned)nb, 256, 0, st>>>(out, base, c, a, n, len);
+}
+
+// ---------------------------------------------------------------------------
+// DPD list <-> dense
+// ---------------------------------------------------------------------------
+__global__ void k_gather(double *__restrict__ dense, DpdMap m, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int s = r % m.ns; r /= m.ns;
+    int q2 = r % m.nr; r /= m.nr;
+    int q = r % m.nq;
+    int p = (int)(r / m.nq);
+    int hpq = m.irr_p[p] ^ m.irr_q[q];
+    int hrs = m.irr_r[q2] ^ m.irr_s[s];
+    double val = 0.0;
+    if (hpq == hrs) {
+      int ri = m.rowidx[p * m.nq + q], ci = m.colidx[q2 * m.ns + s];
+      if (ri >= 0 && ci >= 0) {
+        int a = m.rowsgn[p * m.nq + q], b = m.colsgn[q2 * m.ns + s];
+        double sg = (double)(a == 2 ? 1 : a) * (double)(b == 2 ? 1 : b);
+        val = sg * m.base[hrs][(long long)ci * m.nrows[hrs] + ri];
+      }
+    }
+    dense[idx] = val;
+  }
+}
+
+__global__ void k_scatter(const double *__restrict__ dense, DpdMap m, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    int s = r % m.ns; r /= m.ns;
+    int q2 = r % m.nr; r /= m.nr;
+    int q = r % m.nq;
+    int p = (int)(r / m.nq);
+    int hpq = m.irr_p[p] ^ m.irr_q[q];
+    int hrs = m.irr_r[q2] ^ m.irr_s[s];
+    if (hpq != hrs) continue;
+    int ri = m.rowidx[p * m.nq + q], ci = m.colidx[q2 * m.ns + s];
+    // write only the canonical (positive-sign) representative of packed pairs
+    if (ri < 0 || ci < 0) continue;
+    if (m.rowsgn[p * m.nq + q] != 1 || m.colsgn[q2 * m.ns + s] != 1) continue;
+    m.base[hrs][(long long)ci * m.nrows[hrs] + ri] = dense[idx];
+  }
+}
+
+void launch_gather(double *dense, const DpdMap &m, cudaStream_t st) {
+  long long total = (long long)m.np * m.nq * m.nr * m.ns;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  if (nb < 1) nb = 1;
+  k_gather<<<(unsigned)nb, 256, 0, st>>>(dense, m, total);
+}
+
+void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st) {
+  long long total = (long long)m.np * m.nq * m.nr * m.ns;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  if (nb < 1) nb = 1;
+  k_scatter<<<(unsigned)nb, 256, 0, st>>>(dense, m, total);
+}
+
+}  // namespace acesb200

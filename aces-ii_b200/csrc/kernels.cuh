@@ -1,0 +1,75 @@
+// kernels.cuh -- launchers of the bandwidth-bound kernels of the CC engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace acesb200 {
+
+// ---- resorts ---------------------------------------------------------------
+// out[i0,i1,i2,i3] (C order, dims n[0..3]) = beta*out + sum_t alpha[t] *
+// in_t[i0*s[t][0] + i1*s[t][1] + i2*s[t][2] + i3*s[t][3]]   (up to 4 terms).
+// The index permutations between contractions (libr/sstgen.f, sst02i.f,
+// symtr1.F, symrhf.f, spinad1.f, transp.f) are all instances.
+struct PermTerm {
+  const double *src;
+  double alpha;
+  long long s[4];
+};
+struct PermSpec {
+  int n[4];
+  int nterms;
+  PermTerm t[4];
+  double beta;
+};
+int permute(double *out, const PermSpec &spec, cudaStream_t st);
+
+// ---- elementwise -----------------------------------------------------------
+// tau = t2 + c * t1[i,a] t1[j,b] over [o,o,v,v] (libr/ftau.f)
+void launch_tau(double *tau, const double *t2, const double *t1, double c, int o, int v,
+                cudaStream_t st);
+// t_new = z / (e_i + e_j - e_a - e_b) (libr2/newt2.F) and t1 = z1/(e_i-e_a) (vcc/e4seng.F);
+// z2 is symmetrised in place first (vcc/dodiis0.F SYMETRIZE_T2).
+void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, const double *eo,
+                 const double *ev, int o, int v, cudaStream_t st);
+
+// ---- reductions (FP64) --------------------------------------------------------
+// partial sums for E_AB = sum tau*V and E_AA' = sum tau*(V - V^T(ab)); out[0..1]
+void launch_energy(double *out2, const double *t2, const double *t1, const double *voovv,
+                   const double *fov, int o, int v, double *scratch, cudaStream_t st);
+
+// DIIS: error e = x_new - x_old over [t1 | t2]; writes e, the signed absmax of
+// e over T1, T2(AB) and packed T2(AA) into absmax_out, and dots of e with the
+// n stored error vectors (including e itself when stored) into dots_out.
+int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
+                     int o, int v, double *scratch, cudaStream_t st);
+void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st);
+// signed absmax over [t1 | t2 | packed AA(t2)]
+void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st);
+// solve the bordered DIIS system for n <= 25 on the device (libr/dodiis.F);
+// B is 25x25 row-major, coef_out[0..n-1]; status_out[0] = 0 ok / 1 singular
+void launch_diis_solve(double *coef_out, int *status_out, const double *B, int n, cudaStream_t st);
+// out = base + sum_k c[k] * p[k]  (base may be null); with p = stored errors
+// this is the DIIS residual, with base = that residual and p = stored iterates
+// it is the extrapolated amplitude vector (vcc/dodiis0.F:188-243)
+void launch_lincomb(double *out, const double *base, const double *c, const double *const *p,
+                    int n, long long len, cudaStream_t st);
+
+// ---- DPD list <-> dense ------------------------------------------------------
+// dense[p,q,r,s] for p<np,q<nq,r<nr,s<ns gathered from a list with the given
+// row/col pair-index tables (pair index within block, -1 = not stored; sign
+// table for antisymmetric packed types), block base pointers and row counts by
+// column irrep.
+struct DpdMap {
+  const int *rowidx;   // [np*nq] pair index of (p,q) or -1
+  const int *colidx;   // [nr*ns]
+  const signed char *rowsgn;  // [np*nq] +1/-1/0
+  const signed char *colsgn;  // [nr*ns]
+  const int *irr_p, *irr_q, *irr_r, *irr_s;  // orbital irreps
+  double *const *base;  // per column irrep (device array of pointers)
+  const int *nrows;     // per column irrep
+  int np, nq, nr, ns;
+};
+void launch_gather(double *dense, const DpdMap &m, cudaStream_t st);
+void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st);
+
+}  // namespace acesb200

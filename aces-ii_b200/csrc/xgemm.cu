@@ -1,0 +1,78 @@
+// xgemm.cu -- the reference's XGEMM boundary (tools/xgemm.F:10-49) on device
+// pointers, routed to the engine's contraction kernels.
+#include <cctype>
+
+#include "common.cuh"
+#include "gemm.cuh"
+#include "kernels.cuh"
+
+using namespace acesb200;
+
+namespace {
+// dst[r*cols + c] = src[r + c*ld]: column-major (rows x cols) -> row-major
+int to_kmajor(double **dst, const double *src, int rows, int cols, long long ld,
+              cudaStream_t st) {
+  ACES_CUDA(cudaMalloc(dst, (size_t)rows * cols * 8 + 8));
+  PermSpec s;
+  s.n[0] = 1; s.n[1] = 1; s.n[2] = rows; s.n[3] = cols;
+  s.nterms = 1;
+  s.beta = 0.0;
+  s.t[0].src = src;
+  s.t[0].alpha = 1.0;
+  s.t[0].s[0] = 0; s.t[0].s[1] = 0; s.t[0].s[2] = 1; s.t[0].s[3] = ld;
+  return permute(*dst, s, st);
+}
+}  // namespace
+
+extern "C" int aces_xgemm(char transa, char transb, int m, int n, int k, double alpha,
+                          const double *A, int lda, const double *B, int ldb, double beta,
+                          double *Cm, int ldc, int precision) {
+  char ta = (char)toupper(transa), tb = (char)toupper(transb);
+  if ((ta != 'N' && ta != 'T') || (tb != 'N' && tb != 'T') || m < 0 || n < 0 || k < 0) {
+    set_error("aces_xgemm: bad arguments");
+    return ACES_ERR_ARG;
+  }
+  if ((long long)m * n == 0) return ACES_OK;  // quick return (tools/xgemm.F)
+  if (ldc < (m > 1 ? m : 1)) {
+    set_error("aces_xgemm: ldc < m");
+    return ACES_ERR_ARG;
+  }
+  cudaStream_t st = 0;
+  // NT form: Ak[i*K + l] = op(A)(i,l), Bk[j*K + l] = op(B)(l,j)
+  const double *Ak = A, *Bk = B;
+  long long ldak = lda, ldbk = ldb;
+  double *tA = nullptr, *tB = nullptr;
+  int status = ACES_OK;
+  if (ta == 'N') {  // op(A)(i,l) = A[i + l*lda]
+    status = to_kmajor(&tA, A, m, k, lda, st);
+    Ak = tA;
+    ldak = k;
+  }
+  if (status == ACES_OK && tb == 'T') {  // op(B)(l,j) = B[j + l*ldb]
+    status = to_kmajor(&tB, B, n, k, ldb, st);
+    Bk = tB;
+    ldbk = k;
+  }
+  if (status == ACES_OK) {
+    CView C = cview_colmajor(Cm, ldc);
+    if (precision == ACES_PREC_BF16X3 && k > 0) {
+      SplitOperand sa, sb;
+      status = split_pack(sa, Ak, ldak, m, k, st);
+      if (status == ACES_OK) status = split_pack(sb, Bk, ldbk, n, k, st);
+      if (status == ACES_OK) status = gemm_nt_bf16x3(sa, sb, m, n, alpha, beta, C, st);
+      cudaStreamSynchronize(st);
+      if (sa.hi) cudaFree(sa.hi);
+      if (sb.hi) cudaFree(sb.hi);
+    } else {
+      status = gemm_nt_f64(m, n, k, alpha, Ak, ldak, Bk, ldbk, beta, C, st);
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (tA) cudaFree(tA);
+  if (tB) cudaFree(tB);
+  if (status == ACES_OK && e != cudaSuccess) {
+    set_error("aces_xgemm: %s", cudaGetErrorString(e));
+    status = ACES_ERR_CUDA;
+  }
+  return status;
+}

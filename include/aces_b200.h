@@ -1,0 +1,182 @@
+/*
+ * aces_b200.h -- C-ABI of the B200 coupled-cluster engine (CCSD / (T) / Lambda).
+ *
+ * The entry points mirror the reference's list/record interface and member
+ * programs so that a Fortran or C host can bind them one-for-one.  Every
+ * function returns an int status (ACES_OK = 0, negative on error) where the
+ * reference calls aces_exit(); no function terminates the process.
+ *
+ * Conventions shared with the reference:
+ *   - irreps, list ids and column indices are 1-based (Fortran style);
+ *   - a list is a set of 2-D column-major arrays, one per irrep; column c of
+ *     irrep h holds nrows(h) doubles (acescore/aces_list_touch.F);
+ *   - pair types 1..25 and their packing (PACK a<b, PCK2 a<=b, FULL) follow
+ *     acescore/aces_com_symloc.F; IRPDPD(irrep,type) follows
+ *     acescore/aces_com_sympop.F; DIRPRD is the XOR product of 0-based irreps.
+ *   - all list data live in device memory (one arena per process); the plain
+ *     GETLST/PUTLST entry points stage through host memory like the
+ *     reference's file I/O, the *_dev variants copy device-to-device.
+ */
+#ifndef ACES_B200_H
+#define ACES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+enum {
+  ACES_OK = 0,
+  ACES_ERR_ARG = -1,        /* invalid argument (bad irrep, list, bounds)      */
+  ACES_ERR_NOLIST = -2,     /* list/irrep not touched                          */
+  ACES_ERR_REDIM = -3,      /* re-touch with different dims (aces_list_touch.F:83) */
+  ACES_ERR_CUDA = -4,       /* CUDA runtime error                              */
+  ACES_ERR_NOMEM = -5,      /* device allocation failed (INSMEM)               */
+  ACES_ERR_NOREC = -6,      /* JOBARC record absent (getrec.F)                 */
+  ACES_ERR_NOSYM = -7,      /* symmetry not initialised                        */
+  ACES_ERR_SINGULAR = -8,   /* DIIS bordered system singular (libr/dodiis.F:49) */
+  ACES_ERR_NOCONV = -9,     /* CC equations did not converge (vcc/vcc.F:1439)  */
+  ACES_ERR_NAN = -10,       /* non-finite amplitudes or energy                 */
+  ACES_ERR_TIMEOUT = -11,   /* a bounded device wait gave up                   */
+  ACES_ERR_UNSUPPORTED = -12
+};
+
+/* ---- runtime ---------------------------------------------------------- */
+
+/* aces_init (acescore/aces_init.F): select the CUDA device, reset lists and
+ * records.  Safe to call again (re-initialises). */
+int aces_init(int device);
+/* aces_fin (acescore/aces_fin.F): free every list and record. */
+int aces_fin(void);
+/* Last error message (static storage). */
+const char *aces_last_error(void);
+
+/* ---- symmetry / DPD metadata ------------------------------------------- */
+
+/* Replaces the JOBARC-driven set-up of /SYMINF/, /SYM/, /SYMPOP/ and
+ * /SYMLOC/ (acescore/aces_com_syminf.F, aces_com_sym.F, aces_com_sympop.F,
+ * aces_com_symloc.F) for a closed-shell (RHF) reference: pop[h] occupied and
+ * vrt[h] virtual orbitals per irrep, h = 0..nirrep-1, alpha = beta. */
+int aces_sym_init(int nirrep, const int *pop, const int *vrt);
+/* IRPDPD(irrep, type): number of pairs of pair type `type` (1..22) whose
+ * product irrep is `irrep` (include/sympop.com). */
+int aces_irpdpd(int irrep, int type);
+/* ISYMOFF(irrep_q, irrep_pq, type): 1-based offset of the (irrep_p, irrep_q)
+ * block inside the pairs of total irrep irrep_pq (include/symloc.com). */
+int aces_isymoff(int irrep_q, int irrep_pq, int type);
+/* DIRPRD(i, j) (include/syminf.com). */
+int aces_dirprd(int i, int j);
+
+/* ---- lists (MOINTS / GAMLAM files) -------------------------------------- */
+
+/* ACES_LIST_TOUCH (acescore/aces_list_touch.F:24): create list `list`, irrep
+ * `irrep` with nrows x ncols doubles, zero-filled.  Re-touching with the same
+ * dims is a no-op; different dims return ACES_ERR_REDIM. */
+int aces_list_touch(int ncols, int nrows, int irrep, int list, int nofrag);
+/* UPDMOI (libr/updmoi.F:11): same as aces_list_touch. */
+int aces_updmoi(int ncols, int nrows, int irrep, int list, int iarg1, int iarg2);
+/* INIPCK (libr/inipck.F:4): touch every irrep of `list` with rows of pair type
+ * sytypl (irrep DIRPRD(irrepr, irrepx)) and columns of pair type sytypr
+ * (irrep irrepr); with iset != 0 record ISYTYP(1:2, list). */
+int aces_inipck(int irrepx, int sytypl, int sytypr, int list, int iset);
+/* ISYTYP(1|2, list). */
+int aces_isytyp(int which, int list);
+/* Dimensions of one list irrep (0 rows/cols when untouched). */
+int aces_list_dims(int irrep, int list, int *ncols, int *nrows);
+/* GETLST (acescore/getlst.F:19): copy columns first..first+ncols-1 of
+ * (irrep, list) into host memory `dst` (column-major). */
+int aces_getlst(double *dst, int first, int ncols, int irrep, int list);
+/* PUTLST (acescore/putlst.F:19): the mirror of GETLST. */
+int aces_putlst(const double *src, int first, int ncols, int irrep, int list);
+/* Device-pointer variants (stream 0 ordered, asynchronous w.r.t. the host). */
+int aces_getlst_dev(double *dst, int first, int ncols, int irrep, int list);
+int aces_putlst_dev(const double *src, int first, int ncols, int irrep, int list);
+/* GETALL / PUTALL (acesutil/getall.F, acesutil/putall.f): all irreps
+ * r = 1..nirrep of a list whose column irrep is r, concatenated; `len` is the
+ * expected total length in doubles (checked). */
+int aces_getall(double *dst, long long len, int irrepx, int list);
+int aces_putall(const double *src, long long len, int irrepx, int list);
+/* ACES_LIST_MEMSET (acescore/aces_list_memset.F): byte fill of one irrep. */
+int aces_list_memset(int irrep, int list, int byte);
+/* Device address of (irrep, list) column 1, or NULL. */
+double *aces_list_devptr(int irrep, int list);
+
+/* ---- records (JOBARC) --------------------------------------------------- */
+
+/* PUTREC / GETREC (acescore/putrec.F, acescore/getrec.F): named byte
+ * vectors.  getrec fails with ACES_ERR_NOREC when absent and ACES_ERR_ARG when
+ * nbytes exceeds the stored length. */
+int aces_putrec(const char *label, long long nbytes, const void *buf);
+int aces_getrec(const char *label, long long nbytes, void *buf);
+long long aces_reclen(const char *label);
+
+/* ---- BLAS boundary ------------------------------------------------------ */
+
+/* XGEMM (tools/xgemm.F:10-49, crust/xgemm.F:10-51): column-major
+ * C = alpha * op(A) op(B) + beta * C on DEVICE pointers, op = 'N' or 'T'
+ * (case-insensitive); quick return when m*n == 0.  `precision` selects the
+ * FP64 DMMA kernel or the BF16x3 tcgen05 kernel (ACES_PREC_*).  Synchronous. */
+int aces_xgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+               int lda, const double *B, int ldb, double beta, double *Cmat, int ldc,
+               int precision);
+
+/* ---- member programs ---------------------------------------------------- */
+
+/* Precision of the tensor contractions. */
+enum {
+  ACES_PREC_FP64 = 0,      /* FP64 everywhere (the plain GPU path)            */
+  ACES_PREC_BF16X3 = 1     /* split BF16x3 tcgen05 products, FP32 accumulate,
+                              FP64 denominators / DIIS / energies / norms     */
+};
+
+/* Job parameters: the IFLAGS fields the CC programs read (include/flags.h).
+ * Inputs are the lists and records named at each entry point below;
+ * outputs are written back to lists 46/44 (T2), 90 (T1) and records. */
+typedef struct aces_cc_config {
+  int cc_conv;        /* IFLAGS(4): converge when max |dT| < 10^-cc_conv     */
+  int cc_maxcyc;      /* IFLAGS(7)                                           */
+  int cc_exporder;    /* IFLAGS(12): DIIS subspace (<= 25)                   */
+  int precision;      /* ACES_PREC_*                                         */
+  int triples;        /* 1: run (T) after CCSD (CALC=CCSD(T))                */
+  int use_graph;      /* 1: capture one iteration in a CUDA graph             */
+  int verbose;        /* 1: per-iteration log on stdout (IFLAGS(1))          */
+  int reserved;
+  /* outputs */
+  double e_ccsd;      /* correlation energy of the final amplitudes          */
+  double e_t4;        /* E[4]T                                               */
+  double e_st5;       /* E[5]ST                                              */
+  double last_residual;
+  int ncycle;
+  int converged;
+  double seconds_per_iter;  /* device time per CCSD iteration (CUDA events)  */
+  double seconds_triples;
+} aces_cc_config;
+
+/* PROGRAM VCC (vcc/vcc.F:9): RHF CCSD (and (T) when cfg->triples).  Reads
+ * lists 13, 10, 16, 25, 30, 233 and records SCFEVALA (orbital energies, DPD
+ * order) plus, for a non-Hartree-Fock Fock matrix, record FOCKMAT; writes T1
+ * to list 90 (irrep 1), T2(AB) to list 46, T2(AA) to list 44 and record
+ * TOTENERG-style records CCSDENRG, E4T, E5ST. */
+int xvcc_run(aces_cc_config *cfg);
+
+/* PROGRAM VLAMCC (lambda/vlamcc.F): Lambda equations for the amplitudes left
+ * by xvcc_run; writes L1 to list 190 (irrep 1) and L2(AB) to list 146. */
+int xlambda_run(aces_cc_config *cfg);
+
+/* DENSOO/DENSVV/DENSVO (dens/densoo.F, densvv.F, densvo.F): the CCSD
+ * one-particle density from T and Lambda, written to record DENSMAT (nmo x
+ * nmo, DPD orbital order, row-major). */
+int xdens_1pdm(aces_cc_config *cfg);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACES_B200_H */

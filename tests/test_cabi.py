@@ -1,0 +1,87 @@
+"""CPU tests of the C-ABI library: it loads, exports every symbol declared in
+include/aces_b200.h, and its DPD metadata reproduces the reference's layout
+(acescore/aces_com_symloc.F, aces_com_sympop.F) -- no GPU needed."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import acesb200 as ab
+from acesb200.dpd import DPD, pair_kind
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return ab.load()
+
+
+def test_exports_match_header(lib):
+    hdr = open(os.path.join(ROOT, "include", "aces_b200.h")).read()
+    declared = set(re.findall(r"^\s*(?:const char \*|double \*|long long |int )(\w+)\(", hdr, re.M))
+    assert declared == set(ab.SYMBOLS)
+    for name in declared:
+        assert hasattr(lib.h, name), name
+
+
+def test_dpd_counts_h2o(lib):
+    # H2O/DZP C2v populations of out.zmat.035.ccsd; the reference prints
+    # "Norm of T2AB vector (3087 symmetry allowed elements)" and
+    # "Norm of T1AA vector (39 symmetry allowed elements)"
+    lib.sym_init([3, 1, 1, 0], [10, 3, 6, 2])
+    n_t2ab = sum(lib.irpdpd(h, 13) * lib.irpdpd(h, 14) for h in range(1, 5))
+    assert n_t2ab == 3087
+    assert lib.irpdpd(1, 9) == 39
+    # a<b / i<j packed (types 1, 3) and a<=b (type 5)
+    vrt = np.array([10, 3, 6, 2])
+    assert lib.irpdpd(1, 1) == sum(n * (n - 1) // 2 for n in vrt)
+    assert lib.irpdpd(1, 5) == sum(n * (n + 1) // 2 for n in vrt)
+    assert lib.irpdpd(2, 13) == 2 * (10 * 3 + 6 * 2)
+    assert ab.load().h.aces_dirprd(2, 3) == 4
+
+
+def test_isymoff_offsets_h2o(lib):
+    lib.sym_init([3, 1, 1, 0], [10, 3, 6, 2])
+    # total irrep 2 (B2), FULL (a,b): blocks ordered by irrep of b
+    vrt = [10, 3, 6, 2]
+    off = 1
+    for hq in range(4):
+        hp = hq ^ 1
+        assert lib.isymoff(hq + 1, 2, 13) == off
+        off += vrt[hp] * vrt[hq]
+
+
+def test_dpd_tables_cover_every_pair_once(lib):
+    lib.sym_init([2, 1, 0, 1], [4, 2, 3, 1])
+    irr_o = [0, 0, 1, 3]
+    irr_v = [0, 0, 0, 0, 1, 1, 2, 2, 2, 3]
+    d = DPD(lib, irr_o, irr_v)
+    for t in (1, 3, 5, 9, 11, 13, 14, 18):
+        idx, sgn, hpq = d.table(t)
+        for h in range(4):
+            stored = idx[(hpq == h) & (sgn == 1)]
+            n = lib.irpdpd(h + 1, t)
+            assert sorted(stored.tolist()) == list(range(n)), (t, h)
+        if pair_kind(t)[2] == 1:   # a<b: diagonal pairs are not stored
+            assert np.all(sgn[np.eye(*sgn.shape, dtype=bool)] == 0)
+
+
+def test_records_roundtrip_host_only(lib):
+    x = np.arange(7, dtype=np.float64) * 0.5
+    lib.putrec("TESTREC", x)
+    np.testing.assert_array_equal(lib.getrec("TESTREC", 7), x)
+    assert lib.h.aces_reclen(b"TESTREC") == 56
+    with pytest.raises(ab.AcesError):
+        lib.getrec("NOSUCHREC", 1)
+    with pytest.raises(ab.AcesError):
+        lib.getrec("TESTREC", 8)
+
+
+def test_bad_arguments_return_status(lib):
+    assert lib.h.aces_sym_init(3, (ctypes.c_int * 3)(1, 1, 1), (ctypes.c_int * 3)(1, 1, 1)) < 0
+    lib.sym_init([1], [1])
+    assert lib.h.aces_irpdpd(2, 13) < 0
+    assert lib.h.aces_irpdpd(1, 23) < 0
+    assert lib.h.aces_getlst(None, 1, 1, 9, 1) < 0

@@ -1,0 +1,163 @@
+"""GPU parity tests: the CUDA engine through its C-ABI against the FP64 oracle
+and the reference's golden energies (test/OUTPUT/out.zmat.035.ccsd)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+import acesb200 as ab
+from acesb200.dpd import DPD, get_dense_list, put_dense_list
+from oracle.hamiltonian import from_fixture, synthetic
+from oracle import ccsd
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    lib = ab.load()
+    lib.init(0)
+    return lib
+
+
+def blocks_of(ham):
+    B = ccsd.Blocks(ham)
+    return B, dict(oooo=B.oooo, ooov=B.ooov, oovv=B.oovv, ovov=B.ovov, ovvv=B.ovvv, vvvv=B.vvvv)
+
+
+def setup_lists(lib, ham, fock=False):
+    lib.init(0)
+    pop, vrt = ham.pop_vrt()
+    lib.sym_init(pop, vrt)
+    B, blocks = blocks_of(ham)
+    o = ham.nocc
+    dpd = ab.put_hamiltonian(lib, ham.eps, blocks, ham.irrep[:o], ham.irrep[o:],
+                             fock=ham.fock if fock else None)
+    return B, dpd
+
+
+def read_amplitudes(lib, dpd, o, v):
+    t2 = get_dense_list(lib, dpd, 46, 13, 14).transpose(2, 3, 0, 1)   # [a,b,i,j] -> [i,j,a,b]
+    col = lib.getlst(1, 1, 1, 90)[:, 0]
+    idx, sgn, hpq = dpd.table(9)
+    t1 = np.zeros((o, v))
+    for a in range(v):
+        for i in range(o):
+            if hpq[a, i] == 0:
+                t1[i, a] = col[idx[a, i]]
+    return t1, t2
+
+
+# ---------------------------------------------------------------- XGEMM
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (37, 53, 29), (128, 256, 64), (300, 200, 513),
+                                   (129, 7, 1000)])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+def test_xgemm_fp64_matches_torch(lib, m, n, k, ta, tb):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(m * 7 + n * 3 + k)
+    A = torch.randn((m, k) if ta == "N" else (k, m), generator=g, dtype=torch.float64)
+    B = torch.randn((k, n) if tb == "N" else (n, k), generator=g, dtype=torch.float64)
+    Cm = torch.randn((m, n), generator=g, dtype=torch.float64)
+    opA = A if ta == "N" else A.T
+    opB = B if tb == "N" else B.T
+    ref = 0.7 * opA @ opB - 0.3 * Cm
+    # column-major device copies: store the transpose contiguous
+    dA = A.T.contiguous().cuda()
+    dB = B.T.contiguous().cuda()
+    dC = Cm.T.contiguous().cuda()
+    lda = A.shape[0]
+    ldb = B.shape[0]
+    lib.xgemm(ta, tb, m, n, k, 0.7, dA.data_ptr(), lda, dB.data_ptr(), ldb, -0.3,
+              dC.data_ptr(), m)
+    out = dC.cpu().T
+    err = (out - ref).abs().max().item()
+    assert err <= 1e-12 * max(1.0, ref.abs().max().item()) * np.sqrt(k), err
+
+
+# ---------------------------------------------------------------- lists
+def test_list_roundtrip_dpd(lib):
+    lib.init(0)
+    lib.sym_init([2, 1, 0, 1], [4, 2, 3, 1])
+    irr_o = [0, 0, 1, 3]
+    irr_v = [0, 0, 0, 0, 1, 1, 2, 2, 2, 3]
+    dpd = DPD(lib, irr_o, irr_v)
+    rng = np.random.default_rng(0)
+    io, iv = np.array(irr_o), np.array(irr_v)
+    dense = rng.normal(size=(10, 10, 4, 4))
+    allowed = ((iv[:, None, None, None] ^ iv[None, :, None, None]
+                ^ io[None, None, :, None] ^ io[None, None, None, :]) == 0)
+    dense *= allowed
+    put_dense_list(lib, dpd, 46, 13, 14, dense)
+    back = get_dense_list(lib, dpd, 46, 13, 14)
+    np.testing.assert_array_equal(back, dense)
+    # antisymmetric packed a<b, i<j list
+    aa = dense - dense.transpose(1, 0, 2, 3)
+    aa = aa - aa.transpose(0, 1, 3, 2)
+    put_dense_list(lib, dpd, 44, 1, 3, aa)
+    np.testing.assert_allclose(get_dense_list(lib, dpd, 44, 1, 3), aa, atol=0)
+    # GETALL / PUTALL concatenation over irreps
+    n = sum(lib.irpdpd(h, 13) * lib.irpdpd(h, 14) for h in range(1, 5))
+    vec = lib.getall(n, 1, 46)
+    lib.putall(vec * 2.0, 1, 46)
+    np.testing.assert_array_equal(lib.getall(n, 1, 46), 2.0 * vec)
+    # bounds are checked (acescore/getlst.F:52-90)
+    with pytest.raises(ab.AcesError):
+        lib.getlst(2, lib.list_dims(1, 46)[1], 1, 46)
+
+
+# ---------------------------------------------------------------- CCSD
+def test_ccsd_h2o_dzp_matches_oracle_and_reference(lib):
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat035.npz"))
+    B, dpd = setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=7, cc_maxcyc=50, cc_exporder=5)
+    ref = ccsd.run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5)
+    assert cfg.converged == 1 and cfg.ncycle == ref["ncycle"] == 11
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+    # golden CCSD correlation energy, out.zmat.035.ccsd:628
+    assert abs(cfg.e_ccsd - (-0.226005606663)) < 1e-10
+    t1, t2 = read_amplitudes(lib, dpd, ham.nocc, ham.nvir)
+    np.testing.assert_allclose(t2, ref["t2"], atol=1e-11)
+    np.testing.assert_allclose(t1, ref["t1"], atol=1e-11)
+    # same-spin list 44 = t2 - t2^T (libr2/abtoaa.F)
+    aa = get_dense_list(lib, dpd, 44, 1, 3).transpose(2, 3, 0, 1)
+    np.testing.assert_allclose(aa, ref["t2"] - ref["t2"].transpose(0, 1, 3, 2), atol=1e-11)
+
+
+@pytest.mark.parametrize("o,v,naux,seed", [(6, 24, 40, 5), (9, 41, 60, 11)])
+def test_ccsd_synthetic_c1_matches_oracle(lib, o, v, naux, seed):
+    ham = synthetic(o, v, naux, seed)
+    setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=9, cc_maxcyc=60, cc_exporder=5)
+    ref = ccsd.run_ccsd(ham, cc_conv=9, maxcyc=60, exporder=5)
+    assert cfg.ncycle == ref["ncycle"]
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+
+
+def test_ccsd_synthetic_8_irreps_matches_oracle(lib):
+    ham = synthetic(8, 40, 64, seed=1003, irreps=8)
+    B, dpd = setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=9, cc_maxcyc=60, cc_exporder=5)
+    ref = ccsd.run_ccsd(ham, cc_conv=9, maxcyc=60, exporder=5)
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+    t1, t2 = read_amplitudes(lib, dpd, ham.nocc, ham.nvir)
+    np.testing.assert_allclose(t2, ref["t2"], atol=1e-11)
+
+
+def test_ccsd_non_hartree_fock_fock_matches_oracle(lib):
+    ham = synthetic(5, 20, 30, seed=21)
+    rng = np.random.default_rng(4)
+    h = rng.normal(0, 0.01, (25, 25))
+    ham.fock = ham.fock + 0.5 * (h + h.T)
+    setup_lists(lib, ham, fock=True)
+    cfg = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=6)
+    ref = ccsd.run_ccsd(ham, cc_conv=9, maxcyc=80, exporder=6)
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+
+
+def test_ccsd_errors_are_status_codes(lib):
+    lib.init(0)
+    lib.sym_init([2], [5])
+    with pytest.raises(ab.AcesError) as e:
+        lib.xvcc()
+    assert e.value.status in (-2, -6)   # missing lists / SCFEVALA record

@@ -1,0 +1,132 @@
+"""CPU tests: the oracle pinned to the reference's golden regression outputs.
+
+Golden values are quoted from the reference's captured outputs:
+  test/OUTPUT/out.zmat.035.ccsd (H2O/DZP CCSD, R=0.957 A, A=104.5 deg):
+    SCF energy :443, MP2 pieces FORMT2 block, per-iteration CCSD energies and
+    residual maxima :555-650;
+  test/OUTPUT/out.zmat.020 (H2O/DZP CCSD(T), R=1.0 A, A=104 deg): :650-688.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle.hamiltonian import from_fixture, synthetic
+from oracle import ccsd, ccsd_so
+from oracle.triples import triples
+
+# out.zmat.035.ccsd: "Summary of iterative solution of CC equations"
+GOLD_035_ITER = [
+    -0.216941906555, -0.221394755280, -0.224859749997, -0.225631953135, -0.225982984496,
+    -0.226003683353, -0.226005732666, -0.226005537711, -0.226005607150, -0.226005622312,
+    -0.226005608912,
+]
+GOLD_035_FINAL = -0.226005606663
+# |largest element of residual vector| / |DIIS residual| per iteration
+GOLD_035_RES = [0.80606944e-02, 0.22937753e-02, 0.10929478e-02, 0.16750983e-03,
+                0.12812421e-03, 0.43273349e-04, 0.16675441e-04, 0.24354994e-05,
+                0.38904255e-06, 0.10076627e-06, 0.16830056e-07]
+GOLD_035_DRES = [0.80606944e-02, 0.24718504e-02, 0.86146781e-03, 0.86891628e-04,
+                 0.82442868e-04, 0.17998710e-04, 0.49789397e-05, 0.79920082e-06,
+                 0.24698868e-06, 0.61904624e-07, 0.10316917e-07]
+
+
+@pytest.fixture(scope="module")
+def h2o035():
+    return from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat035.npz"))
+
+
+@pytest.fixture(scope="module")
+def h2o020():
+    return from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat020.npz"))
+
+
+def test_scf_fixture_matches_reference(h2o035, h2o020):
+    # SCFENEG / NUCREP records of test/zmat.035.ccsd and test/zmat.020 TEST.DAT
+    assert abs(h2o035.e_scf - (-76.0465033211)) < 1e-10
+    assert abs(h2o035.e_nuc - 9.19693438045) < 1e-10
+    assert abs(h2o020.e_scf - (-76.0407105174)) < 1e-10
+    # orbital eigenvalues, out.zmat.035.ccsd orbital table (energy order)
+    e = np.sort(h2o035.eps)
+    gold = [-20.5576668354, -1.3457606900, -0.7109542608, -0.5756658799, -0.5027612661,
+            0.2261806614, 0.3179986035, 0.8454784062, 48.0327497683]
+    np.testing.assert_allclose(e[[0, 1, 2, 3, 4, 5, 6, 7, 25]], gold, atol=2e-9)
+    pop, vrt = h2o035.pop_vrt()
+    assert list(pop) == [3, 1, 1, 0] and list(vrt) == [10, 3, 6, 2]
+
+
+def test_mp2_matches_reference(h2o035):
+    B = ccsd.Blocks(h2o035)
+    t1, t2 = ccsd.mp2_guess(B)
+    eaa, eab, etot = ccsd.energy(B, t1, t2)
+    # FORMT2 block of out.zmat.035.ccsd: E2(AA), E2(AB), E2(TOT)
+    assert abs(eaa - (-0.025966426160)) < 1e-10
+    assert abs(eab - (-0.165009054236)) < 1e-10
+    assert abs(etot - (-0.216941906555)) < 1e-10
+    # "Norm of T2AB vector (3087 symmetry allowed elements): 0.1983570155"
+    assert abs(np.linalg.norm(t2) - 0.1983570155) < 1e-9
+    assert np.count_nonzero(np.abs(B.oovv) > 1e-14) <= 3087
+
+
+def test_ccsd_iterations_match_reference(h2o035):
+    h = ccsd.run_ccsd(h2o035, cc_conv=7, maxcyc=50, exporder=5)
+    assert h["converged"] and h["ncycle"] == 11
+    np.testing.assert_allclose(h["energies"], GOLD_035_ITER + [h["energies"][-1]], atol=1e-10)
+    # magnitudes only: the sign of an amplitude depends on the MO phase convention
+    np.testing.assert_allclose(np.abs(h["res"]), GOLD_035_RES, rtol=2e-7)
+    np.testing.assert_allclose(np.abs(h["dres"]), GOLD_035_DRES, rtol=2e-7)
+    assert abs(h["e_final"] - GOLD_035_FINAL) < 1e-10
+    # "Norm of T1AA vector (39 ...): 0.0191689919", "Norm of T2AB vector ...: 0.2195553160"
+    assert abs(np.linalg.norm(h["t1"]) - 0.0191689919) < 1e-9
+    assert abs(np.linalg.norm(h["t2"]) - 0.2195553160) < 1e-9
+
+
+def test_ccsd_t_matches_reference(h2o020):
+    h = ccsd.run_ccsd(h2o020, cc_conv=7, maxcyc=50, exporder=5)
+    # out.zmat.020:650 CCSD total, :679-680 E[4]T / E[5]ST, :688 CCSD(T)
+    assert abs(h["e_final"] + h2o020.e_scf - (-76.269769846591)) < 1e-10
+    e4, e5 = triples(h2o020, h["t1"], h["t2"])
+    assert abs(e4 - (-0.003870011955)) < 2e-11
+    assert abs(e5 - 0.000163057248) < 2e-11
+    assert abs(h["e_final"] + h2o020.e_scf + e4 + e5 - (-76.273476801298)) < 1e-10
+
+
+def test_closed_shell_equals_spin_orbital_nonhf():
+    ham = synthetic(3, 5, 12, seed=7)
+    rng = np.random.default_rng(1)
+    h = rng.normal(0, 0.05, (8, 8))
+    ham.fock = ham.fock + h + h.T
+    B = ccsd.Blocks(ham)
+    t1 = rng.normal(0, 0.05, (3, 5))
+    t2 = ccsd.symmetrize_t2(rng.normal(0, 0.05, (3, 3, 5, 5)))
+    Z1, Z2 = ccsd.residual(B, t1, t2)
+    asym, f, no = ccsd_so.spin_hamiltonian(ham)
+    T1, T2 = ccsd_so.to_spin_amplitudes(t1, t2)
+    S1, S2 = ccsd_so.residual(asym, f, no, T1, T2)
+    np.testing.assert_allclose(S1[0::2, 0::2], Z1, atol=1e-14)
+    np.testing.assert_allclose(S2[0::2, 1::2, 0::2, 1::2], Z2, atol=1e-14)
+    assert abs(ccsd.energy(B, t1, t2)[2] - ccsd_so.energy(asym, f, no, T1, T2)) < 1e-14
+
+
+def test_triples_equals_spin_orbital():
+    ham = synthetic(3, 6, 14, seed=3)
+    h = ccsd.run_ccsd(ham, cc_conv=10)
+    t1, t2 = h["t1"], h["t2"]
+    asym, f, no = ccsd_so.spin_hamiltonian(ham)
+    T1, T2 = ccsd_so.to_spin_amplitudes(t1, t2)
+    o = slice(0, no)
+    v = slice(no, asym.shape[0])
+    eo, ev = np.diag(f)[o], np.diag(f)[v]
+    D = (eo[:, None, None, None, None, None] + eo[None, :, None, None, None, None]
+         + eo[None, None, :, None, None, None] - ev[None, None, None, :, None, None]
+         - ev[None, None, None, None, :, None] - ev[None, None, None, None, None, :])
+    X = (np.einsum("jkae,eibc->ijkabc", T2, asym[v, o, v, v])
+         - np.einsum("imbc,majk->ijkabc", T2, asym[o, v, o, o]))
+    Pi = lambda x: x - x.transpose(1, 0, 2, 3, 4, 5) - x.transpose(2, 1, 0, 3, 4, 5)
+    Pa = lambda x: x - x.transpose(0, 1, 2, 4, 3, 5) - x.transpose(0, 1, 2, 5, 4, 3)
+    t3c = Pa(Pi(X)) / D
+    t3d = Pa(Pi(np.einsum("ia,jkbc->ijkabc", T1, asym[o, o, v, v]))) / D
+    e4, e5 = triples(ham, t1, t2)
+    assert abs(e4 - np.sum(t3c * D * t3c) / 36) < 1e-16
+    assert abs(e5 - np.sum(t3c * D * t3d) / 36) < 1e-18
