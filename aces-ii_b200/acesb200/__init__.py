@@ -46,10 +46,12 @@ class CCConfig(C.Structure):
     _fields_ = [
         ("cc_conv", C.c_int), ("cc_maxcyc", C.c_int), ("cc_exporder", C.c_int),
         ("precision", C.c_int), ("triples", C.c_int), ("use_graph", C.c_int),
-        ("verbose", C.c_int), ("reserved", C.c_int),
+        ("verbose", C.c_int), ("timing_warmup", C.c_int),
         ("e_ccsd", C.c_double), ("e_t4", C.c_double), ("e_st5", C.c_double),
         ("last_residual", C.c_double), ("ncycle", C.c_int), ("converged", C.c_int),
         ("seconds_per_iter", C.c_double), ("seconds_triples", C.c_double),
+        ("seconds_ladder", C.c_double), ("flops_per_iter", C.c_double),
+        ("launches_per_iter", C.c_longlong), ("seconds_setup", C.c_double),
     ]
 
 
@@ -190,10 +192,10 @@ class Lib:
         return cfg
 
     def xvcc(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, triples=0,
-             use_graph=0, verbose=0, allow_noconv=False):
+             use_graph=0, verbose=0, allow_noconv=False, timing_warmup=0):
         cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
                        precision=precision, triples=triples, use_graph=use_graph,
-                       verbose=verbose)
+                       verbose=verbose, timing_warmup=timing_warmup)
         return self._run("xvcc_run", cfg, allow_noconv)
 
     def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0):

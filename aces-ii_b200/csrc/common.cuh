@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -13,6 +14,10 @@
 namespace acesb200 {
 
 void set_error(const char *fmt, ...);
+
+// number of kernels the library has launched (reported by the benchmarks)
+extern std::atomic<long long> g_launches;
+inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 #define ACES_CUDA(call)                                                        \
   do {                                                                         \

@@ -5,6 +5,7 @@
 //
 // Index conventions (C order): t1[i,a]; t2[i,j,a,b] = t_{iJ}^{aB} (the
 // reference's list 46, Ab x Ij, in C1); integrals <pq|rs> as I_xxxx[p,q,r,s].
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
@@ -41,6 +42,9 @@ void CCEngine::release() {
   if (split_tmpB.hi) cudaFree(split_tmpB.hi);
   split_tmpA = SplitOperand();
   split_tmpB = SplitOperand();
+  if (ev_lad0) cudaEventDestroy(ev_lad0);
+  if (ev_lad1) cudaEventDestroy(ev_lad1);
+  ev_lad0 = ev_lad1 = nullptr;
   if (st) cudaStreamDestroy(st);
   st = 0;
 }
@@ -528,8 +532,14 @@ int CCEngine::residual() {
   ACES_TRY(perm(tauT.p, v, v, o, o, 0.0, {PT(tau.p, 1.0, st2[2], st2[3], st2[0], st2[1])}));
   ACES_TRY(G(v * v, o * o, o * o, 1.0, tauT.p, OO, WmnT.p, OO, 1.0, cview_colmajor(Z2.p, VV)));
   // ---- particle-particle ladder (DRLAD ITYPE=6, vcc/ladab1.F:61) ----
+  if (!ev_lad0) {
+    ACES_CUDA(cudaEventCreate(&ev_lad0));
+    ACES_CUDA(cudaEventCreate(&ev_lad1));
+  }
+  ACES_CUDA(cudaEventRecord(ev_lad0, st));
   ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0, cview_colmajor(Z2.p, VV),
              true));
+  ACES_CUDA(cudaEventRecord(ev_lad1, st));
 
   // ---- W(mbej) ABAB and ABBA (DWMBEJ, T1RING), layout W[j,b,m,e] ----
   ACES_TRY(copy(WA.p, WA0.p, (size_t)OO * VV));
@@ -620,6 +630,10 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
   double hd[40];
   ACES_CUDA(cudaMemcpyAsync(hd, d, 40 * 8, cudaMemcpyDeviceToHost, st));
   ACES_CUDA(cudaStreamSynchronize(st));
+  if (int tcs = tc_status_and_clear()) {
+    set_error("tensor-core contraction gave up waiting (code %d) at cycle %d", tcs, icycle);
+    return ACES_ERR_TIMEOUT;
+  }
   e3[0] = hd[1];  // E_AA (printed alpha-alpha part)
   e3[1] = hd[0];  // E_AB
   e3[2] = 2.0 * hd[1] + hd[0] + hd[2];
@@ -740,29 +754,47 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   engine_reset();
   CCEngine &E = *engine_instance(true);
   E.prec = cfg->precision;
-  ACES_TRY(E.load_from_lists());
-  ACES_TRY(E.setup_intermediates());
-  ACES_TRY(E.mp2_guess());
-  const double tol = std::pow(10.0, -cfg->cc_conv);
   cudaEvent_t ev0, ev1;
   ACES_CUDA(cudaEventCreate(&ev0));
   ACES_CUDA(cudaEventCreate(&ev1));
+  {
+    auto t0 = std::chrono::steady_clock::now();
+    ACES_TRY(E.load_from_lists());
+    ACES_TRY(E.setup_intermediates());
+    ACES_TRY(E.mp2_guess());
+    ACES_CUDA(cudaStreamSynchronize(E.st));
+    cfg->seconds_setup =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  const double tol = std::pow(10.0, -cfg->cc_conv);
+  float ms_lad_total = 0.f;
+  int ntimed = 0;
+  long long launches_timed = 0;
   double e3[3] = {0, 0, 0}, res = 0, dres = 0;
   bool converged = false;
   int icycle = 0;
   float ms_total = 0.f;
   for (icycle = 1; icycle <= cfg->cc_maxcyc; ++icycle) {
     bool extrap = false;
+    long long l0 = g_launches.load();
+    E.gemm_flops = 0.0;
     ACES_CUDA(cudaEventRecord(ev0, E.st));
     ACES_TRY(E.iteration(icycle, cfg->cc_exporder, e3, &res, &dres, &extrap));
+    cfg->flops_per_iter = E.gemm_flops;
     int ndimr = icycle < cfg->cc_exporder ? icycle : cfg->cc_exporder;
     bool conv = std::fabs(res) < tol;
     if (!conv) ACES_TRY(accept(E, extrap, ndimr));
     ACES_CUDA(cudaEventRecord(ev1, E.st));
     ACES_CUDA(cudaEventSynchronize(ev1));
-    float ms = 0.f;
+    float ms = 0.f, msl = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    ms_total += ms;
+    cudaEventElapsedTime(&msl, E.ev_lad0, E.ev_lad1);
+    if (icycle > cfg->timing_warmup) {
+      ms_total += ms;
+      ms_lad_total += msl;
+      ntimed++;
+      launches_timed += g_launches.load() - l0;
+    }
     if (cfg->verbose)
       printf("  cycle %3d  E(corr) = %.12f  max res = % .8e  max DIIS res = % .8e  %.3f ms\n",
              icycle, e3[2], res, dres, ms);
@@ -782,7 +814,9 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   cfg->last_residual = res;
   cfg->ncycle = icycle;
   cfg->converged = converged ? 1 : 0;
-  cfg->seconds_per_iter = ms_total * 1e-3 / (icycle > 0 ? icycle : 1);
+  cfg->seconds_per_iter = ntimed ? ms_total * 1e-3 / ntimed : 0.0;
+  cfg->seconds_ladder = ntimed ? ms_lad_total * 1e-3 / ntimed : 0.0;
+  cfg->launches_per_iter = ntimed ? launches_timed / ntimed : 0;
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   ACES_TRY(E.write_back());

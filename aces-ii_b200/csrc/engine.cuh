@@ -60,6 +60,7 @@ class CCEngine {
   // statistics
   long long gemm_calls = 0;
   double gemm_flops = 0.0;
+  cudaEvent_t ev_lad0 = nullptr, ev_lad1 = nullptr;  // around the pp-ladder contraction
 
   ~CCEngine();
   int alloc(DBuf &b, size_t n);

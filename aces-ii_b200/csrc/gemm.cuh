@@ -39,7 +39,7 @@ struct SplitOperand {
   void *hi = nullptr;   // __nv_bfloat16[rows_pad * k_pad]
   void *lo = nullptr;
   int rows = 0, k = 0, rows_pad = 0, k_pad = 0;
-  size_t bytes() const { return (size_t)rows_pad * k_pad * 2 * 2; }
+  size_t cap = 0;       // bytes allocated at hi (both planes)
 };
 
 // rows and K padding of split operands (the tcgen05 kernel's tile sizes)
@@ -53,5 +53,9 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 // acc = A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (TMEM), C = alpha*acc + beta*C (FP64).
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st);
+
+// Error code recorded by a tcgen05 kernel whose bounded wait expired (0 = ok);
+// reading it clears it.
+int tc_status_and_clear();
 
 }  // namespace acesb200

@@ -154,6 +154,7 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
     k_gemm_nt_f64<2><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C);
   else
     k_gemm_nt_f64<1><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C);
+  count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }

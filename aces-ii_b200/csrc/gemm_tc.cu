@@ -1,5 +1,21 @@
-// gemm_tc.cu -- split-precision (BF16x3) operand packing and the tcgen05
-// contraction kernel.
+// gemm_tc.cu -- split-precision (BF16x3) contraction on the Blackwell tensor
+// cores: TMA -> shared memory -> tcgen05.mma (kind::f16, BF16 x BF16 -> FP32
+// in TMEM) -> tcgen05.ld epilogue with FP64 alpha/beta.
+//
+// Each FP64 operand x is stored as two BF16 planes, hi = bf16(x) and
+// lo = bf16(x - hi).  The kernel accumulates hi*hi + hi*lo + lo*hi for every
+// K slice into one TMEM accumulator (the lo*lo term, ~2^-18 relative, is
+// dropped), which gives ~16 significant bits per product and FP32 sums.
+//
+// CTA tile 128 x 128 x 64, 3-stage mbarrier pipeline, 10 warps:
+//   warp 0  TMA producer (one elected lane)
+//   warp 1  TMEM allocator + MMA issuer (one elected lane)
+//   warps 2-9 epilogue: two warps per TMEM lane quadrant, each thread one
+//             output row x 64 columns, accumulated in FP64 across K chunks
+// Every mbarrier wait is bounded by a %globaltimer limit; on expiry the
+// kernel records an error code in g_tc_status, drains its own TMA copies,
+// releases TMEM and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -15,11 +31,9 @@ __global__ void k_split_pack(__nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__re
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     int r = (int)(idx / k_pad), c = (int)(idx % k_pad);
-    float x = 0.f;
     double xd = 0.0;
     if (r < rows && c < k) xd = src[(long long)r * ld + c];
-    x = (float)xd;
-    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    __nv_bfloat16 h = __float2bfloat16_rn((float)xd);
     float rem = (float)(xd - (double)__bfloat162float(h));
     hi[idx] = h;
     lo[idx] = __float2bfloat16_rn(rem);
@@ -31,9 +45,10 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
   int rp = (rows + kSplitRowPad - 1) / kSplitRowPad * kSplitRowPad;
   int kp = (k + kSplitKPad - 1) / kSplitKPad * kSplitKPad;
   size_t need = (size_t)rp * kp * 2 * 2;
-  if (!op.hi || op.bytes() < need) {
+  if (!op.hi || op.cap < need) {
     if (op.hi) cudaFree(op.hi);
     op.hi = op.lo = nullptr;
+    op.cap = 0;
     void *p = nullptr;
     if (cudaMalloc(&p, need) != cudaSuccess) {
       cudaGetLastError();
@@ -41,8 +56,7 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
       return ACES_ERR_NOMEM;
     }
     op.hi = p;
-    op.rows_pad = rp;
-    op.k_pad = kp;
+    op.cap = need;
   }
   op.rows = rows;
   op.k = k;
@@ -54,15 +68,341 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
   if (nb > 148 * 32) nb = 148 * 32;
   k_split_pack<<<(unsigned)nb, 256, 0, st>>>((__nv_bfloat16 *)op.hi, (__nv_bfloat16 *)op.lo, src,
                                              ld, rows, k, rp, kp);
+  count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
 
+namespace {
+constexpr int TBM = 128, TBN = 128, TBK = 64, STAGES = 3;
+constexpr int CHUNK = 2;                              // k tiles per FP32 accumulation chunk
+constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
+constexpr int TILE_B = TBN * TBK * 2;
+constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
+constexpr int kThreads = 32 * (2 + kEpiWarps);
+constexpr int kTmemCols = 2 * TBN;                    // two ping-pong accumulators
+constexpr unsigned long long kWaitNs = 4000000000ULL;  // 4 s bound on any wait
+
+__device__ int g_tc_status;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  unsigned long long t0 = gtimer();
+  while (!mbar_try(bar, parity)) {
+    if (gtimer() - t0 > kWaitNs) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), LBO unused (1), sm100 descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, N>>3, M>>4
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) |
+                            ((uint32_t)(TBM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+// The MMA warp accumulates CHUNK k tiles at a time in FP32 into one of two TMEM
+// accumulators (ping-pong); the epilogue warps drain every finished chunk into
+// FP64 registers while the next chunk is computed.  This bounds the number of
+// FP32 tensor-core accumulations any partial sum sees to 12*CHUNK, so the
+// truncation bias of the tensor-core adders stays at ~1e-6 relative instead of
+// growing with K.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                  int M, int N, int kTiles, double alpha, double beta, CView C) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+  uint64_t *full = bars;                      // [STAGES] TMA -> MMA
+  uint64_t *empty = bars + STAGES;            // [STAGES] MMA -> TMA
+  uint64_t *acc_full = bars + 2 * STAGES;     // [2] MMA -> epilogue
+  uint64_t *acc_empty = bars + 2 * STAGES + 2;  // [2] epilogue -> MMA
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+  const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int issued = 0;
+    for (int kt = 0; kt < kTiles; ++kt) {
+      int s = kt % STAGES;
+      if (kt >= STAGES) {
+        if (!mbar_wait(smem_u32(&empty[s]), ((kt / STAGES) - 1) & 1)) {
+          atomicExch(&g_tc_status, 1);
+          *(volatile int *)abort_flag = 1;
+          break;
+        }
+      }
+      if (*(volatile int *)abort_flag) break;
+      uint32_t fb = smem_u32(&full[s]);
+      unsigned char *st = smem + s * STAGE_BYTES;
+      mbar_expect_tx(fb, STAGE_BYTES);
+      int kx = kt * TBK;
+      tma_load_2d(smem_u32(st), &mAh, kx, m0, fb);
+      tma_load_2d(smem_u32(st + TILE_A), &mAl, kx, m0, fb);
+      tma_load_2d(smem_u32(st + 2 * TILE_A), &mBh, kx, n0, fb);
+      tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &mBl, kx, n0, fb);
+      issued = kt + 1;
+    }
+    // drain: the most recent phase of every stage still possibly in flight
+    int first = issued > STAGES ? issued - STAGES : 0;
+    for (int kt = first; kt < issued; ++kt)
+      if (!mbar_wait(smem_u32(&full[kt % STAGES]), (kt / STAGES) & 1)) atomicExch(&g_tc_status, 2);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    for (int kt = 0; kt < kTiles; ++kt) {
+      const int c = kt / CHUNK, b = c & 1, kin = kt % CHUNK;
+      if (kin == 0 && c >= 2) {
+        if (!mbar_wait(smem_u32(&acc_empty[b]), ((c >> 1) - 1) & 1)) {
+          atomicExch(&g_tc_status, 5);
+          *(volatile int *)abort_flag = 1;
+          break;
+        }
+      }
+      int s = kt % STAGES;
+      if (!mbar_wait(smem_u32(&full[s]), (kt / STAGES) & 1)) {
+        atomicExch(&g_tc_status, 3);
+        *(volatile int *)abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+      uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + TILE_B;
+      uint32_t acc_t = tmem + (uint32_t)(b * TBN);
+#pragma unroll
+      for (int kk = 0; kk < TBK / 16; ++kk) {
+        uint32_t off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzled row
+        uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
+        umma(acc_t, umma_desc(ah + off), umma_desc(bh + off), acc);
+        umma(acc_t, umma_desc(ah + off), umma_desc(bl + off), 1u);
+        umma(acc_t, umma_desc(al + off), umma_desc(bh + off), 1u);
+      }
+      umma_commit(smem_u32(&empty[s]));
+      if (kin == CHUNK - 1 || kt == kTiles - 1) umma_commit(smem_u32(&acc_full[b]));
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue: FP64 accumulation of the chunks ----------------
+    const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
+    const int half = (warp - 2) >> 2;      // which 64 accumulator columns
+    const int row = q * 32 + lane;
+    double acc[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    bool ok = true;
+    for (int c = 0; c < nChunks; ++c) {
+      const int b = c & 1;
+      bool w = mbar_wait(smem_u32(&acc_full[b]), (c >> 1) & 1);
+      if (!w) atomicExch(&g_tc_status, 4);
+      ok = __all_sync(0xffffffffu, w && !*(volatile int *)abort_flag);
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * 64);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t r[32];
+        tmem_ld32(tbase + h * 32, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[h * 32 + j] += (double)__uint_as_float(r[j]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+    }
+    const int m = m0 + row;
+    if (ok && m < M) {
+      const long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
+#pragma unroll
+      for (int j = 0; j < 64; ++j) {
+        int n = n0 + half * 64 + j;
+        if (n < N) {
+          double *cp = C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
+          double v = alpha * acc[j];
+          if (beta != 0.0) v += beta * *cp;
+          *cp = v;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return ACES_ERR_CUDA;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows_pad};
+  cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
+  cuuint32_t box[2] = {(cuuint32_t)TBK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return ACES_ERR_CUDA;
+  }
+  return ACES_OK;
+}
+}  // namespace
+
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st) {
-  (void)A; (void)B; (void)M; (void)N; (void)alpha; (void)beta; (void)C; (void)st;
-  set_error("BF16x3 contraction not available in this build");
-  return ACES_ERR_UNSUPPORTED;
+  if (M <= 0 || N <= 0) return ACES_OK;
+  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad % TBM ||
+      B.rows_pad % TBN || A.k_pad == 0) {
+    set_error("gemm_nt_bf16x3: operand shapes do not match (%d/%d, %d, %d)", A.k_pad, B.k_pad,
+              A.rows, B.rows);
+    return ACES_ERR_ARG;
+  }
+  static bool attr = false;
+  if (!attr) {
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   SMEM_BYTES));
+    int zero = 0;
+    ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
+    attr = true;
+  }
+  CUtensorMap mAh, mAl, mBh, mBl;
+  ACES_TRY(make_map(&mAh, A.hi, A.rows_pad, A.k_pad, TBM));
+  ACES_TRY(make_map(&mAl, A.lo, A.rows_pad, A.k_pad, TBM));
+  ACES_TRY(make_map(&mBh, B.hi, B.rows_pad, B.k_pad, TBN));
+  ACES_TRY(make_map(&mBl, B.lo, B.rows_pad, B.k_pad, TBN));
+  dim3 grid((N + TBN - 1) / TBN, (M + TBM - 1) / TBM);
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, A.k_pad / TBK,
+                                                     alpha, beta, C);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+int tc_status_and_clear() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(int)) != cudaSuccess) return -1;
+  if (v) cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int));
+  return v;
 }
 
 }  // namespace acesb200

@@ -121,10 +121,11 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
     if (D == 0) k_permute_tiled<0><<<(unsigned)nb, blk, 0, st>>>(out, a);
     if (D == 1) k_permute_tiled<1><<<(unsigned)nb, blk, 0, st>>>(out, a);
     if (D == 2) k_permute_tiled<2><<<(unsigned)nb, blk, 0, st>>>(out, a);
+    count_launch();
   } else {
     long long nb = (total + 255) / 256;
     if (nb > 148 * 64) nb = 148 * 64;
-    k_permute_naive<<<(unsigned)nb, 256, 0, st>>>(out, a, total);
+    k_permute_naive<<<(unsigned)nb, 256, 0, st>>>(out, a, total); count_launch();
   }
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -151,7 +152,7 @@ void launch_tau(double *tau, const double *t2, const double *t1, double c, int o
   long long total = (long long)o * o * v * v;
   long long nb = (total + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total);
+  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total); count_launch();
 }
 
 __global__ void k_newt(double *__restrict__ t2n, const double *__restrict__ z2,
@@ -180,7 +181,7 @@ void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, c
   long long total = (long long)o * o * v * v;
   long long nb = (total + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_newt<<<(unsigned)nb, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, total);
+  k_newt<<<(unsigned)nb, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, total); count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -241,8 +242,8 @@ __global__ void k_final_sum(double *out, const double *part, int nblk, int nv) {
 void launch_energy(double *out3, const double *t2, const double *t1, const double *voovv,
                    const double *fov, int o, int v, double *scratch, cudaStream_t st) {
   long long total = (long long)o * o * v * v;
-  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total);
-  k_final_sum<<<3, 32, 0, st>>>(out3, scratch, kRedBlocks, 3);
+  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total); count_launch();
+  k_final_sum<<<3, 32, 0, st>>>(out3, scratch, kRedBlocks, 3); count_launch();
 }
 
 __global__ void k_diff(double *e, const double *a, const double *b, long long n) {
@@ -254,7 +255,7 @@ __global__ void k_diff(double *e, const double *a, const double *b, long long n)
 void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st) {
   long long nb = (n + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_diff<<<(unsigned)nb, 256, 0, st>>>(e, xnew, xold, n);
+  k_diff<<<(unsigned)nb, 256, 0, st>>>(e, xnew, xold, n); count_launch();
 }
 
 struct HistPtrs {
@@ -313,8 +314,8 @@ int launch_diis_dots(double *dots_out, const double *e_new, const double *const 
   if (nh < 1 || nh > 25) return ACES_ERR_ARG;
   HistPtrs h;
   for (int k = 0; k < 25; ++k) h.p[k] = k < nh ? hist[k] : nullptr;
-  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v);
-  k_final_sum<<<nh, 32, 0, st>>>(dots_out, scratch, kRedBlocks, 25);
+  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v); count_launch();
+  k_final_sum<<<nh, 32, 0, st>>>(dots_out, scratch, kRedBlocks, 25); count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
@@ -375,8 +376,8 @@ __global__ void k_absmax_final(double *out, const double *pv, const long long *p
 void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st) {
   double *pv = scratch;
   long long *pi = (long long *)(scratch + kRedBlocks);
-  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v);
-  k_absmax_final<<<1, 1, 0, st>>>(out, pv, pi, kRedBlocks);
+  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v); count_launch();
+  k_absmax_final<<<1, 1, 0, st>>>(out, pv, pi, kRedBlocks); count_launch();
 }
 
 // Bordered DIIS system [[0,-1..],[-1,B]] (lam,c) = (-1,0,..) by LU with
@@ -425,7 +426,7 @@ __global__ void k_diis_solve(double *coef, int *status, const double *B, int n) 
 }
 
 void launch_diis_solve(double *coef_out, int *status_out, const double *B, int n, cudaStream_t st) {
-  k_diis_solve<<<1, 32, 0, st>>>(coef_out, status_out, B, n);
+  k_diis_solve<<<1, 32, 0, st>>>(coef_out, status_out, B, n); count_launch();
 }
 
 __global__ void k_lincomb(double *__restrict__ out, const double *__restrict__ base,
@@ -444,7 +445,7 @@ void launch_lincomb(double *out, const double *base, const double *c, const doub
   for (int k = 0; k < 25; ++k) a.p[k] = k < n ? p[k] : nullptr;
   long long nb = (len + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_lincomb<<<(unsigned)nb, 256, 0, st>>>(out, base, c, a, n, len);
+  k_lincomb<<<(unsigned)nb, 256, 0, st>>>(out, base, c, a, n, len); count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -497,7 +498,7 @@ void launch_gather(double *dense, const DpdMap &m, cudaStream_t st) {
   long long nb = (total + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
   if (nb < 1) nb = 1;
-  k_gather<<<(unsigned)nb, 256, 0, st>>>(dense, m, total);
+  k_gather<<<(unsigned)nb, 256, 0, st>>>(dense, m, total); count_launch();
 }
 
 void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st) {
@@ -505,7 +506,7 @@ void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st) {
   long long nb = (total + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
   if (nb < 1) nb = 1;
-  k_scatter<<<(unsigned)nb, 256, 0, st>>>(dense, m, total);
+  k_scatter<<<(unsigned)nb, 256, 0, st>>>(dense, m, total); count_launch();
 }
 
 }  // namespace acesb200

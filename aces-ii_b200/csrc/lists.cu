@@ -12,6 +12,7 @@
 namespace acesb200 {
 
 static thread_local char g_err[512] = "";
+std::atomic<long long> g_launches{0};
 
 void set_error(const char *fmt, ...) {
   va_list ap;

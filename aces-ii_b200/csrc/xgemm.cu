@@ -74,5 +74,11 @@ extern "C" int aces_xgemm(char transa, char transb, int m, int n, int k, double 
     set_error("aces_xgemm: %s", cudaGetErrorString(e));
     status = ACES_ERR_CUDA;
   }
+  if (status == ACES_OK && precision == ACES_PREC_BF16X3) {
+    if (int tcs = tc_status_and_clear()) {
+      set_error("aces_xgemm: tensor-core contraction gave up waiting (code %d)", tcs);
+      status = ACES_ERR_TIMEOUT;
+    }
+  }
   return status;
 }

@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark: RHF-CCSD seconds per iteration on one B200.
+
+Workload (the reference's headline configuration that fits one GPU): the
+seeded synthetic closed-shell C1 Hamiltonian with nocc=20, nvir=180, naux=600
+(acesb200.workloads 'c2'); <ab|cd> alone is 8.4 GB of FP64 and is streamed by
+every iteration, so every step's inputs exceed the 126 MB L2.
+
+A step is one CCSD iteration (residual, Jacobi update, energy, DIIS) through
+the engine's xvcc_run entry point.  Printed JSON line:
+  value      device time per iteration (CUDA events on the engine stream,
+             inputs resident in HBM, W warm-up cycles excluded), BF16x3 split
+             contractions on tcgen05 (default) or FP64 (--precision fp64);
+  e2e        the same metric through the C-ABI with HOST lists: PUTLST of the
+             six integral lists from pinned memory, xvcc_run for K cycles and
+             GETLST of T2, all inside the timed region, divided by K;
+  roofline   the particle-particle ladder contraction (2 o^2 v^4 flops, 3 BF16
+             products each) against the measured bf16 peak;
+  cpu_baseline  the FP64 numpy restatement of the reference (oracle/) on the
+             host cores, one CCSD iteration of the same system.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "aces-ii_b200"))
+sys.path.insert(0, ROOT)
+
+W_NAME = "c2"
+
+
+def args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64"])
+    p.add_argument("--workload", default=W_NAME)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64-compare", action="store_true")
+    p.add_argument("--kernel-case", default=None,
+                   help="run one contraction shape through aces_xgemm and exit "
+                        "(small cases for ncu captures): ladder-small")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.p is None:
+            return
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        pw = [float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k] == "Active"})
+        loaded = [s for s, p in zip(sm, pw) if p > 250.0] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows), "power_w_max": max(pw) if pw else None}
+
+
+# ------------------------------------------------------------------ inputs
+def host_lists(wl, device):
+    """The six integral lists + orbital energies of the workload as pinned host
+    buffers in the list layout (column-major irrep block, C1), built on the
+    GPU from the seeded DF factors."""
+    import numpy as np
+    import torch
+    from acesb200 import INTEGRAL_LISTS
+    from acesb200.workloads import synthetic_df
+
+    eps, B, irr = synthetic_df(**wl)
+    o, v = wl["nocc"], wl["nvir"]
+    return _lists_from_df(eps, B, o, v, device)
+
+
+def _lists_from_df(eps, B, o, v, device):
+    import torch
+    from acesb200 import INTEGRAL_LISTS
+    Bt = torch.from_numpy(B).to(device)
+    sl = {"o": slice(0, o), "v": slice(o, o + v)}
+    out = {}
+    for lst, (tl, tr, key, perm) in INTEGRAL_LISTS.items():
+        # physicists' <pq|rs> = (pr|qs)
+        p, q, r, s = key
+        L1 = Bt[:, sl[p], sl[r]].reshape(Bt.shape[0], -1)
+        L2 = Bt[:, sl[q], sl[s]].reshape(Bt.shape[0], -1)
+        X = (L1.T @ L2).reshape(Bt[:, sl[p], sl[r]].shape[1:] + Bt[:, sl[q], sl[s]].shape[1:])
+        phys = X.permute(0, 2, 1, 3)                  # [p,q,r,s]
+        dense = phys.permute(*perm)                   # [row p, row q, col r, col s]
+        buf = dense.permute(3, 2, 1, 0).contiguous()  # column-major list matrix
+        host = torch.empty(buf.shape, dtype=torch.float64, pin_memory=(device.type == "cuda"))
+        host.copy_(buf)
+        out[lst] = (tl, tr, host)
+        del X, phys, dense, buf
+    del Bt
+    if device.type == "cuda":
+        torch.cuda.synchronize(device)
+        torch.cuda.empty_cache()
+    return eps, out, o, v
+
+
+def put_lists(lib, eps, lists):
+    lib.putrec("SCFEVALA", eps)
+    nbytes = eps.nbytes
+    for lst, (tl, tr, host) in lists.items():
+        lib.inipck(1, tl, tr, lst)
+        a = host.numpy()
+        lib.putlst_raw(a, 1, lib.irpdpd(1, tr), 1, lst)
+        nbytes += a.nbytes
+    return nbytes
+
+
+# ------------------------------------------------------------------ arms
+def run_ours(a, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import acesb200 as ab
+    from acesb200.workloads import WORKLOADS
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = WORKLOADS[a.workload]
+    prec = ab.PREC_BF16X3 if a.precision == "bf16x3" else ab.PREC_FP64
+    lib = ab.load()
+    eps, lists, o, v = host_lists(wl, dev)
+    K, W = a.steps, a.warmup
+
+    # ---- value: inputs resident, device-timed cycles after W warm-up cycles
+    lib.init(local_rank)
+    lib.sym_init([o], [v])
+    put_lists(lib, eps, lists)
+    torch.cuda.synchronize()
+    barrier(world)
+    with Clocks(local_rank) as clk:
+        cfg = lib.xvcc(cc_conv=30, cc_maxcyc=W + K, cc_exporder=5, precision=prec,
+                       timing_warmup=W, allow_noconv=True)
+        torch.cuda.synchronize()
+    barrier(world)
+    s_iter = max_over_ranks(cfg.seconds_per_iter, world)
+    s_lad = max_over_ranks(cfg.seconds_ladder, world)
+    e_split = cfg.e_ccsd
+
+    # ---- FP64 GPU path, same cycles, for the split-precision comparison
+    fp64 = None
+    if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
+        c64 = lib.xvcc(cc_conv=30, cc_maxcyc=W + K, cc_exporder=5, precision=ab.PREC_FP64,
+                       timing_warmup=W, allow_noconv=True)
+        fp64 = {"seconds_per_iter": c64.seconds_per_iter, "e_corr": c64.e_ccsd,
+                "dE_split_minus_fp64": e_split - c64.e_ccsd,
+                "speedup_split_vs_fp64": c64.seconds_per_iter / cfg.seconds_per_iter}
+
+    # ---- e2e: host lists -> PUTLST -> xvcc_run (K cycles) -> GETLST T2
+    lib.init(local_rank)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    lib.sym_init([o], [v])
+    h2d = put_lists(lib, eps, lists)
+    ce = lib.xvcc(cc_conv=30, cc_maxcyc=K, cc_exporder=5, precision=prec, allow_noconv=True)
+    nr, nc = lib.list_dims(1, 46)
+    t2 = lib.getlst(1, nc, 1, 46)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    barrier(world)
+    e2e = max_over_ranks((t1 - t0) / K, world)
+    d2h = t2.nbytes + 8
+    lib.fin()
+
+    pk, pk_src = peaks()
+    launch_flops = 2.0 * (o * o) * (v * v) * (v * v)
+    if prec == ab.PREC_BF16X3:
+        executed = 3.0 * launch_flops
+        peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+        roof = {"bound": "tensor", "kernel": "k_gemm_bf16x3 (particle-particle ladder)",
+                "achieved": executed / s_lad / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "frac": executed / s_lad / 1e12 / peak,
+                "peak_source": f"bf16_tflops_sustained of {pk_src} MEASURED_PEAKS.json",
+                "algorithmic_flops_per_launch": launch_flops,
+                "executed_bf16_flops_per_launch": executed,
+                "seconds_per_launch": s_lad, "traffic": LADDER_TRAFFIC.get(a.workload)}
+    else:
+        roof = {"bound": "tensor", "kernel": "k_gemm_nt_f64 (particle-particle ladder)",
+                "achieved": launch_flops / s_lad / 1e12, "peak": None, "unit": "TFLOP/s",
+                "frac": None, "peak_source": "no FP64 peak in MEASURED_PEAKS.json",
+                "algorithmic_flops_per_launch": launch_flops, "seconds_per_launch": s_lad,
+                "traffic": None}
+
+    line = {
+        "metric": "CCSD s/iter, synthetic closed-shell o=20 v=180 naux=600 (split BF16x3 vs FP64 GPU)",
+        "value": s_iter, "unit": "s/iter", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": s_iter * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3" if prec == ab.PREC_BF16X3 else "f64",
+        "data": "synthetic: seeded DF generator (acesb200.workloads c2)",
+        "config": {"workload": f"{a.workload}: RHF-CCSD, C1, nocc={o}, nvir={v}, naux={wl['naux']}, "
+                               f"seed={wl['seed']}",
+                   "precision": a.precision, "cycles_timed": K, "diis_order": 5,
+                   "l2": "inputs larger than L2 (<ab|cd> 8.4 GB read every step)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e, "unit": "s/iter", "h2d_bytes_per_step": h2d // K,
+                "d2h_bytes_per_step": d2h // K,
+                "note": "PUTLST of all lists + xvcc_run(K cycles) + GETLST T2, wall clock / K"},
+        "roofline": roof,
+        "gpu_launches": int(cfg.launches_per_iter) * K,
+        "clocks": clk.summary(),
+        "energy": {"e_corr_after_cycles": e_split, "cycles": W + K},
+        "flops_per_iter": cfg.flops_per_iter,
+        "setup_seconds": cfg.seconds_setup,
+    }
+    if fp64:
+        line["fp64_gpu"] = fp64
+    if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
+        line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(a.workload, budget_s=90.0)
+    return line
+
+
+LADDER_TRAFFIC = {}  # filled from profiles/ once an ncu capture exists
+
+
+def accuracy(lib, wname, device):
+    """Split BF16x3 vs FP64 GPU on the convergent variant of the workload, both
+    converged to max|dT| < 1e-9 (CC_CONV=9): |dE| of the correlation energy."""
+    import torch
+    import acesb200 as ab
+    from acesb200.workloads import WORKLOADS
+    from acesb200.workloads import synthetic_df
+    wl = WORKLOADS[wname]
+    eps, B, irr = synthetic_df(**wl)
+    o, v = wl["nocc"], wl["nvir"]
+    lists = _lists_from_df(eps, B, o, v, torch.device("cuda", device))
+    lib.init(device)
+    lib.sym_init([o], [v])
+    put_lists(lib, eps, lists[1])
+    res = {}
+    for prec, name in ((ab.PREC_FP64, "fp64"), (ab.PREC_BF16X3, "bf16x3")):
+        c = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, precision=prec, allow_noconv=True)
+        res[name] = {"e_corr": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
+                     "seconds_per_iter": c.seconds_per_iter}
+    lib.fin()
+    return {"workload": f"{wname}: nocc={o}, nvir={v}, naux={wl['naux']}, seed={wl['seed']}, "
+                        f"B scaled by {wl['bscale']} (convergent variant)",
+            "fp64": res["fp64"], "bf16x3": res["bf16x3"],
+            "abs_dE": abs(res["bf16x3"]["e_corr"] - res["fp64"]["e_corr"]),
+            "speedup_per_iter": res["fp64"]["seconds_per_iter"] / res["bf16x3"]["seconds_per_iter"]}
+
+
+def cpu_baseline(wname, budget_s=90.0, steps=1):
+    """The oracle (FP64 numpy restatement of the reference) on the host cores:
+    one CCSD iteration of the same system; integral build excluded."""
+    import numpy as np
+    from acesb200.workloads import WORKLOADS
+    from oracle.hamiltonian import synthetic
+    from oracle import ccsd
+    wl = WORKLOADS[wname]
+    ham = synthetic(**wl)
+    B = ccsd.Blocks(ham)
+    t1, t2 = ccsd.mp2_guess(B)
+    times = []
+    t_start = time.perf_counter()
+    for k in range(max(1, steps)):
+        t0 = time.perf_counter()
+        t1n, t2n = ccsd.update(B, t1, t2)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    cores = os.cpu_count()
+    return {"value": min(times), "unit": "s/iter", "cores": cores, "kind": "port",
+            "sample": f"{len(times)} full CCSD iteration(s) of the {wname} system "
+                      f"(o={wl['nocc']}, v={wl['nvir']}) with oracle/ccsd.py (numpy FP64, "
+                      f"OpenBLAS threads = {cores}); integral build excluded",
+            "iterations": len(times)}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return None
+    from acesb200.workloads import WORKLOADS
+    from oracle.hamiltonian import synthetic
+    from oracle import ccsd
+    wl = WORKLOADS[a.workload]
+    ham = synthetic(**wl)
+    B = ccsd.Blocks(ham)
+    t1, t2 = ccsd.mp2_guess(B)
+    W = min(a.warmup, 1)
+    for _ in range(W):
+        t1, t2 = ccsd.update(B, t1, t2)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        t1, t2 = ccsd.update(B, t1, t2)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > 150.0:
+            break
+    v = statistics.mean(times)
+    cores = os.cpu_count()
+    return {
+        "impl": "reference",
+        "metric": "CCSD s/iter, synthetic closed-shell o=20 v=180 naux=600 (split BF16x3 vs FP64 GPU)",
+        "value": v, "unit": "s/iter", "n_gpus": world, "steps": len(times), "warmup": W,
+        "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded DF generator",
+        "config": {"workload": f"{a.workload}: RHF-CCSD, C1, nocc={wl['nocc']}, nvir={wl['nvir']}, "
+                               f"naux={wl['naux']}, seed={wl['seed']}",
+                   "note": "the reference (Fortran xvcc) cannot be compiled here (no Fortran "
+                           "compiler); this arm times its numpy FP64 restatement"},
+        "cpu_baseline": {"value": v, "unit": "s/iter", "cores": cores, "kind": "port",
+                         "sample": f"{len(times)} CCSD iterations of the {a.workload} system"},
+        "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------------ ranks
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+KERNEL_CASES = {
+    # particle-particle ladder shape Z(ab,ij) = W(ab,ef) tau(ef,ij) at v=120, o=20:
+    # M = K = v^2 = 14400, N = o^2 = 400; A (FP64 1.66 GB, split 0.83 GB) exceeds L2
+    "ladder-small": dict(m=14400, n=400, k=14400),
+}
+
+
+def run_kernel_case(a):
+    """One XGEMM of a ladder-like shape, FP64 inputs -> split -> tcgen05, then
+    the same shape in FP64 (DMMA); prints device times (CUDA events)."""
+    import torch
+    import acesb200 as ab
+    c = KERNEL_CASES[a.kernel_case]
+    m, n, k = c["m"], c["n"], c["k"]
+    lib = ab.load()
+    lib.init(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn((m, k), dtype=torch.float64, device="cuda", generator=g)   # column-major op(A)=A^T
+    B = torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g)
+    C = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+    out = {}
+    for prec, name in ((ab.PREC_BF16X3, "bf16x3"), (ab.PREC_FP64, "fp64")):
+        for rep in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            # C(m x n) = A^T(m x k) * B(k x n): column-major A stored (k x m) = our row-major (m,k)
+            lib.xgemm("T", "N", m, n, k, 1.0, A.data_ptr(), k, B.data_ptr(), k, 0.0,
+                      C.data_ptr(), m, precision=prec)
+            e1.record()
+            torch.cuda.synchronize()
+            out[name] = e0.elapsed_time(e1) * 1e-3
+    print(json.dumps({"kernel_case": a.kernel_case, "m": m, "n": n, "k": k,
+                      "seconds_including_split_pack": out}), flush=True)
+
+
+def main():
+    a = args()
+    if a.kernel_case:
+        run_kernel_case(a)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        line = run_reference(a, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        line = run_ours(a, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -145,7 +145,7 @@ typedef struct aces_cc_config {
   int triples;        /* 1: run (T) after CCSD (CALC=CCSD(T))                */
   int use_graph;      /* 1: capture one iteration in a CUDA graph             */
   int verbose;        /* 1: per-iteration log on stdout (IFLAGS(1))          */
-  int reserved;
+  int timing_warmup;  /* cycles excluded from the timing outputs             */
   /* outputs */
   double e_ccsd;      /* correlation energy of the final amplitudes          */
   double e_t4;        /* E[4]T                                               */
@@ -153,8 +153,13 @@ typedef struct aces_cc_config {
   double last_residual;
   int ncycle;
   int converged;
-  double seconds_per_iter;  /* device time per CCSD iteration (CUDA events)  */
-  double seconds_triples;
+  double seconds_per_iter;   /* mean device time of a timed cycle (CUDA events) */
+  double seconds_triples;    /* device time of (T)                           */
+  double seconds_ladder;     /* mean device time of the particle-particle ladder
+                                contraction in a timed cycle                 */
+  double flops_per_iter;     /* flops of all contractions of one cycle       */
+  long long launches_per_iter; /* kernels launched in one timed cycle        */
+  double seconds_setup;      /* device time reading lists and resorting integrals */
 } aces_cc_config;
 
 /* PROGRAM VCC (vcc/vcc.F:9): RHF CCSD (and (T) when cfg->triples).  Reads

@@ -110,44 +110,19 @@ def from_fixture(path):
     return ham
 
 
-def synthetic_factors(nocc, nvir, naux, seed, irreps=None):
-    """Seeded DF factors of the synthetic workloads.
-
-    Returns (eps, B, orbital irreps).  With ``irreps`` = number of irreps (8
-    for the batched D2h-style systems) orbitals are dealt into irreps
-    unevenly and each auxiliary function carries an irrep, with
-    B^L_pq = 0 unless irrep(p) ^ irrep(q) == irrep(L), which makes (pq|rs)
-    symmetry-consistent.
-    """
-    rng = np.random.default_rng(seed)
-    eo = np.sort(rng.uniform(-1.5, -0.3, nocc))
-    ev = np.sort(rng.uniform(0.2, 3.0, nvir))
-    nmo = nocc + nvir
-    B = rng.normal(0.0, 0.02, (naux, nmo, nmo))
-    B = 0.5 * (B + B.transpose(0, 2, 1))
-    if irreps and irreps > 1:
-        w = rng.uniform(0.5, 1.5, irreps)
-        w = w / w.sum()
-        occ_irr = rng.choice(irreps, nocc, p=w)
-        vir_irr = rng.choice(irreps, nvir, p=w)
-        orb_irr = np.concatenate([occ_irr, vir_irr])
-        aux_irr = rng.integers(0, irreps, naux)
-        mask = (orb_irr[:, None] ^ orb_irr[None, :])[None, :, :] == aux_irr[:, None, None]
-        B = B * mask
-        eps = np.concatenate([eo, ev])
-        # reference DPD orbital order: by irrep, energy order within an irrep
-        order_o = np.lexsort((eps[:nocc], occ_irr))
-        order_v = nocc + np.lexsort((eps[nocc:], vir_irr))
-        order = np.concatenate([order_o, order_v])
-        eps = eps[order]
-        orb_irr = orb_irr[order]
-        B = B[:, order][:, :, order]
-    else:
-        orb_irr = np.zeros(nmo, dtype=np.int64)
-        eps = np.concatenate([eo, ev])
-    return eps, B, orb_irr
+def synthetic_factors(nocc, nvir, naux, seed, irreps=None, bscale=1.0):
+    """Seeded DF factors of the synthetic workloads: the generator of the
+    engine's benchmark package (acesb200.workloads.synthetic_df), so the oracle
+    and the engine see bit-identical inputs."""
+    import os
+    import sys
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "aces-ii_b200")
+    if pkg not in sys.path:
+        sys.path.insert(0, pkg)
+    from acesb200.workloads import synthetic_df
+    return synthetic_df(nocc, nvir, naux, seed, irreps, bscale)
 
 
-def synthetic(nocc, nvir, naux, seed, irreps=None):
-    eps, B, irr = synthetic_factors(nocc, nvir, naux, seed, irreps)
+def synthetic(nocc, nvir, naux, seed, irreps=None, bscale=1.0):
+    eps, B, irr = synthetic_factors(nocc, nvir, naux, seed, irreps, bscale)
     return MOHamiltonian(nocc, np.diag(eps), irrep=irr, df=B, nirrep=irreps or 1)
