@@ -93,7 +93,15 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
                 long long ldb, double beta, const CView &C, bool constA, bool constB) {
   gemm_calls++;
   gemm_flops += 2.0 * M * N * (double)K;
-  bool split = prec == ACES_PREC_BF16X3 && (double)M * N * K >= 1.0e7 && K >= 16;
+  // matrix-vector products are bandwidth bound: FP64 GEMV
+  if (N == 1) return gemv_f64(M, K, alpha, A, lda, B, beta, C, false, st);
+  if (M == 1) return gemv_f64(N, K, alpha, B, ldb, A, beta, C, true, st);
+  // the tensor-core split path: every contraction with K >= 128 and both
+  // output dimensions >= 16 (a thin dimension such as nocc is padded to the
+  // 128-row tile: the BF16 tensor cores still beat FP64 FMA several-fold);
+  // K = nocc products (low-rank updates) stay on the FP64 kernels
+  bool split = prec == ACES_PREC_BF16X3 && M >= 16 && N >= 16 && K >= 128 &&
+               (double)M * N * K >= 1.0e8;
   if (!split) return gemm_nt_f64(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
   auto get = [&](const double *src, long long ld, int rows, bool cst, SplitOperand &tmp,
                  const SplitOperand **out) -> int {
@@ -824,6 +832,12 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   if (!converged) {
     set_error("CC equations did not converge in %d cycles", cfg->cc_maxcyc);
     return ACES_ERR_NOCONV;
+  }
+  if (cfg->triples) {
+    // (T) on the converged amplitudes (vcc/vcc.F:1215 -> trp/trps.F)
+    ACES_TRY(E.triples(&cfg->e_t4, &cfg->e_st5, &cfg->seconds_triples));
+    aces_putrec("E4T", 8, &cfg->e_t4);
+    aces_putrec("E5ST", 8, &cfg->e_st5);
   }
   return ACES_OK;
 }

@@ -71,6 +71,7 @@ class CCEngine {
   int iteration(int icycle, int exporder, double *e_out3, double *res, double *dres,
                 bool *extrap);
   int write_back();
+  int triples(double *e4, double *e5, double *seconds);   // (T), trp/trps2.F
   void release();
 
   // contraction dispatch (FP64 DMMA or BF16x3 tcgen05)
@@ -80,6 +81,8 @@ class CCEngine {
            std::initializer_list<PermTerm> terms);
   int copy(double *dst, const double *src, size_t n);
 };
+
+constexpr long long kHugeView = 1LL << 62;  // CView divisor meaning "no split"
 
 CCEngine *engine_instance(bool create);
 void engine_reset();

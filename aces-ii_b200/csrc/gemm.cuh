@@ -33,6 +33,15 @@ inline CView cview_colmajor(double *p, long long ldc) {
 int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long lda,
                 const double *B, long long ldb, double beta, const CView &C, cudaStream_t st);
 
+// FP64 matrix-vector product y = alpha * A x + beta * y written through C at
+// (m, 0) (or (0, m) when transpose_out).
+int gemv_f64(int M, int K, double alpha, const double *A, long long lda, const double *x,
+             double beta, const CView &C, bool transpose_out, cudaStream_t st);
+// split-K support shared by the contraction kernels
+double *splitk_workspace(size_t doubles);
+int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
+                  double beta, cudaStream_t st);
+
 // Split-precision operand: x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi),
 // stored K-contiguous and zero-padded to (rows_pad x k_pad).
 struct SplitOperand {
@@ -53,6 +62,11 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 // acc = A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (TMEM), C = alpha*acc + beta*C (FP64).
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st);
+
+// Rows [row0, row0 + rows) of a split operand (no copy).  The view's tensor
+// map ends at the parent's padded rows; rows past the view inside it belong
+// to the next slice and only reach output rows that callers discard.
+SplitOperand split_view(const SplitOperand &p, int row0, int rows);
 
 // Error code recorded by a tcgen05 kernel whose bounded wait expired (0 = ok);
 // reading it clears it.

@@ -5,6 +5,8 @@
 // Tile 128 x 128 x 16, 256 threads (8 warps as 2 x 4, each warp 64 x 32),
 // cp.async double buffering, padded shared-memory rows (20 doubles) so the
 // fragment loads of a half-warp hit 32 distinct banks.
+#include <algorithm>
+
 #include "common.cuh"
 #include "gemm.cuh"
 
@@ -65,7 +67,8 @@ __device__ __forceinline__ void load_stage(double *sA, double *sB, const double 
 template <int VEC>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_nt_f64(int M, int N, int K, double alpha, const double *__restrict__ A, long long lda,
-                  const double *__restrict__ B, long long ldb, double beta, CView C) {
+                  const double *__restrict__ B, long long ldb, double beta, CView C, int kchunk,
+                  double *__restrict__ part) {
   extern __shared__ double smem[];
   double *sA[2] = {smem, smem + kStageDoubles};
   double *sB[2] = {smem + BM * LDS, smem + kStageDoubles + BM * LDS};
@@ -79,15 +82,18 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  const int nk = (K + BK - 1) / BK;
-  load_stage<VEC>(sA[0], sB[0], A, lda, B, ldb, M, N, K, m0, n0, 0);
+  // split-K: blockIdx.z owns K range [kb, ke)
+  const int kb = blockIdx.z * kchunk;
+  const int ke = min(K, kb + kchunk);
+  const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+  if (nk > 0) load_stage<VEC>(sA[0], sB[0], A, lda, B, ldb, M, N, ke, m0, n0, kb);
   cp_commit();
   for (int kt = 0; kt < nk; ++kt) {
     cp_wait0();
     __syncthreads();
     if (kt + 1 < nk) {
-      load_stage<VEC>(sA[(kt + 1) & 1], sB[(kt + 1) & 1], A, lda, B, ldb, M, N, K, m0, n0,
-                      (kt + 1) * BK);
+      load_stage<VEC>(sA[(kt + 1) & 1], sB[(kt + 1) & 1], A, lda, B, ldb, M, N, ke, m0, n0,
+                      kb + (kt + 1) * BK);
       cp_commit();
     }
     const double *a_s = sA[kt & 1] + (wm * 64) * LDS;
@@ -105,6 +111,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
     __syncthreads();
+  }
+  if (part) {
+    // split-K partial: dense [z][M][N]
+    double *pz = part + (size_t)blockIdx.z * M * N;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      int m = m0 + wm * 64 + i * 8 + lr;
+      if (m >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int n = n0 + wn * 32 + j * 8 + lc * 2 + h;
+          if (n < N) pz[(size_t)m * N + n] = acc[i][j][h];
+        }
+    }
+    return;
   }
   // epilogue through the two-level output view
 #pragma unroll
@@ -128,11 +151,268 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 }  // namespace
 
+// C = alpha * sum_z part[z] + beta * C
+__global__ void k_splitk_reduce(CView C, const double *__restrict__ part, int M, int N, int Z,
+                                double alpha, double beta) {
+  long long total = (long long)M * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    int m = (int)(idx / N), n = (int)(idx % N);
+    double s = 0.0;
+    for (int z = 0; z < Z; ++z) s += part[(size_t)z * total + idx];
+    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
+                 (n % C.ndiv) * C.sn0;
+    double r = alpha * s;
+    if (beta != 0.0) r += beta * *cp;
+    *cp = r;
+  }
+}
+
+// y[m] = alpha * sum_k A[m*lda + k] x[k] + beta * y[m]; one warp per row
+__global__ void k_gemv_f64(int M, int K, double alpha, const double *__restrict__ A,
+                           long long lda, const double *__restrict__ x, double beta, CView C,
+                           bool transpose_out) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int m = warp; m < M; m += nwarps) {
+    const double *a = A + (long long)m * lda;
+    double s = 0.0;
+    for (int k = lane; k < K; k += 32) s += a[k] * __ldg(x + k);
+    for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+      int mm = transpose_out ? 0 : m, nn = transpose_out ? m : 0;
+      double *cp = C.p + (mm / C.mdiv) * C.sm1 + (mm % C.mdiv) * C.sm0 + (nn / C.ndiv) * C.sn1 +
+                   (nn % C.ndiv) * C.sn0;
+      double r = alpha * s;
+      if (beta != 0.0) r += beta * *cp;
+      *cp = r;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Thin contractions (one output dimension S <= 32): out(l, s) = sum_k X[l,k] Y[s,k]
+// with X the long operand (L rows) and Y the short one.  64 x 32 output tile
+// per block, K staged in 32-wide shared-memory chunks, 8 outputs per thread in
+// FP64 FMA; split-K over blockIdx.z.  Written to C(m,n) = out(l,s) or out(s,l).
+// These products stream their long operand once: bandwidth bound.
+// ---------------------------------------------------------------------------
+constexpr int TL = 64, TS = 32, TK = 32;
+
+__global__ void __launch_bounds__(256)
+    k_gemm_thin_f64(int L, int S, int K, double alpha, const double *__restrict__ X,
+                    long long ldx, const double *__restrict__ Y, long long ldy, double beta,
+                    CView C, bool s_is_m, int kchunk, double *__restrict__ part) {
+  __shared__ double Xs[TL][TK + 1];
+  __shared__ double Ys[TS][TK + 1];
+  const int l0 = blockIdx.x * TL;
+  const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+  const int t = threadIdx.x, r = t >> 3, c = t & 7;
+  double acc[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = kb; k0 < ke; k0 += TK) {
+    for (int e = t; e < TL * TK; e += 256) {
+      int rr = e / TK, kk = e % TK;
+      int l = l0 + rr, k = k0 + kk;
+      Xs[rr][kk] = (l < L && k < ke) ? X[(long long)l * ldx + k] : 0.0;
+    }
+    for (int e = t; e < TS * TK; e += 256) {
+      int rr = e / TK, kk = e % TK;
+      int k = k0 + kk;
+      Ys[rr][kk] = (rr < S && k < ke) ? Y[(long long)rr * ldy + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < TK; ++kk) {
+      double x0 = Xs[2 * r][kk], x1 = Xs[2 * r + 1][kk];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        double y = Ys[4 * c + j][kk];
+        acc[0][j] = fma(x0, y, acc[0][j]);
+        acc[1][j] = fma(x1, y, acc[1][j]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    int l = l0 + 2 * r + i;
+    if (l >= L) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int sidx = 4 * c + j;
+      if (sidx >= S) continue;
+      int m = s_is_m ? sidx : l, n = s_is_m ? l : sidx;
+      if (part) {
+        part[(size_t)blockIdx.z * (size_t)L * S + (size_t)l * S + sidx] = acc[i][j];
+        continue;
+      }
+      double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
+                   (n % C.ndiv) * C.sn0;
+      double v = alpha * acc[i][j];
+      if (beta != 0.0) v += beta * *cp;
+      *cp = v;
+    }
+  }
+}
+
+// reduce thin split-K partials part[z][l][s] into C
+__global__ void k_thin_reduce(CView C, const double *__restrict__ part, int L, int S, int Z,
+                              double alpha, double beta, bool s_is_m) {
+  long long total = (long long)L * S;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    int l = (int)(idx / S), sidx = (int)(idx % S);
+    double sum = 0.0;
+    for (int z = 0; z < Z; ++z) sum += part[(size_t)z * total + idx];
+    int m = s_is_m ? sidx : l, n = s_is_m ? l : sidx;
+    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
+                 (n % C.ndiv) * C.sn0;
+    double v = alpha * sum;
+    if (beta != 0.0) v += beta * *cp;
+    *cp = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Low-rank updates (K <= 32): C(m,n) = alpha sum_k A[m,k] B[n,k] + beta C(m,n).
+// Output bound: threads run along whichever output index has unit stride in
+// the view so the read-modify-write of C is coalesced; A/B rows are staged.
+// ---------------------------------------------------------------------------
+constexpr int LR_F = 64, LR_S = 8, LR_K = 32;
+
+__global__ void __launch_bounds__(256)
+    k_gemm_lowrank_f64(int M, int N, int K, double alpha, const double *__restrict__ A,
+                       long long lda, const double *__restrict__ B, long long ldb, double beta,
+                       CView C, bool fast_is_m) {
+  __shared__ double Fs[LR_F][LR_K + 1];
+  __shared__ double Ss[LR_S][LR_K + 1];
+  const int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
+  const double *Fp = fast_is_m ? A : B;
+  const double *Sp = fast_is_m ? B : A;
+  const long long ldf = fast_is_m ? lda : ldb, lds = fast_is_m ? ldb : lda;
+  const int tf = (nf + LR_F - 1) / LR_F;
+  const int f0 = (blockIdx.x % tf) * LR_F;
+  const int s0 = (blockIdx.x / tf) * LR_S;
+  for (int e = threadIdx.x; e < LR_F * LR_K; e += 256) {
+    int rr = e / LR_K, kk = e % LR_K;
+    Fs[rr][kk] = (f0 + rr < nf && kk < K) ? Fp[(long long)(f0 + rr) * ldf + kk] : 0.0;
+  }
+  for (int e = threadIdx.x; e < LR_S * LR_K; e += 256) {
+    int rr = e / LR_K, kk = e % LR_K;
+    Ss[rr][kk] = (s0 + rr < ns && kk < K) ? Sp[(long long)(s0 + rr) * lds + kk] : 0.0;
+  }
+  __syncthreads();
+  const int fl = threadIdx.x % LR_F, sl0 = threadIdx.x / LR_F;  // 64 x 4
+  for (int sl = sl0; sl < LR_S; sl += 4) {
+    int f = f0 + fl, sidx = s0 + sl;
+    if (f >= nf || sidx >= ns) continue;
+    double acc = 0.0;
+    for (int kk = 0; kk < K; ++kk) acc = fma(Fs[fl][kk], Ss[sl][kk], acc);
+    int m = fast_is_m ? f : sidx, n = fast_is_m ? sidx : f;
+    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
+                 (n % C.ndiv) * C.sn0;
+    double v = alpha * acc;
+    if (beta != 0.0) v += beta * *cp;
+    *cp = v;
+  }
+}
+
+double *splitk_workspace(size_t doubles) {
+  static double *ws = nullptr;
+  static size_t cap = 0;
+  if (doubles > cap) {
+    if (ws) cudaFree(ws);
+    ws = nullptr;
+    cap = 0;
+    if (cudaMalloc(&ws, doubles * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    cap = doubles;
+  }
+  return ws;
+}
+
+int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
+                  double beta, cudaStream_t st) {
+  long long total = (long long)M * N;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 16) nb = 148 * 16;
+  k_splitk_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+int gemv_f64(int M, int K, double alpha, const double *A, long long lda, const double *x,
+             double beta, const CView &C, bool transpose_out, cudaStream_t st) {
+  if (M <= 0) return ACES_OK;
+  long long warps = M;
+  long long nb = (warps * 32 + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_gemv_f64<<<(unsigned)nb, 256, 0, st>>>(M, K, alpha, A, lda, x, beta, C, transpose_out);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
 int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long lda,
                 const double *B, long long ldb, double beta, const CView &C, cudaStream_t st) {
   if (M <= 0 || N <= 0) return ACES_OK;
   if (K <= 0) {
     // C = beta*C: run with K = 0 is a scale; issue through the kernel with no k tiles
+  }
+  // K <= 32: output-bound low-rank update
+  if (K <= LR_K) {
+    const bool fast_is_m = C.sm0 == 1;  // run threads along the unit-stride output index
+    int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
+    long long nb = (long long)((nf + LR_F - 1) / LR_F) * ((ns + LR_S - 1) / LR_S);
+    k_gemm_lowrank_f64<<<(unsigned)nb, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                     fast_is_m);
+    count_launch();
+    ACES_CUDA(cudaGetLastError());
+    return ACES_OK;
+  }
+  // one output dimension <= 32: thin kernel over the long dimension
+  if (M <= TS || N <= TS) {
+    bool s_is_m = M <= TS && (M <= N);
+    int L = s_is_m ? N : M, S = s_is_m ? M : N;
+    const double *X = s_is_m ? B : A;
+    const double *Y = s_is_m ? A : B;
+    long long ldx = s_is_m ? ldb : lda, ldy = s_is_m ? lda : ldb;
+    long long lt = (L + TL - 1) / TL;
+    int Z = 1, kchunk = K;
+    double *part = nullptr;
+    if (lt < 592 && K >= 4 * TK) {
+      Z = (int)std::min<long long>((592 + lt - 1) / lt, K / (2 * TK));
+      if (Z > 1) {
+        kchunk = ((K + Z - 1) / Z + TK - 1) / TK * TK;
+        Z = (K + kchunk - 1) / kchunk;
+        part = splitk_workspace((size_t)Z * L * S);
+        if (!part) {
+          set_error("gemm thin: split-K workspace allocation failed");
+          return ACES_ERR_NOMEM;
+        }
+      }
+    }
+    dim3 g((unsigned)lt, 1, Z);
+    k_gemm_thin_f64<<<g, 256, 0, st>>>(L, S, K, alpha, X, ldx, Y, ldy, beta, C, s_is_m, kchunk,
+                                       Z > 1 ? part : nullptr);
+    count_launch();
+    ACES_CUDA(cudaGetLastError());
+    if (Z > 1) {
+      long long total = (long long)L * S;
+      long long nb = (total + 255) / 256;
+      if (nb > 148 * 16) nb = 148 * 16;
+      k_thin_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, L, S, Z, alpha, beta, s_is_m);
+      count_launch();
+      ACES_CUDA(cudaGetLastError());
+    }
+    return ACES_OK;
   }
   static bool attr_set = false;
   if (!attr_set) {
@@ -147,15 +427,39 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
     set_error("gemm_nt_f64: M=%d too large", M);
     return ACES_ERR_ARG;
   }
+  // split K when the output has too few tiles to fill the GPU
+  int Z = 1;
+  long long tiles = (long long)grid.x * grid.y;
+  int nkt = (K + BK - 1) / BK;
+  if (tiles < 148 && nkt >= 16) {
+    Z = (int)std::min<long long>((296 + tiles - 1) / tiles, nkt / 8);
+    if (Z < 1) Z = 1;
+  }
+  int kchunk = K;
+  double *part = nullptr;
+  if (Z > 1) {
+    kchunk = ((K + Z - 1) / Z + BK - 1) / BK * BK;
+    Z = (K + kchunk - 1) / kchunk;
+    part = splitk_workspace((size_t)Z * M * N);
+    if (!part) {
+      set_error("gemm_nt_f64: split-K workspace allocation failed");
+      return ACES_ERR_NOMEM;
+    }
+    grid.z = Z;
+  }
   bool vec2 = (lda % 2 == 0) && (ldb % 2 == 0) && (K % 2 == 0) &&
               ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
               ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+  if (kchunk % 2) vec2 = false;
   if (vec2)
-    k_gemm_nt_f64<2><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C);
+    k_gemm_nt_f64<2><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                         kchunk, part);
   else
-    k_gemm_nt_f64<1><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C);
+    k_gemm_nt_f64<1><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                         kchunk, part);
   count_launch();
   ACES_CUDA(cudaGetLastError());
+  if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st);
   return ACES_OK;
 }
 

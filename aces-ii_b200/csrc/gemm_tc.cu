@@ -18,6 +18,8 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "gemm.cuh"
 
@@ -179,7 +181,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                  int M, int N, int kTiles, double alpha, double beta, CView C) {
+                  int M, int N, int kTilesTotal, int ktc, double alpha, double beta, CView C,
+                  double *__restrict__ part) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -192,6 +195,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+  // split-K: blockIdx.z owns k tiles [ktb, ktb + kTiles)
+  const int ktb = blockIdx.z * ktc;
+  const int kTiles = max(0, min(ktc, kTilesTotal - ktb));
   const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
 
   if (threadIdx.x == 0) {
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t fb = smem_u32(&full[s]);
       unsigned char *st = smem + s * STAGE_BYTES;
       mbar_expect_tx(fb, STAGE_BYTES);
-      int kx = kt * TBK;
+      int kx = (ktb + kt) * TBK;
       tma_load_2d(smem_u32(st), &mAh, kx, m0, fb);
       tma_load_2d(smem_u32(st + TILE_A), &mAl, kx, m0, fb);
       tma_load_2d(smem_u32(st + 2 * TILE_A), &mBh, kx, n0, fb);
@@ -306,7 +312,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
     }
     const int m = m0 + row;
-    if (ok && m < M) {
+    if (ok && m < M && part) {
+      double *pz = part + (size_t)blockIdx.z * M * N + (size_t)m * N;
+#pragma unroll
+      for (int j = 0; j < 64; ++j) {
+        int n = n0 + half * 64 + j;
+        if (n < N) pz[n] = acc[j];
+      }
+    } else if (ok && m < M) {
       const long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
 #pragma unroll
       for (int j = 0; j < 64; ++j) {
@@ -371,8 +384,8 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st) {
   if (M <= 0 || N <= 0) return ACES_OK;
-  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad % TBM ||
-      B.rows_pad % TBN || A.k_pad == 0) {
+  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad < TBM ||
+      B.rows_pad < TBN || A.k_pad == 0) {
     set_error("gemm_nt_bf16x3: operand shapes do not match (%d/%d, %d, %d)", A.k_pad, B.k_pad,
               A.rows, B.rows);
     return ACES_ERR_ARG;
@@ -391,11 +404,42 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
   ACES_TRY(make_map(&mBh, B.hi, B.rows_pad, B.k_pad, TBN));
   ACES_TRY(make_map(&mBl, B.lo, B.rows_pad, B.k_pad, TBN));
   dim3 grid((N + TBN - 1) / TBN, (M + TBM - 1) / TBM);
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, A.k_pad / TBK,
-                                                     alpha, beta, C);
+  const int kTiles = A.k_pad / TBK;
+  // split K when the output has too few tiles to fill the 148 SMs
+  long long tiles = (long long)grid.x * grid.y;
+  int Z = 1, ktc = kTiles;
+  double *part = nullptr;
+  if (tiles < 148 && kTiles >= 8) {
+    Z = (int)std::min<long long>((148 + tiles - 1) / tiles, kTiles / 4);
+    if (Z > 1) {
+      ktc = (kTiles + Z - 1) / Z;
+      Z = (kTiles + ktc - 1) / ktc;
+      part = splitk_workspace((size_t)Z * M * N);
+      if (!part) {
+        set_error("gemm_nt_bf16x3: split-K workspace allocation failed");
+        return ACES_ERR_NOMEM;
+      }
+      grid.z = Z;
+    }
+  }
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, kTiles, ktc, alpha,
+                                                     beta, C, part);
   count_launch();
   ACES_CUDA(cudaGetLastError());
+  if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st);
   return ACES_OK;
+}
+
+SplitOperand split_view(const SplitOperand &p, int row0, int rows) {
+  SplitOperand v = p;
+  size_t off = (size_t)row0 * p.k_pad * 2;
+  v.hi = (char *)p.hi + off;
+  v.lo = (char *)p.lo + off;
+  v.rows = rows;
+  int rp = (rows + kSplitRowPad - 1) / kSplitRowPad * kSplitRowPad;
+  v.rows_pad = std::min(rp, p.rows_pad - row0);  // beyond it the tensor map zero-fills
+  v.cap = 0;
+  return v;
 }
 
 int tc_status_and_clear() {

@@ -208,11 +208,15 @@ def run_ours(a, rank, world, local_rank):
     t0 = time.perf_counter()
     lib.sym_init([o], [v])
     h2d = put_lists(lib, eps, lists)
+    tp = time.perf_counter()
     ce = lib.xvcc(cc_conv=30, cc_maxcyc=K, cc_exporder=5, precision=prec, allow_noconv=True)
+    tx = time.perf_counter()
     nr, nc = lib.list_dims(1, 46)
     t2 = lib.getlst(1, nc, 1, 46)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
+    e2e_parts = {"putlst_s": tp - t0, "xvcc_s": tx - tp, "xvcc_setup_s": ce.seconds_setup,
+                 "xvcc_cycles_device_s": ce.seconds_per_iter * K, "getlst_s": t1 - tx}
     barrier(world)
     e2e = max_over_ranks((t1 - t0) / K, world)
     d2h = t2.nbytes + 8
@@ -250,7 +254,8 @@ def run_ours(a, rank, world, local_rank):
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "e2e": {"value": e2e, "unit": "s/iter", "h2d_bytes_per_step": h2d // K,
                 "d2h_bytes_per_step": d2h // K,
-                "note": "PUTLST of all lists + xvcc_run(K cycles) + GETLST T2, wall clock / K"},
+                "note": "PUTLST of all lists + xvcc_run(K cycles) + GETLST T2, wall clock / K",
+                "parts": e2e_parts},
         "roofline": roof,
         "gpu_launches": int(cfg.launches_per_iter) * K,
         "clocks": clk.summary(),
