@@ -36,8 +36,8 @@ SYMBOLS = [
     "aces_isymoff", "aces_dirprd", "aces_list_touch", "aces_updmoi", "aces_inipck",
     "aces_isytyp", "aces_list_dims", "aces_getlst", "aces_putlst", "aces_getlst_dev",
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
-    "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "xvcc_run", "xlambda_run",
-    "xdens_1pdm",
+    "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
+    "xvcc_run", "xlambda_run", "xdens_1pdm",
 ]
 
 
@@ -90,6 +90,9 @@ class Lib:
         h.aces_xgemm.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
                                  C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double,
                                  C.c_void_p, C.c_int, C.c_int]
+        h.aces_xgemm_static.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int,
+                                        C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                        C.c_double, C.c_void_p, C.c_int]
         for fn in ("xvcc_run", "xlambda_run", "xdens_1pdm"):
             getattr(h, fn).argtypes = [C.POINTER(CCConfig)]
 
@@ -183,6 +186,14 @@ class Lib:
         self._chk("aces_xgemm", self.h.aces_xgemm(transa.encode(), transb.encode(), m, n, k,
                                                   alpha, A_ptr, lda, B_ptr, ldb, beta, C_ptr,
                                                   ldc, precision))
+
+    def xgemm_static(self, transa, transb, m, n, k, alpha, A_ptr, lda, B_ptr, ldb, beta, C_ptr,
+                     ldc):
+        """FP64 XGEMM that allocates no device memory (static scratch); see
+        aces_xgemm_static in include/aces_b200.h."""
+        self._chk("aces_xgemm_static",
+                  self.h.aces_xgemm_static(transa.encode(), transb.encode(), m, n, k, alpha,
+                                           A_ptr, lda, B_ptr, ldb, beta, C_ptr, ldc))
 
     # ---- programs -----------------------------------------------------------------
     def _run(self, fn, cfg, allow_noconv=False):

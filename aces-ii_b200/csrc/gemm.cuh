@@ -37,6 +37,11 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
 // (m, 0) (or (0, m) when transpose_out).
 int gemv_f64(int M, int K, double alpha, const double *A, long long lda, const double *x,
              double beta, const CView &C, bool transpose_out, cudaStream_t st);
+// gemm_nt_f64 with all scratch (split-K partials) taken from `ws` (capacity
+// `cap` doubles); allocates nothing.
+int gemm_nt_f64_scratch(int M, int N, int K, double alpha, const double *A, long long lda,
+                        const double *B, long long ldb, double beta, const CView &C,
+                        double *ws, size_t cap, cudaStream_t st);
 // split-K support shared by the contraction kernels
 double *splitk_workspace(size_t doubles);
 int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,

@@ -464,3 +464,100 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
 }
 
 }  // namespace acesb200
+
+namespace acesb200 {
+
+// The same FP64 contraction dispatch as gemm_nt_f64, with every scratch
+// buffer taken from caller-provided device memory `ws` (capacity `cap`
+// doubles) instead of the library's allocated workspace.  Split-K is reduced
+// to what fits; when even the unsplit form needs no scratch it runs unsplit.
+int gemm_nt_f64_scratch(int M, int N, int K, double alpha, const double *A, long long lda,
+                        const double *B, long long ldb, double beta, const CView &C,
+                        double *ws, size_t cap, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return ACES_OK;
+  if (K <= LR_K) {
+    const bool fast_is_m = C.sm0 == 1;
+    int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
+    long long nb = (long long)((nf + LR_F - 1) / LR_F) * ((ns + LR_S - 1) / LR_S);
+    k_gemm_lowrank_f64<<<(unsigned)nb, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                     fast_is_m);
+    count_launch();
+    ACES_CUDA(cudaGetLastError());
+    return ACES_OK;
+  }
+  if (M <= TS || N <= TS) {
+    bool s_is_m = M <= TS && (M <= N);
+    int L = s_is_m ? N : M, S = s_is_m ? M : N;
+    const double *X = s_is_m ? B : A;
+    const double *Y = s_is_m ? A : B;
+    long long ldx = s_is_m ? ldb : lda, ldy = s_is_m ? lda : ldb;
+    long long lt = (L + TL - 1) / TL;
+    int Z = 1, kchunk = K;
+    if (lt < 592 && K >= 4 * TK) {
+      long long zfit = (long long)(cap / ((size_t)L * S));
+      Z = (int)std::min<long long>(std::min<long long>((592 + lt - 1) / lt, K / (2 * TK)), zfit);
+      if (Z > 1) {
+        kchunk = ((K + Z - 1) / Z + TK - 1) / TK * TK;
+        Z = (K + kchunk - 1) / kchunk;
+      } else {
+        Z = 1;
+        kchunk = K;
+      }
+    }
+    dim3 g((unsigned)lt, 1, Z);
+    k_gemm_thin_f64<<<g, 256, 0, st>>>(L, S, K, alpha, X, ldx, Y, ldy, beta, C, s_is_m, kchunk,
+                                       Z > 1 ? ws : nullptr);
+    count_launch();
+    ACES_CUDA(cudaGetLastError());
+    if (Z > 1) {
+      long long total = (long long)L * S;
+      long long nb = (total + 255) / 256;
+      if (nb > 148 * 16) nb = 148 * 16;
+      k_thin_reduce<<<(unsigned)nb, 256, 0, st>>>(C, ws, L, S, Z, alpha, beta, s_is_m);
+      count_launch();
+      ACES_CUDA(cudaGetLastError());
+    }
+    return ACES_OK;
+  }
+  ACES_CUDA(cudaFuncSetAttribute(k_gemm_nt_f64<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSmemBytes));
+  ACES_CUDA(cudaFuncSetAttribute(k_gemm_nt_f64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSmemBytes));
+  dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  if (grid.y > 65535) {
+    set_error("gemm_nt_f64_scratch: M=%d too large", M);
+    return ACES_ERR_ARG;
+  }
+  int Z = 1;
+  long long tiles = (long long)grid.x * grid.y;
+  int nkt = (K + BK - 1) / BK;
+  if (tiles < 148 && nkt >= 16) {
+    long long zfit = (long long)(cap / ((size_t)M * N));
+    Z = (int)std::min<long long>(std::min<long long>((296 + tiles - 1) / tiles, nkt / 8), zfit);
+    if (Z < 1) Z = 1;
+  }
+  int kchunk = K;
+  double *part = nullptr;
+  if (Z > 1) {
+    kchunk = ((K + Z - 1) / Z + BK - 1) / BK * BK;
+    Z = (K + kchunk - 1) / kchunk;
+    part = ws;
+    grid.z = Z;
+  }
+  bool vec2 = (lda % 2 == 0) && (ldb % 2 == 0) && (K % 2 == 0) &&
+              ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
+              ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+  if (kchunk % 2) vec2 = false;
+  if (vec2)
+    k_gemm_nt_f64<2><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                         kchunk, part);
+  else
+    k_gemm_nt_f64<1><<<grid, kThreads, kSmemBytes, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                         kchunk, part);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st);
+  return ACES_OK;
+}
+
+}  // namespace acesb200

@@ -125,6 +125,21 @@ int aces_xgemm(char transa, char transb, int m, int n, int k, double alpha, cons
                int lda, const double *B, int ldb, double beta, double *Cmat, int ldc,
                int precision);
 
+/* The same FP64 product for callers that cannot allocate device memory (no
+ * counterpart in the reference): hosts that gave all device memory to their
+ * own allocator at start-up, or callers that must not pay an allocation's
+ * implicit synchronisation.  It calls no cudaMalloc/cudaFree and no
+ * allocating library routine: its scratch (m*k doubles when transa = 'N',
+ * n*k when transb = 'T', plus optional split-K partials) comes from one
+ * static device array of 2^20 doubles (8 MiB) that every GPU loading the
+ * library holds until exit; larger requests return ACES_ERR_ARG.  The array's
+ * device address is looked up on the first call on each device (call it once
+ * before any stream capture).  Calls share the array: calls that overlap on
+ * the GPU race.  FP64 only; synchronous on the current device. */
+int aces_xgemm_static(char transa, char transb, int m, int n, int k, double alpha,
+                      const double *A, int lda, const double *B, int ldb, double beta,
+                      double *Cmat, int ldc);
+
 /* ---- member programs ---------------------------------------------------- */
 
 /* Precision of the tensor contractions. */
