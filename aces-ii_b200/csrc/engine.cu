@@ -18,14 +18,24 @@ static const long long kHuge = 1LL << 62;
 
 CCEngine::~CCEngine() { release(); }
 
+std::vector<DBuf *> CCEngine::registry() {
+  return {&eo, &ev, &foo, &fvv, &fov, &offo, &offv, &fovT, &I_oooo, &I_ooov, &I_oovv,
+          &I_ovov, &I_ovvv, &I_vvvv, &L_oovv, &LF, &LovP, &LooP, &LmeP, &I1, &I2, &IvP,
+          &IvP2, &IX, &IX2, &WA0, &WB0, &IoP3, &IvT, &IvT2, &IooT, &LT1, &X, &Xn, &Z1,
+          &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
+          &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
+          &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec, &L, &Ln, &gE,
+          &lrhs, &bwdA, &bwdB, &bwdC, &bwdD};
+}
+
 void CCEngine::release() {
-  DBuf *all[] = {&eo, &ev, &foo, &fvv, &fov, &offo, &offv, &fovT, &I_oooo, &I_ooov, &I_oovv,
-                 &I_ovov, &I_ovvv, &I_vvvv, &L_oovv, &LF, &LovP, &LooP, &LmeP, &I1, &I2, &IvP,
-                 &IvP2, &IX, &IX2, &WA0, &WB0, &IoP3, &IvT, &IvT2, &IooT, &LT1, &X, &Xn, &Z1,
-                 &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
-                 &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
-                 &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec};
-  for (DBuf *b : all) {
+  for (auto &kv : adjoint) if (kv.second.p) cudaFree(kv.second.p);
+  adjoint.clear();
+  for (auto &kv : tcache) if (kv.second.p) cudaFree(kv.second.p);
+  tcache.clear();
+  tape.clear();
+  active.clear();
+  for (DBuf *b : registry()) {
     if (b->p) cudaFree(b->p);
     b->p = nullptr;
     b->n = 0;
@@ -66,7 +76,32 @@ int CCEngine::alloc(DBuf &b, size_t n) {
 }
 
 int CCEngine::copy(double *dst, const double *src, size_t n) {
+  if (recording) {
+    TapeOp op;
+    op.kind = TapeOp::COPY;
+    op.dst = dst;
+    op.src = src;
+    op.count = n;
+    if (is_active(src)) mark_active(dst);
+    tape.push_back(op);
+  }
   if (n) ACES_CUDA(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, st));
+  return ACES_OK;
+}
+
+int CCEngine::tau_op(double *out, const double *t2v, const double *t1v, double c) {
+  if (recording) {
+    TapeOp op;
+    op.kind = TapeOp::TAU;
+    op.tau = out;
+    op.t2 = t2v;
+    op.t1 = t1v;
+    op.c = c;
+    mark_active(out);
+    tape.push_back(op);
+  }
+  launch_tau(out, t2v, t1v, c, o, v, st);
+  ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
 
@@ -77,6 +112,19 @@ int CCEngine::perm(double *out, int n0, int n1, int n2, int n3, double beta,
   s.nterms = 0;
   s.beta = beta;
   for (const PermTerm &t : terms) s.t[s.nterms++] = t;
+  if (recording) {
+    TapeOp op;
+    op.kind = TapeOp::PERM;
+    op.out = out;
+    op.spec = s;
+    bool any = beta != 0.0 && is_active(out);
+    for (int t = 0; t < s.nterms; ++t) {
+      op.t_act[t] = is_active(s.t[t].src);
+      any = any || op.t_act[t];
+    }
+    if (any) mark_active(out);
+    tape.push_back(op);
+  }
   return permute(out, s, st);
 }
 
@@ -93,6 +141,19 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
                 long long ldb, double beta, const CView &C, bool constA, bool constB) {
   gemm_calls++;
   gemm_flops += 2.0 * M * N * (double)K;
+  if (recording) {
+    TapeOp op;
+    op.kind = TapeOp::GEMM;
+    op.M = M; op.N = N; op.K = K;
+    op.alpha = alpha; op.beta = beta;
+    op.A = A; op.B = B; op.lda = lda; op.ldb = ldb;
+    op.C = C;
+    op.a_act = is_active(A);
+    op.b_act = is_active(B);
+    op.c_act = is_active(C.p);
+    if (op.a_act || op.b_act) mark_active(C.p);
+    tape.push_back(op);
+  }
   // matrix-vector products are bandwidth bound: FP64 GEMV
   if (N == 1) return gemv_f64(M, K, alpha, A, lda, B, beta, C, false, st);
   if (M == 1) return gemv_f64(N, K, alpha, B, ldb, A, beta, C, true, st);
@@ -474,8 +535,8 @@ int CCEngine::residual() {
   // t1T[a,m]
   ACES_TRY(perm(t1T.p, 1, 1, v, o, 0.0, {PT(T1, 1.0, 0, 0, 1, V)}));
   // FTAU (libr/ftau.f)
-  launch_tau(tau.p, T2, T1, 1.0, o, v, st);
-  launch_tau(taut.p, T2, T1, 0.5, o, v, st);
+  ACES_TRY(tau_op(tau.p, T2, T1, 1.0));
+  ACES_TRY(tau_op(taut.p, T2, T1, 0.5));
   // ---- F(ae): QUAD3 + T1RING (vcc/quad3.f, libr/t1ring.F) ----
   ACES_TRY(copy(Fae.p, offv.p, VV));
   ACES_TRY(G(v, v, o, -0.5, t1T.p, O, fovT.p, O, 1.0, cview_rowmajor(Fae.p, V)));
@@ -559,10 +620,9 @@ int CCEngine::residual() {
   ACES_TRY(perm(XnP.p, o, v, o, v, 0.0, {PT(T2, 0.5, st2[0], st2[3], st2[1], st2[2])}));
   // + t1[j,f] t1[n,b]: rank-1 per (j,b,n,f) -> GEMM over a unit K: A[(j),f]... use outer product
   {
-    // XnP[(j,b),(n,f)] += t1[j,f] t1[n,b] : as C[(j,n,f? )] is awkward; do it as K=1 products
-    // C[m=(j,f), n=(n,b)] = t1[j,f] * t1[n,b] mapped to XnP[j,b,n,f]
+    // XnP[j,b,n,f] += t1[j,f] t1[n,b]: a K = 1 product C[(j,f),(n,b)] written through the view
     CView vx{XnP.p, V, OVV, 1, V, V, OV};
-    ACES_TRY(gemm_nt_f64(o * v, o * v, 1, 1.0, T1, 1, T1, 1, 1.0, vx, st));
+    ACES_TRY(G(o * v, o * v, 1, 1.0, T1, 1, T1, 1, 1.0, vx));
   }
   ACES_TRY(perm(Y1.p, o, v, o, v, 0.0,
                 {PT(Y2.p, 1.0, OVV, OV, V, 1), PT(XnP.p, -1.0, OVV, OV, V, 1)}));
@@ -613,12 +673,22 @@ int CCEngine::residual() {
 
 // One CC cycle: residual, Jacobi update, energy, DIIS (vcc/vcc.F:797-1087).
 int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, double *dres,
-                        bool *extrap) {
+                        bool *extrap, bool lambda) {
   const long long len = (long long)o * v + (long long)o * o * v * v;
-  ACES_TRY(residual());
-  launch_newt(t2n(), Z2.p, t1n(), Z1.p, eo.p, ev.p, o, v, st);
+  const long long ov = (long long)o * v;
   double *d = dev_small.p;  // [0..2] energy, [3] res, [4] dres, [8..32] dots, [40..64] coef
-  launch_energy(d, t2n(), t1n(), I_oovv.p, fov.p, o, v, scratch.p, st);
+  double *cur = lambda ? L.p : X.p;
+  double *nxt = lambda ? Ln.p : Xn.p;
+  if (!lambda) {
+    ACES_TRY(residual());
+    launch_newt(t2n(), Z2.p, t1n(), Z1.p, eo.p, ev.p, o, v, st);
+    launch_energy(d, t2n(), t1n(), I_oovv.p, fov.p, o, v, scratch.p, st);
+  } else {
+    // Lambda: new multipliers = (dE/dT + (dZ/dT)^T lambda) / D
+    ACES_TRY(lambda_rhs());
+    launch_newt(Ln.p + ov, lrhs.p + ov, Ln.p, lrhs.p, eo.p, ev.p, o, v, st);
+    ACES_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(double), st));
+  }
   int ndimr = icycle < exporder ? icycle : exporder;
   int idimr = (icycle - 1) % exporder;
   if ((int)hx.size() < exporder) {
@@ -629,8 +699,8 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
     ACES_TRY(alloc(hx[idimr], len));
     ACES_TRY(alloc(he[idimr], len));
   }
-  ACES_TRY(copy(hx[idimr].p, X.p, len));
-  launch_diff(he[idimr].p, Xn.p, X.p, len, st);
+  ACES_TRY(copy(hx[idimr].p, cur, len));
+  launch_diff(he[idimr].p, nxt, cur, len, st);
   launch_absmax(d + 3, he[idimr].p, o, v, scratch.p, st);
   std::vector<const double *> hp(ndimr);
   for (int k = 0; k < ndimr; ++k) hp[k] = he[k].p;
@@ -678,49 +748,52 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
 }
 
 // accept the new amplitudes: extrapolated (DIIS) or plain Jacobi (DRMOVE)
-static int accept(CCEngine &E, bool extrap, int ndimr) {
+int accept_update(CCEngine &E, bool extrap, int ndimr, bool lambda) {
   const long long len = (long long)E.o * E.v + (long long)E.o * E.o * E.v * E.v;
+  double *cur = lambda ? E.L.p : E.X.p;
+  double *nxt = lambda ? E.Ln.p : E.Xn.p;
   if (extrap) {
     std::vector<const double *> px(ndimr);
     for (int k = 0; k < ndimr; ++k) px[k] = E.hx[k].p;
-    launch_lincomb(E.X.p, E.dvec.p, E.dev_small.p + 40, px.data(), ndimr, len, E.st);
+    launch_lincomb(cur, E.dvec.p, E.dev_small.p + 40, px.data(), ndimr, len, E.st);
   } else {
-    ACES_TRY(E.copy(E.X.p, E.Xn.p, len));
+    ACES_TRY(E.copy(cur, nxt, len));
   }
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
 
-int CCEngine::write_back() {
+int CCEngine::write_amplitudes(const double *a1, const double *a2, int list1, int list2ab,
+                               int list2aa) {
   const long long O = o, V = v;
   const SymInfo &s = state().sym;
-  // T2(AB) -> list 46 (13,14): dense [a,b,i,j] = t2[i,j,a,b]
-  DBuf tmp;
-  ACES_TRY(alloc(tmp, O * O * V * V));
+  // doubles (AB) -> list2ab (13,14): dense [a,b,i,j] = a2[i,j,a,b]
+  DBuf tmpb;
+  ACES_TRY(alloc(tmpb, O * O * V * V));
   const long long st2[4] = {O * V * V, V * V, V, 1};
-  ACES_TRY(perm(tmp.p, v, v, o, o, 0.0, {PT(t2(), 1.0, st2[2], st2[3], st2[0], st2[1])}));
+  ACES_TRY(perm(tmpb.p, v, v, o, o, 0.0, {PT(a2, 1.0, st2[2], st2[3], st2[0], st2[1])}));
   {
     DevMap dm;
-    ACES_TRY(make_map(dm, 46, 13, 14, irr_o, irr_v, true));
-    launch_scatter(tmp.p, dm.m, st);
+    ACES_TRY(make_map(dm, list2ab, 13, 14, irr_o, irr_v, true));
+    launch_scatter(tmpb.p, dm.m, st);
     ACES_CUDA(cudaStreamSynchronize(st));
   }
-  // T2(AA) -> list 44 (1,3): dense [a,b,i,j] = t2[i,j,a,b] - t2[i,j,b,a]
-  ACES_TRY(perm(tmp.p, v, v, o, o, 0.0,
-                {PT(t2(), 1.0, st2[2], st2[3], st2[0], st2[1]),
-                 PT(t2(), -1.0, st2[3], st2[2], st2[0], st2[1])}));
+  // same-spin doubles -> list2aa (1,3): dense [a,b,i,j] = a2[i,j,a,b] - a2[i,j,b,a]
+  ACES_TRY(perm(tmpb.p, v, v, o, o, 0.0,
+                {PT(a2, 1.0, st2[2], st2[3], st2[0], st2[1]),
+                 PT(a2, -1.0, st2[3], st2[2], st2[0], st2[1])}));
   {
     DevMap dm;
-    ACES_TRY(make_map(dm, 44, 1, 3, irr_o, irr_v, true));
-    launch_scatter(tmp.p, dm.m, st);
+    ACES_TRY(make_map(dm, list2aa, 1, 3, irr_o, irr_v, true));
+    launch_scatter(tmpb.p, dm.m, st);
     ACES_CUDA(cudaStreamSynchronize(st));
   }
-  // T1 -> list 90 irrep 1, a single column over (a,i) pairs of type 9
+  // singles -> list1 irrep 1, one column over (a,i) pairs of type 9
   {
     int n9 = s.irpdpd[0][8];
-    ACES_TRY(aces_list_touch(1, n9, 1, 90, 0));
+    ACES_TRY(aces_list_touch(1, n9, 1, list1, 0));
     std::vector<double> h1((size_t)o * v), col((size_t)n9, 0.0);
-    ACES_CUDA(cudaMemcpy(h1.data(), t1(), h1.size() * 8, cudaMemcpyDeviceToHost));
+    ACES_CUDA(cudaMemcpy(h1.data(), a1, h1.size() * 8, cudaMemcpyDeviceToHost));
     std::vector<int> lo(o), lv(v);
     int cnt[8] = {0};
     for (int i = 0; i < o; ++i) lo[i] = cnt[irr_o[i]]++;
@@ -730,11 +803,14 @@ int CCEngine::write_back() {
       for (int a = 0; a < v; ++a)
         if (irr_o[i] == irr_v[a])
           col[pair_index(s, 9, irr_v[a], lv[a], irr_o[i], lo[i])] = h1[(size_t)i * v + a];
-    ACES_TRY(aces_putlst(col.data(), 1, 1, 1, 90));
+    ACES_TRY(aces_putlst(col.data(), 1, 1, 1, list1));
   }
-  cudaFree(tmp.p);
+  cudaFree(tmpb.p);
   return ACES_OK;
 }
+
+// T1 -> list 90, T2(AB) -> list 46, T2(AA) -> list 44 (vcc/vcc.F list map)
+int CCEngine::write_back() { return write_amplitudes(t1(), t2(), 90, 46, 44); }
 
 static CCEngine *g_engine = nullptr;
 CCEngine *engine_instance(bool create) {
@@ -791,7 +867,7 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
     cfg->flops_per_iter = E.gemm_flops;
     int ndimr = icycle < cfg->cc_exporder ? icycle : cfg->cc_exporder;
     bool conv = std::fabs(res) < tol;
-    if (!conv) ACES_TRY(accept(E, extrap, ndimr));
+    if (!conv) ACES_TRY(accept_update(E, extrap, ndimr, false));
     ACES_CUDA(cudaEventRecord(ev1, E.st));
     ACES_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f, msl = 0.f;
@@ -829,6 +905,8 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   cudaEventDestroy(ev1);
   ACES_TRY(E.write_back());
   aces_putrec("CCSDENRG", 8, &cfg->e_ccsd);
+  E.have_amplitudes = converged;
+  E.have_lambda = false;
   if (!converged) {
     set_error("CC equations did not converge in %d cycles", cfg->cc_maxcyc);
     return ACES_ERR_NOCONV;

@@ -3,8 +3,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "common.cuh"
 #include "gemm.cuh"
 #include "kernels.cuh"
@@ -57,6 +59,31 @@ class CCEngine {
   std::vector<SplitEntry> split_cache;
   SplitOperand split_tmpA, split_tmpB;
 
+  // Lambda (adjoint) state: lambda = [l1 | l2] like X, dE/dT, tape
+  DBuf L, Ln, gE, lrhs;
+  bool have_amplitudes = false, have_lambda = false;
+  std::vector<TapeOp> tape;
+  bool recording = false;
+  std::vector<DBuf *> active;
+  std::map<DBuf *, DBuf> adjoint;
+  std::map<const double *, DBuf> tcache;     // transposes of constant operands
+  std::vector<const double *> symmetric;     // constant matrices equal to their transpose
+  DBuf bwdA, bwdB, bwdC, bwdD;
+  std::vector<DBuf *> registry();
+  DBuf *owner(const void *p);
+  bool is_active(const void *p);
+  void mark_active(const void *p);
+  double *adj(const void *p);
+  int tmp(DBuf &b, size_t n);
+  const double *transposed(const double *src, int rows, int cols, long long ld, bool cst,
+                           DBuf &scratch);
+  int backward();
+  void zero_adjoints();
+  int record_residual(bool fock_active);
+  int tau_op(double *out, const double *t2, const double *t1, double c);
+  int lambda_rhs();
+  int density(std::vector<double> &D);
+
   // statistics
   long long gemm_calls = 0;
   double gemm_flops = 0.0;
@@ -69,8 +96,9 @@ class CCEngine {
   int mp2_guess();
   int residual();   // Z1, Z2 from X
   int iteration(int icycle, int exporder, double *e_out3, double *res, double *dres,
-                bool *extrap);
+                bool *extrap, bool lambda = false);
   int write_back();
+  int write_amplitudes(const double *a1, const double *a2, int list1, int list2ab, int list2aa);
   int triples(double *e4, double *e5, double *seconds);   // (T), trp/trps2.F
   void release();
 
@@ -84,6 +112,7 @@ class CCEngine {
 
 constexpr long long kHugeView = 1LL << 62;  // CView divisor meaning "no split"
 
+int accept_update(CCEngine &E, bool extrap, int ndimr, bool lambda);
 CCEngine *engine_instance(bool create);
 void engine_reset();
 

@@ -291,15 +291,20 @@ def accuracy(lib, wname, device):
     put_lists(lib, eps, lists[1])
     res = {}
     for prec, name in ((ab.PREC_FP64, "fp64"), (ab.PREC_BF16X3, "bf16x3")):
-        c = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, precision=prec, allow_noconv=True)
+        c = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, precision=prec, allow_noconv=True,
+                     triples=1)
         res[name] = {"e_corr": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
-                     "seconds_per_iter": c.seconds_per_iter}
+                     "seconds_per_iter": c.seconds_per_iter, "e_t4": c.e_t4, "e_st5": c.e_st5,
+                     "seconds_triples": c.seconds_triples}
     lib.fin()
     return {"workload": f"{wname}: nocc={o}, nvir={v}, naux={wl['naux']}, seed={wl['seed']}, "
                         f"B scaled by {wl['bscale']} (convergent variant)",
             "fp64": res["fp64"], "bf16x3": res["bf16x3"],
             "abs_dE": abs(res["bf16x3"]["e_corr"] - res["fp64"]["e_corr"]),
-            "speedup_per_iter": res["fp64"]["seconds_per_iter"] / res["bf16x3"]["seconds_per_iter"]}
+            "abs_dE_T": abs(res["bf16x3"]["e_t4"] + res["bf16x3"]["e_st5"]
+                            - res["fp64"]["e_t4"] - res["fp64"]["e_st5"]),
+            "speedup_per_iter": res["fp64"]["seconds_per_iter"] / res["bf16x3"]["seconds_per_iter"],
+            "speedup_triples": res["fp64"]["seconds_triples"] / res["bf16x3"]["seconds_triples"]}
 
 
 def cpu_baseline(wname, budget_s=90.0, steps=1):

@@ -23,14 +23,36 @@ import numpy as np
 from .diis import ReferenceDIIS
 
 
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
 def _ct(spec, a, b):
+    if _is_torch(a) or _is_torch(b):
+        import torch
+        return torch.einsum(spec, a, b)
     return np.einsum(spec, a, b, optimize=True)
+
+
+def _tr(x, *axes):
+    return x.permute(*axes) if _is_torch(x) else x.transpose(*axes)
+
+
+def _diag(x):
+    if _is_torch(x):
+        import torch
+        return torch.diag(x)
+    return np.diag(x)
+
+
+def _copy(x):
+    return x.clone() if _is_torch(x) else x.copy()
 
 
 def _P(x):
     """P(ia,jb) X = X_ijab + X_jiba: the permutation that RHF spin adaptation
     reduces P(ij)P(ab) to for the alpha-beta block."""
-    return x + x.transpose(1, 0, 3, 2)
+    return x + _tr(x, 1, 0, 3, 2)
 
 
 class Blocks:
@@ -67,7 +89,7 @@ def mp2_guess(B):
 
 def tau(t1, t2, fac=1.0):
     """FTAU (libr/ftau.f): tau(ab,ij) = t2 + fac * t1(ai) t1(bj) (AB spin case)."""
-    return t2 + fac * np.einsum("ia,jb->ijab", t1, t1)
+    return t2 + fac * _ct("ia,jb->ijab", t1, t1)
 
 
 def energy(B, t1, t2):
@@ -88,11 +110,11 @@ def intermediates(B, t1, t2):
     o, v = B.o, B.v
     taut = tau(t1, t2, 0.5)
     tt = tau(t1, t2)
-    L_oovv = 2.0 * B.oovv - B.oovv.transpose(0, 1, 3, 2)      # 2<mn|ef>-<mn|fe>
-    L_ovvv = 2.0 * B.ovvv - B.ovvv.transpose(0, 1, 3, 2)      # L[m,a,f,e] = 2<ma|fe>-<ma|ef>
-    L_ooov = 2.0 * B.ooov - B.ooov.transpose(1, 0, 2, 3)      # 2<mn|ie>-<nm|ie>
-    offv = B.fvv - np.diag(B.ev)
-    offo = B.foo - np.diag(B.eo)
+    L_oovv = 2.0 * B.oovv - _tr(B.oovv, 0, 1, 3, 2)      # 2<mn|ef>-<mn|fe>
+    L_ovvv = 2.0 * B.ovvv - _tr(B.ovvv, 0, 1, 3, 2)      # L[m,a,f,e] = 2<ma|fe>-<ma|ef>
+    L_ooov = 2.0 * B.ooov - _tr(B.ooov, 1, 0, 2, 3)      # 2<mn|ie>-<nm|ie>
+    offv = B.fvv - _diag(B.ev)
+    offo = B.foo - _diag(B.eo)
     # QUAD3 + T1RING(F(ae) part) + fock terms (vcc/quad3.f, libr/t1ring.F)
     Fae = (offv - 0.5 * _ct("me,ma->ae", B.fov, t1)
            + _ct("mf,mafe->ae", t1, L_ovvv)
@@ -109,14 +131,14 @@ def intermediates(B, t1, t2):
              + _ct("ie,nmje->mnij", t1, B.ooov)
              + _ct("ijef,mnef->mnij", tt, B.oovv))
     # DWMBEJ + T1RING (vcc/dwmbej.F): W(mbej) ABAB and ABBA spin blocks
-    Xn = 0.5 * t2 + np.einsum("jf,nb->jnfb", t1, t1)           # (1/2 t2 + t1 t1)[j,n,f,b]
+    Xn = 0.5 * t2 + _ct("jf,nb->jnfb", t1, t1)           # (1/2 t2 + t1 t1)[j,n,f,b]
     W_abab = (B.ovvo + _ct("jf,mbef->mbej", t1, B.ovvv)
-              - _ct("nb,mnej->mbej", t1, B.ooov.transpose(1, 0, 3, 2))   # <mn|ej> = <nm|je>
+              - _ct("nb,mnej->mbej", t1, _tr(B.ooov, 1, 0, 3, 2))   # <mn|ej> = <nm|je>
               - _ct("jnfb,mnef->mbej", Xn, B.oovv)
               + _ct("njfb,mnef->mbej", t2, B.oovv)
               - 0.5 * _ct("njfb,mnfe->mbej", t2, B.oovv))
     # W_abba[m,b,e,j] (m alpha, b beta, e beta, j alpha)
-    W_abba = (-B.ovov.transpose(0, 1, 3, 2)
+    W_abba = (-_tr(B.ovov, 0, 1, 3, 2)
               - _ct("jf,mbfe->mbej", t1, B.ovvv)
               + _ct("nb,mnje->mbej", t1, B.ooov)
               + _ct("jnfb,mnfe->mbej", Xn, B.oovv))
@@ -132,8 +154,8 @@ def residual(B, t1, t2):
     Fae, Fmi, Fme = I["Fae"], I["Fmi"], I["Fme"]
     tt = I["tau"]
     # INITIN (vcc/initin.f): Z2 <- <ij|ab>;  INITSN: Z1 <- f(ia)
-    Z2 = B.oovv.copy()
-    Z1 = B.fov.copy()
+    Z2 = _copy(B.oovv)
+    Z1 = _copy(B.fov)
     # FEACONT (vcc/feacont.f): P(ab) sum_e t(ij,ae)[F(be) - 1/2 t(mb)F(me)]; T1 += t(ie)F(ae)
     Fp = Fae - 0.5 * _ct("mb,me->be", t1, Fme)
     Z2 += _P(_ct("ijae,be->ijab", t2, Fp))
@@ -143,14 +165,14 @@ def residual(B, t1, t2):
     Z2 -= _P(_ct("imab,mj->ijab", t2, Fpp))
     Z1 -= _ct("ma,mi->ia", t1, Fmi)
     # FMECONT (vcc/fmecont.f): T1 += sum_me (2 t(im,ae) - t(mi,ae)) F(me)
-    u = 2.0 * t2 - t2.transpose(1, 0, 2, 3)
+    u = 2.0 * t2 - _tr(t2, 1, 0, 2, 3)
     Z1 += _ct("imae,me->ia", u, Fme)
     # T1INT2A (vcc/t1int2a.f): -P(ab) sum_m t(ma) <mb|ij>
     Z2 -= _P(_ct("ma,mbij->ijab", t1, _ovoo(B)))
     # T1INT2B (vcc/t1int2b.f): +P(ij) sum_e t(ie) <ab|ej>
     Z2 += _P(_ct("ie,abej->ijab", t1, _vvvo(B)))
     # T1INT1 (vcc/t1int1.F): T1 += sum_nf t(nf) (2<na|fi> - <na|if>)
-    Z1 += _ct("nf,nafi->ia", t1, 2.0 * B.ovvo - B.ovov.transpose(0, 1, 3, 2))
+    Z1 += _ct("nf,nafi->ia", t1, 2.0 * B.ovvo - _tr(B.ovov, 0, 1, 3, 2))
     # DRE3EN -> DRLAD (vcc/drlad.f, vcc/ladab1.F): hole-hole ladder sum_mn tau(mn,ab) W(mn,ij)
     Z2 += _ct("mnab,mnij->ijab", tt, I["Wmnij"])
     # DRLAD ITYPE=6: particle-particle ladder sum_ef <ab|ef> tau(ef,ij) (list 233)
@@ -159,8 +181,8 @@ def residual(B, t1, t2):
     Zmbij = _ct("mbef,ijef->mbij", B.ovvv, tt)
     Z2 -= _P(_ct("ma,mbij->ijab", t1, Zmbij))
     # T12INT2 (vcc/t12int2.F): -P(ij)P(ab) sum_me t(ie) t(ma) <mb|ej>
-    Z2 -= _P(_ct("imea,mbej->ijab", np.einsum("ie,ma->imea", t1, t1), B.ovvo)
-             + _ct("jmea,mbie->ijab", np.einsum("je,ma->jmea", t1, t1), B.ovov))
+    Z2 -= _P(_ct("imea,mbej->ijab", _ct("ie,ma->imea", t1, t1), B.ovvo)
+             + _ct("jmea,mbie->ijab", _ct("je,ma->jmea", t1, t1), B.ovov))
     # DRRNG -> RNGDRV (vcc/drrng.f, vcc/rngdrv.f): ring terms with the ABAB
     # and ABBA W(mbej), symmetrised by SUMRNG
     Wab, Wba = I["W_abab"], I["W_abba"]
@@ -169,7 +191,7 @@ def residual(B, t1, t2):
             + _ct("mjae,mbei->ijab", t2, Wba))
     Z2 += _P(ring)
     # E4S -> T2T1AB1/T2T1AB2 (vcc/e4s.F, libr/t2t1ab1.f, libr/t2t1ab2.f)
-    w = 2.0 * t2 - t2.transpose(0, 1, 3, 2)
+    w = 2.0 * t2 - _tr(t2, 0, 1, 3, 2)
     Z1 += _ct("imfe,maef->ia", w, B.ovvv)
     Z1 -= _ct("mnae,mnie->ia", u, B.ooov)
     return Z1, Z2
@@ -177,12 +199,12 @@ def residual(B, t1, t2):
 
 def _ovoo(B):
     """<mb|ij> as [m,b,i,j]; with real orbitals <mb|ij> = <ij|mb> = ooov[i,j,m,b]."""
-    return B.ooov.transpose(2, 3, 0, 1)
+    return _tr(B.ooov, 2, 3, 0, 1)
 
 
 def _vvvo(B):
     """<ab|ej> as [a,b,e,j]: <ab|ej> = <ej|ab> = <je|ba> = ovvv[j,e,b,a]."""
-    return B.ovvv.transpose(3, 2, 1, 0)
+    return _tr(B.ovvv, 3, 2, 1, 0)
 
 
 def update(B, t1, t2):
