@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
+#include <utility>
 
 #include "engine.cuh"
 
@@ -164,6 +165,17 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
   bool split = prec == ACES_PREC_BF16X3 && M >= 16 && N >= 16 && K >= 128 &&
                (double)M * N * K >= 1.0e8;
   if (!split) return gemm_nt_f64(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
+  // the tensor-core epilogue gives each thread one output row m (consecutive
+  // lanes: consecutive m); an output whose unit stride runs along n is
+  // computed as C^T = B A^T so that the lanes' stores coalesce
+  CView Cv = C;
+  if (C.sm0 != 1 && C.sn0 == 1) {
+    std::swap(M, N);
+    std::swap(A, B);
+    std::swap(lda, ldb);
+    std::swap(constA, constB);
+    Cv = CView{C.p, C.ndiv, C.sn1, C.sn0, C.mdiv, C.sm1, C.sm0};
+  }
   auto get = [&](const double *src, long long ld, int rows, bool cst, SplitOperand &tmp,
                  const SplitOperand **out) -> int {
     if (cst) {
@@ -183,7 +195,7 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
   const SplitOperand *a = nullptr, *b = nullptr;
   ACES_TRY(get(A, lda, M, constA, split_tmpA, &a));
   ACES_TRY(get(B, ldb, N, constB, split_tmpB, &b));
-  return gemm_nt_bf16x3(*a, *b, M, N, alpha, beta, C, st);
+  return gemm_nt_bf16x3(*a, *b, M, N, alpha, beta, Cv, st);
 }
 
 // ---------------------------------------------------------------------------

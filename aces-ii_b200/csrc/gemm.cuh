@@ -44,8 +44,10 @@ int gemm_nt_f64_scratch(int M, int N, int K, double alpha, const double *A, long
                         double *ws, size_t cap, cudaStream_t st);
 // split-K support shared by the contraction kernels
 double *splitk_workspace(size_t doubles);
+// C = alpha * sum_z part[z] + beta * C; part[z] is [M][N] row-major, or
+// [N][M] (m fastest) with mfast
 int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
-                  double beta, cudaStream_t st);
+                  double beta, cudaStream_t st, bool mfast = false);
 
 // Split-precision operand: x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi),
 // stored K-contiguous and zero-padded to (rows_pad x k_pad).

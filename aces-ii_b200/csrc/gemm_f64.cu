@@ -129,22 +129,32 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     return;
   }
-  // epilogue through the two-level output view
+  // epilogue through the two-level output view; the beta*C loads of a row
+  // are issued together before its stores
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     int m = m0 + wm * 64 + i * 8 + lr;
     if (m >= M) continue;
     long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
+    double old[4][2];
+    if (beta != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int n = n0 + wn * 32 + j * 8 + lc * 2 + h;
+          old[j][h] = n < N ? __ldg(C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0) : 0.0;
+        }
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         int n = n0 + wn * 32 + j * 8 + lc * 2 + h;
         if (n >= N) continue;
-        double *cp = C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
         double r = alpha * acc[i][j][h];
-        if (beta != 0.0) r += beta * *cp;
-        *cp = r;
+        if (beta != 0.0) r += beta * old[j][h];
+        C.p[mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0] = r;
       }
     }
   }
@@ -152,12 +162,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 }  // namespace
 
 // C = alpha * sum_z part[z] + beta * C
+// part[z][m][n] (mfast false) or part[z][n][m] (mfast true)
 __global__ void k_splitk_reduce(CView C, const double *__restrict__ part, int M, int N, int Z,
-                                double alpha, double beta) {
+                                double alpha, double beta, bool mfast) {
   long long total = (long long)M * N;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    int m = (int)(idx / N), n = (int)(idx % N);
+    int m = mfast ? (int)(idx % M) : (int)(idx / N);
+    int n = mfast ? (int)(idx / M) : (int)(idx % N);
     double s = 0.0;
     for (int z = 0; z < Z; ++z) s += part[(size_t)z * total + idx];
     double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
@@ -338,11 +350,11 @@ double *splitk_workspace(size_t doubles) {
 }
 
 int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
-                  double beta, cudaStream_t st) {
+                  double beta, cudaStream_t st, bool mfast) {
   long long total = (long long)M * N;
   long long nb = (total + 255) / 256;
   if (nb > 148 * 16) nb = 148 * 16;
-  k_splitk_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta);
+  k_splitk_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, mfast);
   count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;

@@ -77,11 +77,14 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 
 namespace {
 constexpr int TBM = 128, TBN = 128, TBK = 64, STAGES = 3;
-constexpr int CHUNK = 2;                              // k tiles per FP32 accumulation chunk
+#ifndef ACES_TC_CHUNK
+#define ACES_TC_CHUNK 4
+#endif
+constexpr int CHUNK = ACES_TC_CHUNK;                  // k tiles per FP32 accumulation chunk
 constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
 constexpr int TILE_B = TBN * TBK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment + barriers
 constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols = 2 * TBN;                    // two ping-pong accumulators
@@ -176,12 +179,33 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // accumulators (ping-pong); the epilogue warps drain every finished chunk into
 // FP64 registers while the next chunk is computed.  This bounds the number of
 // FP32 tensor-core accumulations any partial sum sees to 12*CHUNK, so the
-// truncation bias of the tensor-core adders stays at ~1e-6 relative instead of
-// growing with K.
+// truncation bias of the tensor-core adders stays small instead of growing
+// with K.
+//
+// The kernel is persistent: gridDim.x <= #SMs CTAs walk the output tiles
+// t = blockIdx.x, blockIdx.x + gridDim.x, ... (n tile fastest, then m tile,
+// then the split-K slice z).  The TMA producer and the MMA issuer run their
+// k-tile sequence straight across tile boundaries (stage and TMEM-buffer
+// parities are global counters), so the loads and products of the next tile
+// overlap the epilogue of the current one.
+struct TileSched {
+  int tilesN, tilesM, ktc, kTilesTotal;
+  __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &ktb,
+                                         int &kTiles) const {
+    const int tn = t % tilesN, r = t / tilesN;
+    const int tm = r % tilesM;
+    z = r / tilesM;
+    m0 = tm * TBM;
+    n0 = tn * TBN;
+    ktb = z * ktc;
+    kTiles = max(0, min(ktc, kTilesTotal - ktb));
+  }
+};
+
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                  int M, int N, int kTilesTotal, int ktc, double alpha, double beta, CView C,
+                  int M, int N, TileSched sch, int nTiles, double alpha, double beta, CView C,
                   double *__restrict__ part) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -190,15 +214,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t *empty = bars + STAGES;            // [STAGES] MMA -> TMA
   uint64_t *acc_full = bars + 2 * STAGES;     // [2] MMA -> epilogue
   uint64_t *acc_empty = bars + 2 * STAGES + 2;  // [2] epilogue -> MMA
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
+  uint64_t *mma_done = bars + 2 * STAGES + 4;   // all products retired (teardown)
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
-  // split-K: blockIdx.z owns k tiles [ktb, ktb + kTiles)
-  const int ktb = blockIdx.z * ktc;
-  const int kTiles = max(0, min(ktc, kTilesTotal - ktb));
-  const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -209,6 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(smem_u32(&acc_full[b]), 1);
       mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);
     }
+    mbar_init(smem_u32(mma_done), 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -225,110 +246,161 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
-    int issued = 0;
-    for (int kt = 0; kt < kTiles; ++kt) {
-      int s = kt % STAGES;
-      if (kt >= STAGES) {
-        if (!mbar_wait(smem_u32(&empty[s]), ((kt / STAGES) - 1) & 1)) {
+    int it = 0;  // k tiles issued by this CTA
+    bool stop = false;
+    for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
+      int m0, n0, z, ktb, kTiles;
+      sch.decode(t, m0, n0, z, ktb, kTiles);
+      for (int kt = 0; kt < kTiles; ++kt) {
+        const int s = it % STAGES;
+        if (it >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((it / STAGES) - 1) & 1)) {
           atomicExch(&g_tc_status, 1);
           *(volatile int *)abort_flag = 1;
+          stop = true;
           break;
         }
+        if (*(volatile int *)abort_flag) {
+          stop = true;
+          break;
+        }
+        const uint32_t fb = smem_u32(&full[s]);
+        unsigned char *st = smem + s * STAGE_BYTES;
+        mbar_expect_tx(fb, STAGE_BYTES);
+        const int kx = (ktb + kt) * TBK;
+        tma_load_2d(smem_u32(st), &mAh, kx, m0, fb);
+        tma_load_2d(smem_u32(st + TILE_A), &mAl, kx, m0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A), &mBh, kx, n0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &mBl, kx, n0, fb);
+        ++it;
       }
-      if (*(volatile int *)abort_flag) break;
-      uint32_t fb = smem_u32(&full[s]);
-      unsigned char *st = smem + s * STAGE_BYTES;
-      mbar_expect_tx(fb, STAGE_BYTES);
-      int kx = (ktb + kt) * TBK;
-      tma_load_2d(smem_u32(st), &mAh, kx, m0, fb);
-      tma_load_2d(smem_u32(st + TILE_A), &mAl, kx, m0, fb);
-      tma_load_2d(smem_u32(st + 2 * TILE_A), &mBh, kx, n0, fb);
-      tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &mBl, kx, n0, fb);
-      issued = kt + 1;
     }
     // drain: the most recent phase of every stage still possibly in flight
-    int first = issued > STAGES ? issued - STAGES : 0;
-    for (int kt = first; kt < issued; ++kt)
-      if (!mbar_wait(smem_u32(&full[kt % STAGES]), (kt / STAGES) & 1)) atomicExch(&g_tc_status, 2);
+    const int first = it > STAGES ? it - STAGES : 0;
+    for (int k = first; k < it; ++k)
+      if (!mbar_wait(smem_u32(&full[k % STAGES]), (k / STAGES) & 1)) atomicExch(&g_tc_status, 2);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    for (int kt = 0; kt < kTiles; ++kt) {
-      const int c = kt / CHUNK, b = c & 1, kin = kt % CHUNK;
-      if (kin == 0 && c >= 2) {
-        if (!mbar_wait(smem_u32(&acc_empty[b]), ((c >> 1) - 1) & 1)) {
+    int it = 0, gc = 0;  // k tiles consumed, accumulation chunks started
+    bool stop = false;
+    for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
+      int m0, n0, z, ktb, kTiles;
+      sch.decode(t, m0, n0, z, ktb, kTiles);
+      for (int kt = 0; kt < kTiles; ++kt) {
+        const int kin = kt % CHUNK, b = gc & 1;
+        if (kin == 0 && gc >= 2 &&
+            !mbar_wait(smem_u32(&acc_empty[b]), ((gc >> 1) - 1) & 1)) {
           atomicExch(&g_tc_status, 5);
           *(volatile int *)abort_flag = 1;
+          stop = true;
           break;
         }
-      }
-      int s = kt % STAGES;
-      if (!mbar_wait(smem_u32(&full[s]), (kt / STAGES) & 1)) {
-        atomicExch(&g_tc_status, 3);
-        *(volatile int *)abort_flag = 1;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint32_t base = smem_u32(smem + s * STAGE_BYTES);
-      uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + TILE_B;
-      uint32_t acc_t = tmem + (uint32_t)(b * TBN);
+        const int s = it % STAGES;
+        if (!mbar_wait(smem_u32(&full[s]), (it / STAGES) & 1)) {
+          atomicExch(&g_tc_status, 3);
+          *(volatile int *)abort_flag = 1;
+          stop = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + TILE_B;
+        const uint32_t acc_t = tmem + (uint32_t)(b * TBN);
 #pragma unroll
-      for (int kk = 0; kk < TBK / 16; ++kk) {
-        uint32_t off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzled row
-        uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
-        umma(acc_t, umma_desc(ah + off), umma_desc(bh + off), acc);
-        umma(acc_t, umma_desc(ah + off), umma_desc(bl + off), 1u);
-        umma(acc_t, umma_desc(al + off), umma_desc(bh + off), 1u);
+        for (int kk = 0; kk < TBK / 16; ++kk) {
+          const uint32_t off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzled row
+          const uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
+          umma(acc_t, umma_desc(ah + off), umma_desc(bh + off), acc);
+          umma(acc_t, umma_desc(ah + off), umma_desc(bl + off), 1u);
+          umma(acc_t, umma_desc(al + off), umma_desc(bh + off), 1u);
+        }
+        umma_commit(smem_u32(&empty[s]));
+        ++it;
+        if (kin == CHUNK - 1 || kt == kTiles - 1) {
+          umma_commit(smem_u32(&acc_full[b]));
+          ++gc;
+        }
       }
-      umma_commit(smem_u32(&empty[s]));
-      if (kin == CHUNK - 1 || kt == kTiles - 1) umma_commit(smem_u32(&acc_full[b]));
     }
+    // every product issued by this thread has retired before TMEM is released
+    umma_commit(smem_u32(mma_done));
+    if (!mbar_wait(smem_u32(mma_done), 0)) atomicExch(&g_tc_status, 6);
   } else if (warp >= 2) {
     // ---------------- epilogue: FP64 accumulation of the chunks ----------------
     const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
     const int half = (warp - 2) >> 2;      // which 64 accumulator columns
     const int row = q * 32 + lane;
-    double acc[64];
-#pragma unroll
-    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    // lanes are consecutive output rows: with unit m stride a warp's stores coalesce
+    const bool coalesced = C.sm0 == 1;
+    int gc = 0;
     bool ok = true;
-    for (int c = 0; c < nChunks; ++c) {
-      const int b = c & 1;
-      bool w = mbar_wait(smem_u32(&acc_full[b]), (c >> 1) & 1);
-      if (!w) atomicExch(&g_tc_status, 4);
-      ok = __all_sync(0xffffffffu, w && !*(volatile int *)abort_flag);
+    for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
+      int m0, n0, z, ktb, kTiles;
+      sch.decode(t, m0, n0, z, ktb, kTiles);
+      const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
+      const int ncol = min(64, N - (n0 + half * 64));  // live columns of this warp (may be <= 0)
+      double acc[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int c = 0; c < nChunks; ++c, ++gc) {
+        const int b = gc & 1;
+        const bool w = mbar_wait(smem_u32(&acc_full[b]), (gc >> 1) & 1);
+        if (!w) atomicExch(&g_tc_status, 4);
+        ok = __all_sync(0xffffffffu, w && !*(volatile int *)abort_flag);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tbase =
+            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * 64);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (ncol > h * 32) {  // warp-uniform: skip column groups past N
+            uint32_t r[32];
+            tmem_ld32(tbase + h * 32, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[h * 32 + j] += (double)__uint_as_float(r[j]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+      }
       if (!ok) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * 64);
+      const int m = m0 + row;
+      if (m >= M || ncol <= 0) continue;
+      const int nb = n0 + half * 64;
+      if (part) {
+        // split-K partial, [z][n][m]: lanes write consecutive m
+        double *pz = part + (size_t)z * M * N + m;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        uint32_t r[32];
-        tmem_ld32(tbase + h * 32, r);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int j = 0; j < 64; ++j)
+          if (j < ncol) pz[(size_t)(nb + j) * M] = acc[j];
+      } else {
+        const long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
+        auto addr = [&](int n) -> double * {
+          return C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
+        };
+        if (beta == 0.0) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[h * 32 + j] += (double)__uint_as_float(r[j]);
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
-    }
-    const int m = m0 + row;
-    if (ok && m < M && part) {
-      double *pz = part + (size_t)blockIdx.z * M * N + (size_t)m * N;
+          for (int j = 0; j < 64; ++j)
+            if (j < ncol) *addr(nb + j) = alpha * acc[j];
+        } else if (beta == 1.0 && coalesced) {
+          // one fire-and-forget FP64 add per element (RED): every element has a
+          // single owner thread, so the result equals load + add + store
 #pragma unroll
-      for (int j = 0; j < 64; ++j) {
-        int n = n0 + half * 64 + j;
-        if (n < N) pz[n] = acc[j];
-      }
-    } else if (ok && m < M) {
-      const long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
+          for (int j = 0; j < 64; ++j)
+            if (j < ncol) atomicAdd(addr(nb + j), alpha * acc[j]);
+        } else {
+          // read-modify-write in batches of 8: all loads of a batch are issued
+          // before its stores, so the memory latency is paid once per batch
 #pragma unroll
-      for (int j = 0; j < 64; ++j) {
-        int n = n0 + half * 64 + j;
-        if (n < N) {
-          double *cp = C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
-          double v = alpha * acc[j];
-          if (beta != 0.0) v += beta * *cp;
-          *cp = v;
+          for (int j0 = 0; j0 < 64; j0 += 8) {
+            double old[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) old[j] = j0 + j < ncol ? __ldg(addr(nb + j0 + j)) : 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (j0 + j < ncol) *addr(nb + j0 + j) = alpha * acc[j0 + j] + beta * old[j];
+          }
         }
       }
     }
@@ -340,6 +412,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols));
   }
+}
+
+// multiprocessor count of the current device (persistent grid size)
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -403,30 +489,39 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
   ACES_TRY(make_map(&mAl, A.lo, A.rows_pad, A.k_pad, TBM));
   ACES_TRY(make_map(&mBh, B.hi, B.rows_pad, B.k_pad, TBN));
   ACES_TRY(make_map(&mBl, B.lo, B.rows_pad, B.k_pad, TBN));
-  dim3 grid((N + TBN - 1) / TBN, (M + TBM - 1) / TBM);
-  const int kTiles = A.k_pad / TBK;
-  // split K when the output has too few tiles to fill the 148 SMs
-  long long tiles = (long long)grid.x * grid.y;
-  int Z = 1, ktc = kTiles;
+  TileSched sch;
+  sch.tilesN = (N + TBN - 1) / TBN;
+  sch.tilesM = (M + TBM - 1) / TBM;
+  sch.kTilesTotal = A.k_pad / TBK;
+  sch.ktc = sch.kTilesTotal;
+  // split K when the output has too few tiles to fill the SMs
+  const long long tiles = (long long)sch.tilesN * sch.tilesM;
+  const int nsm = num_sms();
+  int Z = 1;
   double *part = nullptr;
-  if (tiles < 148 && kTiles >= 8) {
-    Z = (int)std::min<long long>((148 + tiles - 1) / tiles, kTiles / 4);
+  if (tiles < nsm && sch.kTilesTotal >= 8) {
+    Z = (int)std::min<long long>((nsm + tiles - 1) / tiles, sch.kTilesTotal / 4);
     if (Z > 1) {
-      ktc = (kTiles + Z - 1) / Z;
-      Z = (kTiles + ktc - 1) / ktc;
+      sch.ktc = (sch.kTilesTotal + Z - 1) / Z;
+      Z = (sch.kTilesTotal + sch.ktc - 1) / sch.ktc;
       part = splitk_workspace((size_t)Z * M * N);
       if (!part) {
         set_error("gemm_nt_bf16x3: split-K workspace allocation failed");
         return ACES_ERR_NOMEM;
       }
-      grid.z = Z;
     }
   }
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, kTiles, ktc, alpha,
-                                                     beta, C, part);
+  const long long nTiles = tiles * Z;
+  if (nTiles > (1LL << 31) - 1) {
+    set_error("gemm_nt_bf16x3: %lld output tiles exceed the scheduler range", nTiles);
+    return ACES_ERR_ARG;
+  }
+  const unsigned grid = (unsigned)std::min<long long>(nTiles, nsm);
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, sch, (int)nTiles,
+                                                     alpha, beta, C, part);
   count_launch();
   ACES_CUDA(cudaGetLastError());
-  if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st);
+  if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st, true);
   return ACES_OK;
 }
 

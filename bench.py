@@ -394,6 +394,9 @@ KERNEL_CASES = {
     # particle-particle ladder shape Z(ab,ij) = W(ab,ef) tau(ef,ij) at v=120, o=20:
     # M = K = v^2 = 14400, N = o^2 = 400; A (FP64 1.66 GB, split 0.83 GB) exceeds L2
     "ladder-small": dict(m=14400, n=400, k=14400),
+    # T1-dressing shape W(ajb,i) = sum_e <ajb|e> t(i,e) at o=20, v=180:
+    # M = o*v*v = 648000, N = o = 20, K = v = 180
+    "thin-t1": dict(m=648000, n=20, k=180),
 }
 
 

@@ -24,10 +24,14 @@ def lib():
     return lib
 
 
+# (1000, 260, 777) takes the split-K path; (2000, 1300, 200) and (70000, 20, 180)
+# have more output tiles than SMs, so each persistent CTA walks several tiles
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 64), (37, 53, 29), (300, 200, 513),
-                                   (129, 7, 1000), (1000, 260, 777)])
+                                   (129, 7, 1000), (1000, 260, 777), (2000, 1300, 200),
+                                   (70000, 20, 180)])
 @pytest.mark.parametrize("ta,tb", [("T", "N"), ("N", "T")])
-def test_xgemm_bf16x3_error_bound(lib, m, n, k, ta, tb):
+@pytest.mark.parametrize("beta", [0.5, 0.0, 1.0])
+def test_xgemm_bf16x3_error_bound(lib, m, n, k, ta, tb, beta):
     import torch
     g = torch.Generator(device="cpu").manual_seed(m + 11 * n + 101 * k)
     A = torch.randn((m, k) if ta == "N" else (k, m), generator=g, dtype=torch.float64)
@@ -37,12 +41,12 @@ def test_xgemm_bf16x3_error_bound(lib, m, n, k, ta, tb):
     Cm = torch.randn((m, n), generator=g, dtype=torch.float64)
     opA = A if ta == "N" else A.T
     opB = B if tb == "N" else B.T
-    ref = 1.3 * opA @ opB + 0.5 * Cm
+    ref = 1.3 * opA @ opB + beta * Cm
     bound = 1.3 * opA.abs() @ opB.abs()
     dA = A.T.contiguous().cuda()
     dB = B.T.contiguous().cuda()
     dC = Cm.T.contiguous().cuda()
-    lib.xgemm(ta, tb, m, n, k, 1.3, dA.data_ptr(), A.shape[0], dB.data_ptr(), B.shape[0], 0.5,
+    lib.xgemm(ta, tb, m, n, k, 1.3, dA.data_ptr(), A.shape[0], dB.data_ptr(), B.shape[0], beta,
               dC.data_ptr(), m, precision=ab.PREC_BF16X3)
     out = dC.cpu().T
     err = (out - ref).abs()
