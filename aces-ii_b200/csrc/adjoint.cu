@@ -8,7 +8,7 @@ namespace acesb200 {
 
 namespace {
 __device__ __forceinline__ long long view_off(const CView &C, long long m, long long n) {
-  return (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
+  return cview_off(C, (int)m, (int)n);
 }
 
 __global__ void k_view_gather(double *__restrict__ dense, CView C, int M, int N, double scale) {

@@ -14,6 +14,8 @@
 namespace acesb200 {
 
 void set_error(const char *fmt, ...);
+// destroys the CC engine (amplitudes, intermediates, split caches) of this process
+void engine_reset();
 
 // number of kernels the library has launched (reported by the benchmarks)
 extern std::atomic<long long> g_launches;
@@ -34,6 +36,28 @@ inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed);
     int _s = (call);                                                           \
     if (_s != ACES_OK) return _s;                                              \
   } while (0)
+
+// Division of 32-bit indices below 2^31 by a run-time invariant divisor with
+// a multiply-high, add and shift (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994): with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1,
+// n / d = (umulhi(n, m) + n) >> s for 0 <= n < 2^31.
+struct FastDiv {
+  unsigned d = 1, m = 1, s = 0;
+  FastDiv() = default;
+  explicit FastDiv(unsigned divisor) : d(divisor ? divisor : 1) {
+    s = 0;
+    while ((1ull << s) < d) ++s;
+    m = (unsigned)(((1ull << 32) * ((1ull << s) - d)) / d + 1);
+  }
+  __host__ __device__ __forceinline__ unsigned div(unsigned n) const {
+#ifdef __CUDA_ARCH__
+    return (__umulhi(n, m) + n) >> s;
+#else
+    return (unsigned)((((unsigned long long)n * m) >> 32) + n) >> s;
+#endif
+  }
+};
 
 // One irrep block of a list: nrows x ncols doubles, column-major, on device.
 struct ListBlock {

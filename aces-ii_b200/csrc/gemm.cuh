@@ -20,6 +20,15 @@ struct CView {
   long long ndiv, sn1, sn0;
 };
 
+// Offset of index i along one view dimension: (i / div) * s1 + (i % div) * s0.
+// Divisors above 2^31 mean a single-level dimension; the others take a 32-bit
+// division (a 64-bit one costs several times more per output element).
+__host__ __device__ __forceinline__ long long cview_dim(long long div, long long s1,
+                                                        long long s0, int i) {
+  if (div > 0x7fffffff) return (long long)i * s0;
+  const int d = (int)div, q = i / d;
+  return (long long)q * s1 + (long long)(i - q * d) * s0;
+}
 // plain row-major C[m*ldc + n]
 inline CView cview_rowmajor(double *p, long long ldc) {
   return CView{p, 1LL << 62, 0, ldc, 1LL << 62, 0, 1};
@@ -28,6 +37,41 @@ inline CView cview_rowmajor(double *p, long long ldc) {
 inline CView cview_colmajor(double *p, long long ldc) {
   return CView{p, 1LL << 62, 0, 1, 1LL << 62, 0, ldc};
 }
+__host__ __device__ __forceinline__ long long cview_off(const CView &C, int m, int n) {
+  return cview_dim(C.mdiv, C.sm1, C.sm0, m) + cview_dim(C.ndiv, C.sn1, C.sn0, n);
+}
+
+// Walks i = i0, i0+1, ... along one view dimension (divisor div, strides s1,
+// s0) without dividing per step (the epilogues' inner loops).
+struct ViewWalk {
+  long long off, s1, s0;
+  int r, d;
+  __device__ __forceinline__ ViewWalk(long long div, long long s1_, long long s0_, int i0)
+      : s1(s1_), s0(s0_) {
+    if (div > 0x7fffffff) {
+      d = 0x7fffffff;
+      r = 0;
+      off = (long long)i0 * s0;
+    } else {
+      d = (int)div;
+      const int q = i0 / d;
+      r = i0 - q * d;
+      off = (long long)q * s1 + (long long)r * s0;
+    }
+  }
+  __device__ __forceinline__ void next() {
+    if (++r == d) {
+      r = 0;
+      off += s1 - (long long)(d - 1) * s0;
+    } else {
+      off += s0;
+    }
+  }
+};
+struct CViewNWalk : ViewWalk {
+  __device__ __forceinline__ CViewNWalk(const CView &C, int n0)
+      : ViewWalk(C.ndiv, C.sn1, C.sn0, n0) {}
+};
 
 // FP64 tensor-core (DMMA) contraction.
 int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long lda,
@@ -50,7 +94,9 @@ int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, doubl
                   double beta, cudaStream_t st, bool mfast = false);
 
 // Split-precision operand: x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi),
-// stored K-contiguous and zero-padded to (rows_pad x k_pad).
+// stored K-contiguous with K zero-padded to k_pad.  rows_pad is the row extent
+// of the TMA tensor map (= rows): the rows of a 128-row box past it are
+// zero-filled by the TMA unit, so thin operands need no padding in memory.
 struct SplitOperand {
   void *hi = nullptr;   // __nv_bfloat16[rows_pad * k_pad]
   void *lo = nullptr;
@@ -58,8 +104,7 @@ struct SplitOperand {
   size_t cap = 0;       // bytes allocated at hi (both planes)
 };
 
-// rows and K padding of split operands (the tcgen05 kernel's tile sizes)
-constexpr int kSplitRowPad = 128;
+// K padding of split operands (the tcgen05 kernel's k tile)
 constexpr int kSplitKPad = 64;
 
 // Fill a split operand from an FP64 K-contiguous matrix (src[r*ld + k]).

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   for (int i = 0; i < 8; ++i) {
     int m = m0 + wm * 64 + i * 8 + lr;
     if (m >= M) continue;
-    long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
+    long long mo = cview_dim(C.mdiv, C.sm1, C.sm0, m);
     double old[4][2];
     if (beta != 0.0) {
 #pragma unroll
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           int n = n0 + wn * 32 + j * 8 + lc * 2 + h;
-          old[j][h] = n < N ? __ldg(C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0) : 0.0;
+          old[j][h] = n < N ? __ldg(C.p + mo + cview_dim(C.ndiv, C.sn1, C.sn0, n)) : 0.0;
         }
     }
 #pragma unroll
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (n >= N) continue;
         double r = alpha * acc[i][j][h];
         if (beta != 0.0) r += beta * old[j][h];
-        C.p[mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0] = r;
+        C.p[mo + cview_dim(C.ndiv, C.sn1, C.sn0, n)] = r;
       }
     }
   }
@@ -172,8 +172,7 @@ __global__ void k_splitk_reduce(CView C, const double *__restrict__ part, int M,
     int n = mfast ? (int)(idx / M) : (int)(idx % N);
     double s = 0.0;
     for (int z = 0; z < Z; ++z) s += part[(size_t)z * total + idx];
-    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
-                 (n % C.ndiv) * C.sn0;
+    double *cp = C.p + cview_off(C, m, n);
     double r = alpha * s;
     if (beta != 0.0) r += beta * *cp;
     *cp = r;
@@ -188,13 +187,21 @@ __global__ void k_gemv_f64(int M, int K, double alpha, const double *__restrict_
   int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int m = warp; m < M; m += nwarps) {
     const double *a = A + (long long)m * lda;
-    double s = 0.0;
-    for (int k = lane; k < K; k += 32) s += a[k] * __ldg(x + k);
+    // four independent partial sums keep four row loads in flight per lane
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int k = lane;
+    for (; k + 96 < K; k += 128) {
+      s0 += a[k] * __ldg(x + k);
+      s1 += a[k + 32] * __ldg(x + k + 32);
+      s2 += a[k + 64] * __ldg(x + k + 64);
+      s3 += a[k + 96] * __ldg(x + k + 96);
+    }
+    for (; k < K; k += 32) s0 += a[k] * __ldg(x + k);
+    double s = (s0 + s1) + (s2 + s3);
     for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
     if (lane == 0) {
       int mm = transpose_out ? 0 : m, nn = transpose_out ? m : 0;
-      double *cp = C.p + (mm / C.mdiv) * C.sm1 + (mm % C.mdiv) * C.sm0 + (nn / C.ndiv) * C.sn1 +
-                   (nn % C.ndiv) * C.sn0;
+      double *cp = C.p + cview_off(C, mm, nn);
       double r = alpha * s;
       if (beta != 0.0) r += beta * *cp;
       *cp = r;
@@ -262,8 +269,7 @@ __global__ void __launch_bounds__(256)
         part[(size_t)blockIdx.z * (size_t)L * S + (size_t)l * S + sidx] = acc[i][j];
         continue;
       }
-      double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
-                   (n % C.ndiv) * C.sn0;
+      double *cp = C.p + cview_off(C, m, n);
       double v = alpha * acc[i][j];
       if (beta != 0.0) v += beta * *cp;
       *cp = v;
@@ -281,8 +287,7 @@ __global__ void k_thin_reduce(CView C, const double *__restrict__ part, int L, i
     double sum = 0.0;
     for (int z = 0; z < Z; ++z) sum += part[(size_t)z * total + idx];
     int m = s_is_m ? sidx : l, n = s_is_m ? l : sidx;
-    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
-                 (n % C.ndiv) * C.sn0;
+    double *cp = C.p + cview_off(C, m, n);
     double v = alpha * sum;
     if (beta != 0.0) v += beta * *cp;
     *cp = v;
@@ -291,46 +296,107 @@ __global__ void k_thin_reduce(CView C, const double *__restrict__ part, int L, i
 
 // ---------------------------------------------------------------------------
 // Low-rank updates (K <= 32): C(m,n) = alpha sum_k A[m,k] B[n,k] + beta C(m,n).
-// Output bound: threads run along whichever output index has unit stride in
-// the view so the read-modify-write of C is coalesced; A/B rows are staged.
+// Output bound.  A block owns 128 outputs along the "fast" index (the one with
+// unit stride in the view, so the update of C coalesces) x 32 along the other.
+// Both short operands are staged in shared memory with an odd row stride; each
+// thread runs 8 independent FMA chains (one per slow index) over k, then
+// updates its 8 outputs: one RED per element for beta = 1 on a coalesced view
+// (a single owner per element, so the sum equals load + add + store), else a
+// batched read-modify-write.
 // ---------------------------------------------------------------------------
-constexpr int LR_F = 64, LR_S = 8, LR_K = 32;
+constexpr int LR_F = 128, LR_S = 32, LR_K = 32;
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(LR_F)
     k_gemm_lowrank_f64(int M, int N, int K, double alpha, const double *__restrict__ A,
                        long long lda, const double *__restrict__ B, long long ldb, double beta,
-                       CView C, bool fast_is_m) {
-  __shared__ double Fs[LR_F][LR_K + 1];
-  __shared__ double Ss[LR_S][LR_K + 1];
+                       CView C, bool fast_is_m, int tiles_f) {
+  extern __shared__ double lr_smem[];
+  const int ks = K | 1;  // odd row stride: column reads across threads are conflict free
+  double *Fs = lr_smem;              // [LR_F][ks]
+  double *Ss = lr_smem + LR_F * ks;  // [LR_S][ks]
   const int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
   const double *Fp = fast_is_m ? A : B;
   const double *Sp = fast_is_m ? B : A;
   const long long ldf = fast_is_m ? lda : ldb, lds = fast_is_m ? ldb : lda;
-  const int tf = (nf + LR_F - 1) / LR_F;
-  const int f0 = (blockIdx.x % tf) * LR_F;
-  const int s0 = (blockIdx.x / tf) * LR_S;
-  for (int e = threadIdx.x; e < LR_F * LR_K; e += 256) {
-    int rr = e / LR_K, kk = e % LR_K;
-    Fs[rr][kk] = (f0 + rr < nf && kk < K) ? Fp[(long long)(f0 + rr) * ldf + kk] : 0.0;
+  const int f0 = (blockIdx.x % tiles_f) * LR_F;
+  const int s0 = (blockIdx.x / tiles_f) * LR_S;
+  for (int e = threadIdx.x; e < LR_F * K; e += LR_F) {
+    const int rr = e / K, kk = e - rr * K;
+    Fs[rr * ks + kk] = f0 + rr < nf ? Fp[(long long)(f0 + rr) * ldf + kk] : 0.0;
   }
-  for (int e = threadIdx.x; e < LR_S * LR_K; e += 256) {
-    int rr = e / LR_K, kk = e % LR_K;
-    Ss[rr][kk] = (s0 + rr < ns && kk < K) ? Sp[(long long)(s0 + rr) * lds + kk] : 0.0;
+  for (int e = threadIdx.x; e < LR_S * K; e += LR_F) {
+    const int rr = e / K, kk = e - rr * K;
+    Ss[rr * ks + kk] = s0 + rr < ns ? Sp[(long long)(s0 + rr) * lds + kk] : 0.0;
   }
   __syncthreads();
-  const int fl = threadIdx.x % LR_F, sl0 = threadIdx.x / LR_F;  // 64 x 4
-  for (int sl = sl0; sl < LR_S; sl += 4) {
-    int f = f0 + fl, sidx = s0 + sl;
-    if (f >= nf || sidx >= ns) continue;
-    double acc = 0.0;
-    for (int kk = 0; kk < K; ++kk) acc = fma(Fs[fl][kk], Ss[sl][kk], acc);
-    int m = fast_is_m ? f : sidx, n = fast_is_m ? sidx : f;
-    double *cp = C.p + (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0 + (n / C.ndiv) * C.sn1 +
-                 (n % C.ndiv) * C.sn0;
-    double v = alpha * acc;
-    if (beta != 0.0) v += beta * *cp;
-    *cp = v;
+  const int f = f0 + threadIdx.x;
+  if (f >= nf) return;
+  const int nsl = min(LR_S, ns - s0);
+  // fast and slow view dimensions
+  const long long fdiv = fast_is_m ? C.mdiv : C.ndiv, fs1 = fast_is_m ? C.sm1 : C.sn1,
+                  fs0 = fast_is_m ? C.sm0 : C.sn0;
+  const long long sdiv = fast_is_m ? C.ndiv : C.mdiv, ss1 = fast_is_m ? C.sn1 : C.sm1,
+                  ss0 = fast_is_m ? C.sn0 : C.sm0;
+  double *const cf = C.p + cview_dim(fdiv, fs1, fs0, f);
+  ViewWalk w(sdiv, ss1, ss0, s0);
+  const bool red = beta == 1.0 && fs0 == 1;
+  const double *fr = Fs + threadIdx.x * ks;
+#pragma unroll 1
+  for (int sb = 0; sb < nsl; sb += 8) {
+    double acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+    const double *sr = Ss + sb * ks;  // rows sb..sb+7 < LR_S (zero past ns)
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+      const double fv = fr[k];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] = fma(fv, sr[j * ks + k], acc[j]);
+    }
+    long long off[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc[j] *= alpha;
+      off[j] = w.off;
+      w.next();
+    }
+    if (beta == 0.0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (sb + j < nsl) cf[off[j]] = acc[j];
+    } else if (red) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (sb + j < nsl) atomicAdd(cf + off[j], acc[j]);
+    } else {
+      double old[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) old[j] = sb + j < nsl ? __ldg(cf + off[j]) : 0.0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (sb + j < nsl) cf[off[j]] = acc[j] + beta * old[j];
+    }
   }
+}
+
+static int launch_lowrank(int M, int N, int K, double alpha, const double *A, long long lda,
+                          const double *B, long long ldb, double beta, const CView &C,
+                          cudaStream_t st) {
+  // run threads along the unit-stride output index
+  const bool fast_is_m = C.sm0 == 1 || C.sn0 != 1;
+  const int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
+  const int tiles_f = (nf + LR_F - 1) / LR_F;
+  const long long nb = (long long)tiles_f * ((ns + LR_S - 1) / LR_S);
+  if (nb > 0x7fffffffLL) {
+    set_error("low-rank contraction grid too large (%lld blocks)", nb);
+    return ACES_ERR_ARG;
+  }
+  const size_t smem = (size_t)(LR_F + LR_S) * (K | 1) * sizeof(double);
+  k_gemm_lowrank_f64<<<(unsigned)nb, LR_F, smem, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                       fast_is_m, tiles_f);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
 }
 
 double *splitk_workspace(size_t doubles) {
@@ -379,16 +445,7 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
     // C = beta*C: run with K = 0 is a scale; issue through the kernel with no k tiles
   }
   // K <= 32: output-bound low-rank update
-  if (K <= LR_K) {
-    const bool fast_is_m = C.sm0 == 1;  // run threads along the unit-stride output index
-    int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
-    long long nb = (long long)((nf + LR_F - 1) / LR_F) * ((ns + LR_S - 1) / LR_S);
-    k_gemm_lowrank_f64<<<(unsigned)nb, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                     fast_is_m);
-    count_launch();
-    ACES_CUDA(cudaGetLastError());
-    return ACES_OK;
-  }
+  if (K <= LR_K) return launch_lowrank(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
   // one output dimension <= 32: thin kernel over the long dimension
   if (M <= TS || N <= TS) {
     bool s_is_m = M <= TS && (M <= N);
@@ -487,16 +544,7 @@ int gemm_nt_f64_scratch(int M, int N, int K, double alpha, const double *A, long
                         const double *B, long long ldb, double beta, const CView &C,
                         double *ws, size_t cap, cudaStream_t st) {
   if (M <= 0 || N <= 0) return ACES_OK;
-  if (K <= LR_K) {
-    const bool fast_is_m = C.sm0 == 1;
-    int nf = fast_is_m ? M : N, ns = fast_is_m ? N : M;
-    long long nb = (long long)((nf + LR_F - 1) / LR_F) * ((ns + LR_S - 1) / LR_S);
-    k_gemm_lowrank_f64<<<(unsigned)nb, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                     fast_is_m);
-    count_launch();
-    ACES_CUDA(cudaGetLastError());
-    return ACES_OK;
-  }
+  if (K <= LR_K) return launch_lowrank(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
   if (M <= TS || N <= TS) {
     bool s_is_m = M <= TS && (M <= N);
     int L = s_is_m ? N : M, S = s_is_m ? M : N;

@@ -5,16 +5,18 @@
 // Each FP64 operand x is stored as two BF16 planes, hi = bf16(x) and
 // lo = bf16(x - hi).  The kernel accumulates hi*hi + hi*lo + lo*hi for every
 // K slice into one TMEM accumulator (the lo*lo term, ~2^-18 relative, is
-// dropped), which gives ~16 significant bits per product and FP32 sums.
+// dropped), which gives ~16 significant bits per product and FP32 sums that
+// are promoted to FP64 every CHUNK k tiles.
 //
-// CTA tile 128 x 128 x 64, 3-stage mbarrier pipeline, 10 warps:
+// Persistent kernel, one CTA per SM, output tile 128 x 128, k tile 64,
+// 3-stage mbarrier pipeline, 10 warps:
 //   warp 0  TMA producer (one elected lane)
 //   warp 1  TMEM allocator + MMA issuer (one elected lane)
 //   warps 2-9 epilogue: two warps per TMEM lane quadrant, each thread one
 //             output row x 64 columns, accumulated in FP64 across K chunks
 // Every mbarrier wait is bounded by a %globaltimer limit; on expiry the
 // kernel records an error code in g_tc_status, drains its own TMA copies,
-// releases TMEM and returns.
+// waits for its issued products, releases TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -25,26 +27,38 @@
 
 namespace acesb200 {
 
-// hi = bf16(x) (round to nearest even), lo = bf16(x - hi); padding is zero.
-__global__ void k_split_pack(__nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
-                             const double *__restrict__ src, long long ld, int rows, int k,
-                             int rows_pad, int k_pad) {
-  long long total = (long long)rows_pad * k_pad;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+// hi = bf16(x) (round to nearest even), lo = bf16(x - hi); K padding is zero.
+// Each thread converts two neighbouring K elements and stores them as one
+// 32-bit BF16 pair per plane; Wide = false splits the pair index with FastDiv.
+template <bool Wide>
+__global__ void k_split_pack(__nv_bfloat162 *__restrict__ hi, __nv_bfloat162 *__restrict__ lo,
+                             const double *__restrict__ src, long long ld, int k,
+                             long long total_pairs, FastDiv fpairs) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total_pairs;
        idx += (long long)gridDim.x * blockDim.x) {
-    int r = (int)(idx / k_pad), c = (int)(idx % k_pad);
-    double xd = 0.0;
-    if (r < rows && c < k) xd = src[(long long)r * ld + c];
-    __nv_bfloat16 h = __float2bfloat16_rn((float)xd);
-    float rem = (float)(xd - (double)__bfloat162float(h));
-    hi[idx] = h;
-    lo[idx] = __float2bfloat16_rn(rem);
+    long long r;
+    int c;
+    if (Wide) {
+      r = idx / fpairs.d;
+      c = 2 * (int)(idx - r * fpairs.d);
+    } else {
+      const unsigned q = fpairs.div((unsigned)idx);
+      r = q;
+      c = 2 * (int)((unsigned)idx - q * fpairs.d);
+    }
+    const double *row = src + r * ld;
+    const double x0 = c < k ? row[c] : 0.0, x1 = c + 1 < k ? row[c + 1] : 0.0;
+    const __nv_bfloat16 h0 = __float2bfloat16_rn((float)x0), h1 = __float2bfloat16_rn((float)x1);
+    const float r0 = (float)(x0 - (double)__bfloat162float(h0));
+    const float r1 = (float)(x1 - (double)__bfloat162float(h1));
+    hi[idx] = __halves2bfloat162(h0, h1);
+    lo[idx] = __halves2bfloat162(__float2bfloat16_rn(r0), __float2bfloat16_rn(r1));
   }
 }
 
 int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int k,
                cudaStream_t st) {
-  int rp = (rows + kSplitRowPad - 1) / kSplitRowPad * kSplitRowPad;
+  int rp = rows;
   int kp = (k + kSplitKPad - 1) / kSplitKPad * kSplitKPad;
   size_t need = (size_t)rp * kp * 2 * 2;
   if (!op.hi || op.cap < need) {
@@ -65,11 +79,16 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
   op.rows_pad = rp;
   op.k_pad = kp;
   op.lo = (char *)op.hi + (size_t)rp * kp * 2;
-  long long total = (long long)rp * kp;
-  long long nb = (total + 255) / 256;
+  const long long pairs = (long long)rp * (kp / 2);
+  long long nb = (pairs + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_split_pack<<<(unsigned)nb, 256, 0, st>>>((__nv_bfloat16 *)op.hi, (__nv_bfloat16 *)op.lo, src,
-                                             ld, rows, k, rp, kp);
+  const FastDiv fp((unsigned)(kp / 2));
+  if (pairs < (1LL << 31))
+    k_split_pack<false><<<(unsigned)nb, 256, 0, st>>>(
+        (__nv_bfloat162 *)op.hi, (__nv_bfloat162 *)op.lo, src, ld, k, pairs, fp);
+  else
+    k_split_pack<true><<<(unsigned)nb, 256, 0, st>>>(
+        (__nv_bfloat162 *)op.hi, (__nv_bfloat162 *)op.lo, src, ld, k, pairs, fp);
   count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -78,7 +97,7 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 namespace {
 constexpr int TBM = 128, TBN = 128, TBK = 64, STAGES = 3;
 #ifndef ACES_TC_CHUNK
-#define ACES_TC_CHUNK 4
+#define ACES_TC_CHUNK 8
 #endif
 constexpr int CHUNK = ACES_TC_CHUNK;                  // k tiles per FP32 accumulation chunk
 constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
@@ -86,6 +105,8 @@ constexpr int TILE_B = TBN * TBK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment + barriers
 constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
+constexpr int kCols = 4 * TBN / kEpiWarps;            // accumulator columns per epilogue thread
+static_assert(kCols % 32 == 0 && kCols >= 32, "epilogue column span");
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols = 2 * TBN;                    // two ping-pong accumulators
 constexpr unsigned long long kWaitNs = 4000000000ULL;  // 4 s bound on any wait
@@ -180,7 +201,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // FP64 registers while the next chunk is computed.  This bounds the number of
 // FP32 tensor-core accumulations any partial sum sees to 12*CHUNK, so the
 // truncation bias of the tensor-core adders stays small instead of growing
-// with K.
+// with K.  The energy error of a CCSD solve grows linearly with CHUNK (o=20,
+// v=180: 1.4e-8 Eh at 2, 2.7e-8 at 4, 5.3e-8 at 8) while the drain cost per
+// product halves with every doubling; 8 keeps the error 20x inside 1e-6 Eh.
 //
 // The kernel is persistent: gridDim.x <= #SMs CTAs walk the output tiles
 // t = blockIdx.x, blockIdx.x + gridDim.x, ... (n tile fastest, then m tile,
@@ -327,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp >= 2) {
     // ---------------- epilogue: FP64 accumulation of the chunks ----------------
     const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
-    const int half = (warp - 2) >> 2;      // which 64 accumulator columns
+    const int half = (warp - 2) >> 2;      // which kCols accumulator columns
     const int row = q * 32 + lane;
     // lanes are consecutive output rows: with unit m stride a warp's stores coalesce
     const bool coalesced = C.sm0 == 1;
@@ -337,10 +360,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       int m0, n0, z, ktb, kTiles;
       sch.decode(t, m0, n0, z, ktb, kTiles);
       const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
-      const int ncol = min(64, N - (n0 + half * 64));  // live columns of this warp (may be <= 0)
-      double acc[64];
+      const int ncol = min(kCols, N - (n0 + half * kCols));  // live columns (may be <= 0)
+      double acc[kCols];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int j = 0; j < kCols; ++j) acc[j] = 0.0;
       for (int c = 0; c < nChunks; ++c, ++gc) {
         const int b = gc & 1;
         const bool w = mbar_wait(smem_u32(&acc_full[b]), (gc >> 1) & 1);
@@ -349,9 +372,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tbase =
-            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * 64);
+            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * kCols);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < kCols / 32; ++h) {
           if (ncol > h * 32) {  // warp-uniform: skip column groups past N
             uint32_t r[32];
             tmem_ld32(tbase + h * 32, r);
@@ -367,39 +390,41 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!ok) break;
       const int m = m0 + row;
       if (m >= M || ncol <= 0) continue;
-      const int nb = n0 + half * 64;
+      const int nb = n0 + half * kCols;
       if (part) {
         // split-K partial, [z][n][m]: lanes write consecutive m
         double *pz = part + (size_t)z * M * N + m;
 #pragma unroll
-        for (int j = 0; j < 64; ++j)
+        for (int j = 0; j < kCols; ++j)
           if (j < ncol) pz[(size_t)(nb + j) * M] = acc[j];
       } else {
-        const long long mo = (m / C.mdiv) * C.sm1 + (m % C.mdiv) * C.sm0;
-        auto addr = [&](int n) -> double * {
-          return C.p + mo + (n / C.ndiv) * C.sn1 + (n % C.ndiv) * C.sn0;
-        };
+        double *const cm = C.p + cview_dim(C.mdiv, C.sm1, C.sm0, m);
+        CViewNWalk w(C, nb);
         if (beta == 0.0) {
 #pragma unroll
-          for (int j = 0; j < 64; ++j)
-            if (j < ncol) *addr(nb + j) = alpha * acc[j];
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) cm[w.off] = alpha * acc[j];
         } else if (beta == 1.0 && coalesced) {
           // one fire-and-forget FP64 add per element (RED): every element has a
           // single owner thread, so the result equals load + add + store
 #pragma unroll
-          for (int j = 0; j < 64; ++j)
-            if (j < ncol) atomicAdd(addr(nb + j), alpha * acc[j]);
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) atomicAdd(cm + w.off, alpha * acc[j]);
         } else {
           // read-modify-write in batches of 8: all loads of a batch are issued
           // before its stores, so the memory latency is paid once per batch
 #pragma unroll
-          for (int j0 = 0; j0 < 64; j0 += 8) {
+          for (int j0 = 0; j0 < kCols; j0 += 8) {
             double old[8];
+            long long off[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) old[j] = j0 + j < ncol ? __ldg(addr(nb + j0 + j)) : 0.0;
+            for (int j = 0; j < 8; ++j, w.next()) {
+              off[j] = w.off;
+              old[j] = j0 + j < ncol ? __ldg(cm + off[j]) : 0.0;
+            }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
-              if (j0 + j < ncol) *addr(nb + j0 + j) = alpha * acc[j0 + j] + beta * old[j];
+              if (j0 + j < ncol) cm[off[j]] = alpha * acc[j0 + j] + beta * old[j];
           }
         }
       }
@@ -470,8 +495,8 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st) {
   if (M <= 0 || N <= 0) return ACES_OK;
-  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad < TBM ||
-      B.rows_pad < TBN || A.k_pad == 0) {
+  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad < M ||
+      B.rows_pad < N || A.k_pad == 0) {
     set_error("gemm_nt_bf16x3: operand shapes do not match (%d/%d, %d, %d)", A.k_pad, B.k_pad,
               A.rows, B.rows);
     return ACES_ERR_ARG;
@@ -531,8 +556,7 @@ SplitOperand split_view(const SplitOperand &p, int row0, int rows) {
   v.hi = (char *)p.hi + off;
   v.lo = (char *)p.lo + off;
   v.rows = rows;
-  int rp = (rows + kSplitRowPad - 1) / kSplitRowPad * kSplitRowPad;
-  v.rows_pad = std::min(rp, p.rows_pad - row0);  // beyond it the tensor map zero-fills
+  v.rows_pad = std::min(rows, p.rows_pad - row0);  // beyond it the tensor map zero-fills
   v.cap = 0;
   return v;
 }

@@ -1,5 +1,6 @@
 // kernels.cu -- bandwidth-bound kernels of the CC engine: resorts, FTAU,
 // NEWT2/E4SENG, CMPENG, DIIS reductions, the DIIS solve and DPD gathers.
+#include <algorithm>
 #include <cstdio>
 
 #include "common.cuh"
@@ -17,16 +18,28 @@ struct PermArgs {
   double alpha[4];
   long long s[4][4];
   double beta;
+  FastDiv fd1, fd2, fd3;  // divisors n[1], n[2], n[3]
 };
 
+// Wide = false: element count below 2^31, indices split with FastDiv.
+template <bool Wide>
 __global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long total) {
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    long long r = idx;
-    int i3 = r % a.n[3]; r /= a.n[3];
-    int i2 = r % a.n[2]; r /= a.n[2];
-    int i1 = r % a.n[1]; r /= a.n[1];
-    int i0 = (int)r;
+    int i0, i1, i2, i3;
+    if (Wide) {
+      long long r = idx;
+      i3 = r % a.n[3]; r /= a.n[3];
+      i2 = r % a.n[2]; r /= a.n[2];
+      i1 = r % a.n[1]; r /= a.n[1];
+      i0 = (int)r;
+    } else {
+      unsigned r = (unsigned)idx, q;
+      q = a.fd3.div(r); i3 = (int)(r - q * a.fd3.d); r = q;
+      q = a.fd2.div(r); i2 = (int)(r - q * a.fd2.d); r = q;
+      q = a.fd1.div(r); i1 = (int)(r - q * a.fd1.d);
+      i0 = (int)q;
+    }
     double acc = a.beta == 0.0 ? 0.0 : a.beta * out[idx];
     for (int t = 0; t < a.nterms; ++t)
       acc += a.alpha[t] * __ldg(a.src[t] + i0 * a.s[t][0] + i1 * a.s[t][1] + i2 * a.s[t][2] +
@@ -94,6 +107,9 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
   if (total == 0) return ACES_OK;
   a.nterms = spec.nterms;
   a.beta = spec.beta;
+  a.fd1 = FastDiv((unsigned)a.n[1]);
+  a.fd2 = FastDiv((unsigned)a.n[2]);
+  a.fd3 = FastDiv((unsigned)a.n[3]);
   for (int t = 0; t < 4; ++t) {
     a.src[t] = t < spec.nterms ? spec.t[t].src : nullptr;
     a.alpha[t] = t < spec.nterms ? spec.t[t].alpha : 0.0;
@@ -125,7 +141,11 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
   } else {
     long long nb = (total + 255) / 256;
     if (nb > 148 * 64) nb = 148 * 64;
-    k_permute_naive<<<(unsigned)nb, 256, 0, st>>>(out, a, total); count_launch();
+    if (total < (1LL << 31))
+      k_permute_naive<false><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
+    else
+      k_permute_naive<true><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
+    count_launch();
   }
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -134,16 +154,37 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Elementwise
 // ---------------------------------------------------------------------------
+// [i,j,a,b] index of an o*o*v*v element: pair p = i*o + j (below 2^31 / v^2)
+// and ab = a*v + b split with FastDiv
+struct Ijab {
+  int i, j, a, b;
+};
+__device__ __forceinline__ Ijab split_ijab(long long idx, const FastDiv &fvv, const FastDiv &fv,
+                                           const FastDiv &fo) {
+  Ijab r;
+  unsigned p, ab;
+  if (idx < (1LL << 31)) {
+    p = fvv.div((unsigned)idx);
+    ab = (unsigned)idx - p * fvv.d;
+  } else {  // 64-bit division only past 2^31 elements; the pair index still fits
+    const long long q = idx / fvv.d;
+    p = (unsigned)q;
+    ab = (unsigned)(idx - q * fvv.d);
+  }
+  r.a = (int)fv.div(ab);
+  r.b = (int)(ab - (unsigned)r.a * fv.d);
+  r.i = (int)fo.div(p);
+  r.j = (int)(p - (unsigned)r.i * fo.d);
+  return r;
+}
+
 __global__ void k_tau(double *__restrict__ tau, const double *__restrict__ t2,
-                      const double *__restrict__ t1, double c, int o, int v, long long total) {
+                      const double *__restrict__ t1, double c, int o, int v, long long total,
+                      FastDiv fvv, FastDiv fv, FastDiv fo) {
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    long long r = idx;
-    int b = r % v; r /= v;
-    int a = r % v; r /= v;
-    int j = r % o;
-    int i = (int)(r / o);
-    tau[idx] = t2[idx] + c * t1[i * v + a] * t1[j * v + b];
+    const Ijab x = split_ijab(idx, fvv, fv, fo);
+    tau[idx] = t2[idx] + c * t1[x.i * v + x.a] * t1[x.j * v + x.b];
   }
 }
 
@@ -152,36 +193,70 @@ void launch_tau(double *tau, const double *t2, const double *t1, double c, int o
   long long total = (long long)o * o * v * v;
   long long nb = (total + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
-  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total); count_launch();
+  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total, FastDiv((unsigned)(v * v)),
+                                      FastDiv((unsigned)v), FastDiv((unsigned)o));
+  count_launch();
 }
 
-__global__ void k_newt(double *__restrict__ t2n, const double *__restrict__ z2,
-                       double *__restrict__ t1n, const double *__restrict__ z1,
-                       const double *__restrict__ eo, const double *__restrict__ ev, int o, int v,
-                       long long total) {
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    long long r = idx;
-    int b = r % v; r /= v;
-    int a = r % v; r /= v;
-    int j = r % o;
-    int i = (int)(r / o);
-    long long tidx = (((long long)j * o + i) * v + b) * v + a;
-    double z = 0.5 * (z2[idx] + z2[tidx]);
-    t2n[idx] = z / (eo[i] + eo[j] - ev[a] - ev[b]);
-    if (idx < (long long)o * v) {
-      int ii = (int)(idx / v), aa = (int)(idx % v);
-      t1n[idx] = z1[idx] / (eo[ii] - ev[aa]);
+// NEWT2 for a closed-shell pair-symmetric T2: t2n[i,j,a,b] = t2n[j,i,b,a] =
+// (z2[i,j,a,b] + z2[j,i,b,a]) / 2 / (e_i + e_j - e_a - e_b).  One block per
+// (pair i <= j, 32 x 32 tile of (a, b)); the [j,i] block is read and written
+// through a shared-memory transpose so every global access is coalesced.
+__global__ void __launch_bounds__(256)
+    k_newt(double *__restrict__ t2n, const double *__restrict__ z2, double *__restrict__ t1n,
+           const double *__restrict__ z1, const double *__restrict__ eo,
+           const double *__restrict__ ev, int o, int v) {
+  __shared__ double tz[32][33];
+  __shared__ double tw[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  if (blockIdx.y == 0) {
+    // T1: z1 / (e_i - e_a), spread over the blocks of the first grid row
+    for (int e = blockIdx.x * 256 + threadIdx.x; e < o * v; e += gridDim.x * 256)
+      t1n[e] = z1[e] / (eo[e / v] - ev[e % v]);
+  }
+  const int tiles = (v + 31) / 32;
+  const int a0 = (blockIdx.x / tiles) * 32, b0 = (blockIdx.x % tiles) * 32;
+  const size_t vv = (size_t)v * v;
+  for (int pr = blockIdx.y; pr < o * o; pr += gridDim.y) {
+    const int i = pr / o, j = pr % o;
+    if (i > j) continue;  // block-uniform: the [j,i] pair is written by block [i,j]
+    const double *zij = z2 + ((size_t)i * o + j) * vv;
+    const double *zji = z2 + ((size_t)j * o + i) * vv;
+    double *wij = t2n + ((size_t)i * o + j) * vv;
+    double *wji = t2n + ((size_t)j * o + i) * vv;
+    __syncthreads();  // tz/tw of the previous pair are consumed
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
+      tz[bl][tx] = (a < v && b < v) ? zji[(size_t)b * v + a] : 0.0;
+    }
+    __syncthreads();
+    const double eij = eo[i] + eo[j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int al = ty + 8 * k, a = a0 + al, b = b0 + tx;
+      if (a < v && b < v) {
+        const double x = 0.5 * (zij[(size_t)a * v + b] + tz[tx][al]) / (eij - ev[a] - ev[b]);
+        wij[(size_t)a * v + b] = x;
+        tw[al][tx] = x;
+      }
+    }
+    if (i == j) continue;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
+      if (a < v && b < v) wji[(size_t)b * v + a] = tw[tx][bl];
     }
   }
 }
 
 void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, const double *eo,
                  const double *ev, int o, int v, cudaStream_t st) {
-  long long total = (long long)o * o * v * v;
-  long long nb = (total + 255) / 256;
-  if (nb > 148 * 32) nb = 148 * 32;
-  k_newt<<<(unsigned)nb, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, total); count_launch();
+  const int tiles = (v + 31) / 32;
+  dim3 grid((unsigned)(tiles * tiles), (unsigned)std::min(o * o, 65535));
+  k_newt<<<grid, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -209,20 +284,22 @@ __device__ void block_reduce(double (&vals)[N], double *out) {
   }
 }
 
+// E = sum tau[ijab] (2 V[ijab] - V[ijba]) + 2 sum f_ia t_ia, accumulated as
+// s0 = sum tau V, s1 = sum tau (V[ijab] - V[ijba]) / 2, s2 = 2 sum f t1.  For
+// real orbitals <ij|ba> = <ji|ab>, so the exchange integral is read from the
+// [j,i] pair block at the same (a, b): every load is coalesced.
 __global__ void k_energy(double *__restrict__ part, const double *__restrict__ t2,
                          const double *__restrict__ t1, const double *__restrict__ V,
-                         const double *__restrict__ fov, int o, int v, long long total) {
+                         const double *__restrict__ fov, int o, int v, long long total,
+                         FastDiv fvv, FastDiv fv, FastDiv fo) {
   double s[3] = {0.0, 0.0, 0.0};
+  const long long vv = (long long)v * v;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    long long r = idx;
-    int b = r % v; r /= v;
-    int a = r % v; r /= v;
-    int j = r % o;
-    int i = (int)(r / o);
-    double tau = t2[idx] + t1[i * v + a] * t1[j * v + b];
+    const Ijab x = split_ijab(idx, fvv, fv, fo);
+    double tau = t2[idx] + t1[x.i * v + x.a] * t1[x.j * v + x.b];
     double vij = V[idx];
-    double vji = V[idx - (long long)b - (long long)a * v + (long long)a + (long long)b * v];
+    double vji = V[idx + ((long long)(x.j - x.i) * o + (x.i - x.j)) * vv];
     s[0] += tau * vij;
     s[1] += 0.5 * tau * (vij - vji);
     if (idx < (long long)o * v) s[2] += 2.0 * fov[idx] * t1[idx];
@@ -242,7 +319,10 @@ __global__ void k_final_sum(double *out, const double *part, int nblk, int nv) {
 void launch_energy(double *out3, const double *t2, const double *t1, const double *voovv,
                    const double *fov, int o, int v, double *scratch, cudaStream_t st) {
   long long total = (long long)o * o * v * v;
-  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total); count_launch();
+  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total,
+                                       FastDiv((unsigned)(v * v)), FastDiv((unsigned)v),
+                                       FastDiv((unsigned)o));
+  count_launch();
   k_final_sum<<<3, 32, 0, st>>>(out3, scratch, kRedBlocks, 3); count_launch();
 }
 
@@ -262,34 +342,31 @@ struct HistPtrs {
   const double *p[25];
 };
 
-// dots of e with hist[k] over T1, T2(AB) and packed T2(AA) (i<j, a<b)
+// dots of e with hist[k] over T1, T2(AB) and packed T2(AA) (i<j, a<b).  The
+// AA block of a pair-symmetric vector x (x[i,j,a,b] = x[j,i,b,a], which every
+// amplitude, difference and extrapolated vector is, bit for bit) obeys
+//   sum_{i<j,a<b} (x_ijab - x_ijba)(y_ijab - y_ijba) = sum_{i<j} sum_ab x_ijab (y_ijab - y_jiab),
+// so the exchange partner is read from the [j,i] pair block at the same (a,b)
+// and every load is coalesced.
 __global__ void k_diis_dots(double *__restrict__ part, const double *__restrict__ e, HistPtrs h,
-                            int nh, int o, int v) {
+                            int nh, int o, int v, FastDiv fvv, FastDiv fv, FastDiv fo) {
   double s[25];
   for (int k = 0; k < 25; ++k) s[k] = 0.0;
   const long long n1 = (long long)o * v;
   const long long n2 = (long long)o * o * v * v;
+  const long long vv = (long long)v * v;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
        idx += (long long)gridDim.x * blockDim.x) {
-    double x = e[idx];
-    bool aa = false;
-    long long tix = 0;
+    const double x = e[idx];
+    long long tix = -1;
     if (idx >= n1) {
-      long long r = idx - n1;
-      int b = r % v; r /= v;
-      int a = r % v; r /= v;
-      int j = r % o;
-      int i = (int)(r / o);
-      if (i < j && a < b) {
-        aa = true;
-        tix = idx + (long long)(b - a) * v + (a - b);  // (i,j,b,a)
-      }
+      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
+      if (q.i < q.j) tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;  // [j,i,a,b]
     }
-    double xa = aa ? x - e[tix] : 0.0;
     for (int k = 0; k < nh; ++k) {
-      double y = h.p[k][idx];
+      const double y = h.p[k][idx];
       double acc = x * y;
-      if (aa) acc += xa * (y - h.p[k][tix]);
+      if (tix >= 0) acc += x * (y - h.p[k][tix]);
       s[k] += acc;
     }
   }
@@ -314,7 +391,9 @@ int launch_diis_dots(double *dots_out, const double *e_new, const double *const 
   if (nh < 1 || nh > 25) return ACES_ERR_ARG;
   HistPtrs h;
   for (int k = 0; k < 25; ++k) h.p[k] = k < nh ? hist[k] : nullptr;
-  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v); count_launch();
+  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v, FastDiv((unsigned)(v * v)),
+                                          FastDiv((unsigned)v), FastDiv((unsigned)o));
+  count_launch();
   k_final_sum<<<nh, 32, 0, st>>>(dots_out, scratch, kRedBlocks, 25); count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -328,23 +407,24 @@ __device__ inline void amax_merge(double &bv, long long &bi, double v, long long
   }
 }
 
+// largest |element| of T1, T2(AB) and packed T2(AA); the AA element
+// (i<j, a<b) x_ijab - x_ijba is formed as x_ijab - x_jiab (pair symmetry, see
+// k_diis_dots) so the partner load is coalesced
 __global__ void k_absmax(double *__restrict__ pv, long long *__restrict__ pi,
-                         const double *__restrict__ x, int o, int v) {
+                         const double *__restrict__ x, int o, int v, FastDiv fvv, FastDiv fv,
+                         FastDiv fo) {
   const long long n1 = (long long)o * v;
   const long long n2 = (long long)o * o * v * v;
+  const long long vv = (long long)v * v;
   double bv = 0.0;
   long long bi = 0x7fffffffffffffffLL;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
        idx += (long long)gridDim.x * blockDim.x) {
     amax_merge(bv, bi, x[idx], idx);
     if (idx >= n1) {
-      long long r = idx - n1;
-      int b = r % v; r /= v;
-      int a = r % v; r /= v;
-      int j = r % o;
-      int i = (int)(r / o);
-      if (i < j && a < b) {
-        long long tix = idx + (long long)(b - a) * v + (a - b);
+      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
+      if (q.i < q.j && q.a < q.b) {
+        const long long tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;
         amax_merge(bv, bi, x[idx] - x[tix], n1 + n2 + idx);
       }
     }
@@ -366,18 +446,27 @@ __global__ void k_absmax(double *__restrict__ pv, long long *__restrict__ pi,
   }
 }
 
+// one warp; amax_merge orders candidates by (|value| descending, index
+// ascending), a total order, so the merge order does not change the result
 __global__ void k_absmax_final(double *out, const double *pv, const long long *pi, int nb) {
   double bv = 0.0;
   long long bi = 0x7fffffffffffffffLL;
-  for (int b = 0; b < nb; ++b) amax_merge(bv, bi, pv[b], pi[b]);
-  out[0] = bv;
+  for (int b = threadIdx.x; b < nb; b += 32) amax_merge(bv, bi, pv[b], pi[b]);
+  for (int off = 16; off; off >>= 1) {
+    double ov = __shfl_down_sync(0xffffffff, bv, off);
+    long long oi = __shfl_down_sync(0xffffffff, bi, off);
+    amax_merge(bv, bi, ov, oi);
+  }
+  if (threadIdx.x == 0) out[0] = bv;
 }
 
 void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st) {
   double *pv = scratch;
   long long *pi = (long long *)(scratch + kRedBlocks);
-  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v); count_launch();
-  k_absmax_final<<<1, 1, 0, st>>>(out, pv, pi, kRedBlocks); count_launch();
+  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v, FastDiv((unsigned)(v * v)),
+                                       FastDiv((unsigned)v), FastDiv((unsigned)o));
+  count_launch();
+  k_absmax_final<<<1, 32, 0, st>>>(out, pv, pi, kRedBlocks); count_launch();
 }
 
 // Bordered DIIS system [[0,-1..],[-1,B]] (lam,c) = (-1,0,..) by LU with

@@ -134,6 +134,7 @@ const char *aces_last_error(void) { return g_err; }
 int aces_init(int device) {
   State &st = state();
   std::lock_guard<std::recursive_mutex> lk(st.mu);
+  if (st.device >= 0) engine_reset();
   st.arena.release();
   st.lists.clear();
   st.isytyp.clear();
@@ -148,6 +149,7 @@ int aces_fin(void) {
   State &st = state();
   std::lock_guard<std::recursive_mutex> lk(st.mu);
   if (st.device >= 0) cudaDeviceSynchronize();
+  engine_reset();
   st.arena.release();
   st.lists.clear();
   st.isytyp.clear();

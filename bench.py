@@ -397,6 +397,9 @@ KERNEL_CASES = {
     # T1-dressing shape W(ajb,i) = sum_e <ajb|e> t(i,e) at o=20, v=180:
     # M = o*v*v = 648000, N = o = 20, K = v = 180
     "thin-t1": dict(m=648000, n=20, k=180),
+    # T1-dressing rank-o update W(jbm,e) += sum_n t(n,e) X(jbm,n) at o=20, v=180,
+    # accumulated into the existing output: M = o*o*v = 72000, N = v = 180, K = o = 20
+    "lowrank-t1": dict(m=72000, n=180, k=20, beta=1.0),
 }
 
 
@@ -407,6 +410,7 @@ def run_kernel_case(a):
     import acesb200 as ab
     c = KERNEL_CASES[a.kernel_case]
     m, n, k = c["m"], c["n"], c["k"]
+    beta = c.get("beta", 0.0)
     lib = ab.load()
     lib.init(0)
     g = torch.Generator(device="cuda").manual_seed(0)
@@ -420,12 +424,12 @@ def run_kernel_case(a):
             torch.cuda.synchronize()
             e0.record()
             # C(m x n) = A^T(m x k) * B(k x n): column-major A stored (k x m) = our row-major (m,k)
-            lib.xgemm("T", "N", m, n, k, 1.0, A.data_ptr(), k, B.data_ptr(), k, 0.0,
+            lib.xgemm("T", "N", m, n, k, 1.0, A.data_ptr(), k, B.data_ptr(), k, beta,
                       C.data_ptr(), m, precision=prec)
             e1.record()
             torch.cuda.synchronize()
             out[name] = e0.elapsed_time(e1) * 1e-3
-    print(json.dumps({"kernel_case": a.kernel_case, "m": m, "n": n, "k": k,
+    print(json.dumps({"kernel_case": a.kernel_case, "m": m, "n": n, "k": k, "beta": beta,
                       "seconds_including_split_pack": out}), flush=True)
 
 
