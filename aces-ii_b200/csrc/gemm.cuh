@@ -114,6 +114,11 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 // acc = A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (TMEM), C = alpha*acc + beta*C (FP64).
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st);
+// Sum of up to 4 split products over one output: C = alpha sum_s A[s] B[s]^T
+// + beta C (K segments of a single launch; every A[s] has >= M rows and every
+// B[s] >= N rows, each segment its own K)
+int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
+                         double alpha, double beta, const CView &C, cudaStream_t st);
 
 // Rows [row0, row0 + rows) of a split operand (no copy).  The view's tensor
 // map ends at the parent's padded rows; rows past the view inside it belong

@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 #include "gemm.cuh"
@@ -225,11 +226,18 @@ struct TileSched {
   }
 };
 
+// K segments: C = alpha * sum_s A_s B_s^T + beta C, segment s owning the
+// global k tiles [kt0[s], kt0[s+1]) with its own tensor maps
+constexpr int kMaxSeg = 4;
+struct SegMaps {
+  CUtensorMap ah[kMaxSeg], al[kMaxSeg], bh[kMaxSeg], bl[kMaxSeg];
+  int kt0[kMaxSeg + 1];
+  int nseg;
+};
+
 __global__ void __launch_bounds__(kThreads, 1)
-    k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                  int M, int N, TileSched sch, int nTiles, double alpha, double beta, CView C,
-                  double *__restrict__ part) {
+    k_gemm_bf16x3(const __grid_constant__ SegMaps maps, int M, int N, TileSched sch, int nTiles,
+                  double alpha, double beta, CView C, double *__restrict__ part) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -289,11 +297,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t fb = smem_u32(&full[s]);
         unsigned char *st = smem + s * STAGE_BYTES;
         mbar_expect_tx(fb, STAGE_BYTES);
-        const int kx = (ktb + kt) * TBK;
-        tma_load_2d(smem_u32(st), &mAh, kx, m0, fb);
-        tma_load_2d(smem_u32(st + TILE_A), &mAl, kx, m0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A), &mBh, kx, n0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &mBl, kx, n0, fb);
+        const int g = ktb + kt;  // global k tile -> segment and its local k offset
+        int sg = 0;
+        while (sg + 1 < maps.nseg && g >= maps.kt0[sg + 1]) ++sg;
+        const int kx = (g - maps.kt0[sg]) * TBK;
+        tma_load_2d(smem_u32(st), &maps.ah[sg], kx, m0, fb);
+        tma_load_2d(smem_u32(st + TILE_A), &maps.al[sg], kx, m0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A), &maps.bh[sg], kx, n0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &maps.bl[sg], kx, n0, fb);
         ++it;
       }
     }
@@ -492,13 +503,11 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
 }
 }  // namespace
 
-int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
-                   double beta, const CView &C, cudaStream_t st) {
+int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
+                         double alpha, double beta, const CView &C, cudaStream_t st) {
   if (M <= 0 || N <= 0) return ACES_OK;
-  if (A.k_pad != B.k_pad || A.rows < M || B.rows < N || A.k_pad % TBK || A.rows_pad < M ||
-      B.rows_pad < N || A.k_pad == 0) {
-    set_error("gemm_nt_bf16x3: operand shapes do not match (%d/%d, %d, %d)", A.k_pad, B.k_pad,
-              A.rows, B.rows);
+  if (nseg < 1 || nseg > kMaxSeg) {
+    set_error("gemm_nt_bf16x3: %d K segments (1..%d)", nseg, kMaxSeg);
     return ACES_ERR_ARG;
   }
   static bool attr = false;
@@ -509,15 +518,29 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
     attr = true;
   }
-  CUtensorMap mAh, mAl, mBh, mBl;
-  ACES_TRY(make_map(&mAh, A.hi, A.rows_pad, A.k_pad, TBM));
-  ACES_TRY(make_map(&mAl, A.lo, A.rows_pad, A.k_pad, TBM));
-  ACES_TRY(make_map(&mBh, B.hi, B.rows_pad, B.k_pad, TBN));
-  ACES_TRY(make_map(&mBl, B.lo, B.rows_pad, B.k_pad, TBN));
+  SegMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  maps.nseg = nseg;
+  maps.kt0[0] = 0;
+  for (int g = 0; g < nseg; ++g) {
+    const SplitOperand &a = A[g], &b = B[g];
+    if (a.k_pad != b.k_pad || a.rows < M || b.rows < N || a.k_pad % TBK || a.rows_pad < M ||
+        b.rows_pad < N || a.k_pad == 0) {
+      set_error("gemm_nt_bf16x3: operand shapes of segment %d do not match (%d/%d, %d, %d)", g,
+                a.k_pad, b.k_pad, a.rows, b.rows);
+      return ACES_ERR_ARG;
+    }
+    ACES_TRY(make_map(&maps.ah[g], a.hi, a.rows_pad, a.k_pad, TBM));
+    ACES_TRY(make_map(&maps.al[g], a.lo, a.rows_pad, a.k_pad, TBM));
+    ACES_TRY(make_map(&maps.bh[g], b.hi, b.rows_pad, b.k_pad, TBN));
+    ACES_TRY(make_map(&maps.bl[g], b.lo, b.rows_pad, b.k_pad, TBN));
+    maps.kt0[g + 1] = maps.kt0[g] + a.k_pad / TBK;
+  }
+  for (int g = nseg + 1; g <= kMaxSeg; ++g) maps.kt0[g] = maps.kt0[nseg];
   TileSched sch;
   sch.tilesN = (N + TBN - 1) / TBN;
   sch.tilesM = (M + TBM - 1) / TBM;
-  sch.kTilesTotal = A.k_pad / TBK;
+  sch.kTilesTotal = maps.kt0[nseg];
   sch.ktc = sch.kTilesTotal;
   // split K when the output has too few tiles to fill the SMs
   const long long tiles = (long long)sch.tilesN * sch.tilesM;
@@ -542,12 +565,17 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
     return ACES_ERR_ARG;
   }
   const unsigned grid = (unsigned)std::min<long long>(nTiles, nsm);
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(mAh, mAl, mBh, mBl, M, N, sch, (int)nTiles,
-                                                     alpha, beta, C, part);
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(maps, M, N, sch, (int)nTiles, alpha, beta, C,
+                                                     part);
   count_launch();
   ACES_CUDA(cudaGetLastError());
   if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st, true);
   return ACES_OK;
+}
+
+int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
+                   double beta, const CView &C, cudaStream_t st) {
+  return gemm_nt_bf16x3_multi(&A, &B, 1, M, N, alpha, beta, C, st);
 }
 
 SplitOperand split_view(const SplitOperand &p, int row0, int rows) {

@@ -22,58 +22,121 @@
 namespace acesb200 {
 
 namespace {
-// orderings of (a,b,c): 012 021 102 120 201 210
-__constant__ int c_T[6][6][4];  // [reorder q][permutation p][abc, bca, cab, cba] -> slot
+// The six orderings s of a virtual set x = (x0, x1, x2): ordering s reads
+// W at (x[kOrd[s][0]], x[kOrd[s][1]], x[kOrd[s][2]]).
+constexpr int kOrd[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
 
+constexpr int ord_index(int a, int b, int c) {
+  for (int s = 0; s < 6; ++s)
+    if (kOrd[s][0] == a && kOrd[s][1] == b && kOrd[s][2] == c) return s;
+  return -1;
+}
+
+// kT.v[q][p][m]: for the triplet permutation p and the set ordering q, the
+// ordering of the set that supplies W_abc, W_bca, W_cab and W_cba (m = 0..3)
+// of the closed-shell energy expression.  Built at compile time so the
+// energy kernel indexes its six W values with constants (registers).
+struct TripleTable {
+  int v[6][6][4];
+};
+constexpr TripleTable make_triple_table() {
+  TripleTable t{};
+  const int args[4][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  int S[6][4] = {};
+  int comp[6][6] = {};
+  for (int p = 0; p < 6; ++p)
+    for (int m = 0; m < 4; ++m) {
+      int pos[3] = {0, 0, 0};
+      for (int r = 0; r < 3; ++r) pos[kOrd[p][r]] = args[m][r];
+      S[p][m] = ord_index(pos[0], pos[1], pos[2]);
+    }
+  for (int q = 0; q < 6; ++q)
+    for (int s = 0; s < 6; ++s)
+      comp[q][s] = ord_index(kOrd[q][kOrd[s][0]], kOrd[q][kOrd[s][1]], kOrd[q][kOrd[s][2]]);
+  for (int q = 0; q < 6; ++q)
+    for (int p = 0; p < 6; ++p)
+      for (int m = 0; m < 4; ++m) t.v[q][p][m] = comp[q][S[p][m]];
+  return t;
+}
+constexpr TripleTable kT = make_triple_table();
+
+// the table entries as template constants (usable in device code)
+template <int Q, int P, int M>
+struct TT {
+  static constexpr int value = kT.v[Q][P][M];
+};
+template <int Q, int P>
+__device__ __forceinline__ void accum_orders(const double (&u)[6], const double (&vd)[6],
+                                             double &g4, double &g5) {
+  constexpr int s0 = TT<Q, P, 0>::value, s1 = TT<Q, P, 1>::value, s2 = TT<Q, P, 2>::value,
+                s3 = TT<Q, P, 3>::value;
+  const double Z = 4.0 * u[s0] + u[s1] + u[s2];
+  g4 += Z * (u[s0] - u[s3]);
+  g5 += Z * (vd[s0] - vd[s3]);
+  if constexpr (P < 5) accum_orders<Q, P + 1>(u, vd, g4, g5);
+}
+template <int Q>
+__device__ __forceinline__ void accum_sets(const bool (&use)[6], const double (&u)[6],
+                                           const double (&vd)[6], double &g4, double &g5) {
+  if (use[Q]) accum_orders<Q, 0>(u, vd, g4, g5);
+  if constexpr (Q < 5) accum_sets<Q + 1>(use, u, vd, g4, g5);
+}
+
+// a >= b >= c from the flat index n of the set in the order
+// (a, then b <= a, then c <= b): n = a(a+1)(a+2)/6 + b(b+1)/2 + c
+__device__ __forceinline__ void decode_set(int n, int &a, int &b, int &c) {
+  int x = (int)cbrtf(6.0f * (float)n);
+  while ((long long)x * (x + 1) * (x + 2) / 6 > n) --x;
+  while ((long long)(x + 1) * (x + 2) * (x + 3) / 6 <= n) ++x;
+  a = x;
+  int r = n - (int)((long long)x * (x + 1) * (x + 2) / 6);
+  int y = (int)((sqrtf(8.0f * (float)r + 1.0f) - 1.0f) * 0.5f);
+  while (y * (y + 1) / 2 > r) --y;
+  while ((y + 1) * (y + 2) / 2 <= r) ++y;
+  b = y;
+  c = r - y * (y + 1) / 2;
+}
+
+// One triplet's contribution to E[4]T and E[5]ST: one thread per virtual set
+// {a >= b >= c}, all six orderings of the set read once; the distinct
+// orderings q of repeated virtuals are counted once.  Partial sums per block,
+// reduced in a fixed order.
 __global__ void __launch_bounds__(256)
     k_triples_energy(const double *__restrict__ W, const double *__restrict__ t1,
                      const double *__restrict__ Ioovv, const double *__restrict__ eo,
                      const double *__restrict__ ev, int i, int j, int k, int o, int v,
                      double scale, double *__restrict__ part) {
   const long long v2 = (long long)v * v;
-  const int ti[3] = {i, j, k};
-  double s4 = 0.0, s5 = 0.0;
+  const int nsets = v * (v + 1) * (v + 2) / 6;
   const double eijk = eo[i] + eo[j] + eo[k];
-  for (int a = blockIdx.x; a < v; a += gridDim.x) {
-    const int np = (a + 1) * (a + 1);
-    for (int idx = threadIdx.x; idx < np; idx += blockDim.x) {
-      const int b = idx / (a + 1), c = idx % (a + 1);
-      if (c > b) continue;
-      const int x[3] = {a, b, c};
-      const int ord[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-      double u[6], vd[6];
+  // the three <jk|..>, <ik|..>, <ij|..> slabs of <ij|ab> and the t1 rows
+  const double *Ijk = Ioovv + ((long long)j * o + k) * v2;
+  const double *Iik = Ioovv + ((long long)i * o + k) * v2;
+  const double *Iij = Ioovv + ((long long)i * o + j) * v2;
+  const double *ti = t1 + (long long)i * v, *tj = t1 + (long long)j * v, *tk = t1 + (long long)k * v;
+  double s4 = 0.0, s5 = 0.0;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nsets; n += gridDim.x * blockDim.x) {
+    int a, b, c;
+    decode_set(n, a, b, c);
+    // orderings (a,b,c) (a,c,b) (b,a,c) (b,c,a) (c,a,b) (c,b,a), as kOrd
+    const int ordv[6][3] = {{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a}, {c, a, b}, {c, b, a}};
+    double u[6], vd[6];
 #pragma unroll
-      for (int s = 0; s < 6; ++s) {
-        const int p0 = x[ord[s][0]], p1 = x[ord[s][1]], p2 = x[ord[s][2]];
-        u[s] = W[p0 * v2 + (long long)p1 * v + p2];
-        // V - W at (p0,p1,p2) for the triplet (i,j,k)
-        vd[s] = t1[(long long)ti[0] * v + p0] * Ioovv[(((long long)ti[1] * o + ti[2]) * v + p1) * v + p2] +
-                t1[(long long)ti[1] * v + p1] * Ioovv[(((long long)ti[0] * o + ti[2]) * v + p0) * v + p2] +
-                t1[(long long)ti[2] * v + p2] * Ioovv[(((long long)ti[0] * o + ti[1]) * v + p0) * v + p1];
-      }
-      const double D = eijk - ev[a] - ev[b] - ev[c];
-      double g4 = 0.0, g5 = 0.0;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        // skip orderings of (a,b,c) already counted (repeated virtuals)
-        bool dup = false;
-        for (int q2 = 0; q2 < q; ++q2)
-          if (x[ord[q2][0]] == x[ord[q][0]] && x[ord[q2][1]] == x[ord[q][1]] &&
-              x[ord[q2][2]] == x[ord[q][2]])
-            dup = true;
-        if (dup) continue;
-#pragma unroll
-        for (int pp = 0; pp < 6; ++pp) {
-          const int s0 = c_T[q][pp][0], s1 = c_T[q][pp][1], s2 = c_T[q][pp][2],
-                    s3 = c_T[q][pp][3];
-          const double Z = 4.0 * u[s0] + u[s1] + u[s2];
-          g4 += Z * (u[s0] - u[s3]);
-          g5 += Z * (vd[s0] - vd[s3]);
-        }
-      }
-      s4 += g4 / D;
-      s5 += g5 / D;
+    for (int s = 0; s < 6; ++s) {
+      const int p0 = ordv[s][0], p1 = ordv[s][1], p2 = ordv[s][2];
+      u[s] = W[p0 * v2 + (long long)p1 * v + p2];
+      // V - W at (p0,p1,p2): t_i^p0 <jk|p1p2> + t_j^p1 <ik|p0p2> + t_k^p2 <ij|p0p1>
+      vd[s] = ti[p0] * Ijk[p1 * v + p2] + tj[p1] * Iik[p0 * v + p2] + tk[p2] * Iij[p0 * v + p1];
     }
+    // ordering q duplicates an earlier one when the set repeats a virtual:
+    // a = b keeps q = 0, 1, 4; b = c keeps q = 0, 2, 3; a = b = c keeps q = 0
+    const bool ab = a == b, bc = b == c;
+    const bool use[6] = {true, !bc, !ab, !ab, !bc, !(ab || bc)};
+    const double D = eijk - ev[a] - ev[b] - ev[c];
+    double g4 = 0.0, g5 = 0.0;
+    accum_sets<0>(use, u, vd, g4, g5);
+    s4 += g4 / D;
+    s5 += g5 / D;
   }
   // block reduction (fixed order)
   __shared__ double sh[2][8];
@@ -92,10 +155,11 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-__global__ void k_sum_pairs(double *out, const double *part, long long n) {
-  // one warp, fixed order
+// sum of n (E4, E5) partial pairs: 1024 threads stride the list, then a
+// fixed-shape tree; the order of additions does not depend on timing
+__global__ void __launch_bounds__(1024) k_sum_pairs(double *out, const double *part, long long n) {
   double a = 0.0, b = 0.0;
-  for (long long t = threadIdx.x; t < n; t += 32) {
+  for (long long t = threadIdx.x; t < n; t += blockDim.x) {
     a += part[2 * t];
     b += part[2 * t + 1];
   }
@@ -103,40 +167,40 @@ __global__ void k_sum_pairs(double *out, const double *part, long long n) {
     a += __shfl_down_sync(0xffffffffu, a, off);
     b += __shfl_down_sync(0xffffffffu, b, off);
   }
-  if (threadIdx.x == 0) { out[0] = a; out[1] = b; }
-}
-
-void fill_tables() {
-  static bool done = false;
-  if (done) return;
-  const int O[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-  auto index_of = [&](int a, int b, int c) {
-    for (int s = 0; s < 6; ++s)
-      if (O[s][0] == a && O[s][1] == b && O[s][2] == c) return s;
-    return -1;
-  };
-  const int ARGS[4][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-  int S[6][4], COMP[6][6], T[6][6][4];
-  for (int p = 0; p < 6; ++p)
-    for (int m = 0; m < 4; ++m) {
-      int pos[3];
-      for (int r = 0; r < 3; ++r) pos[O[p][r]] = ARGS[m][r];
-      S[p][m] = index_of(pos[0], pos[1], pos[2]);
+  __shared__ double sa[32], sb[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sa[wid] = a; sb[wid] = b; }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    a = lane < nw ? sa[lane] : 0.0;
+    b = lane < nw ? sb[lane] : 0.0;
+    for (int off = 16; off; off >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, off);
+      b += __shfl_down_sync(0xffffffffu, b, off);
     }
-  for (int q = 0; q < 6; ++q)
-    for (int s = 0; s < 6; ++s) COMP[q][s] = index_of(O[q][O[s][0]], O[q][O[s][1]], O[q][O[s][2]]);
-  for (int q = 0; q < 6; ++q)
-    for (int p = 0; p < 6; ++p)
-      for (int m = 0; m < 4; ++m) T[q][p][m] = COMP[q][S[p][m]];
-  cudaMemcpyToSymbol(c_T, T, sizeof(T));
-  done = true;
+    if (lane == 0) { out[0] = a; out[1] = b; }
+  }
 }
 }  // namespace
 
+// The 12 contractions of a triplet (6 permutations x 2 terms) fall into three
+// classes by the position of the virtual that is not a pair index of the
+// pair-side operands: class c (W index c on the t2/H side, pairs (a,b)),
+// class a (pairs (b,c), index a) and class b (pairs (a,c), index b).  All four
+// terms of a class share one output orientation, so each class is ONE
+// tensor-core launch with four K segments (2 x K = v, 2 x K = o); every
+// output view has unit stride along m, the first class stores and the other
+// two accumulate with RED.  Per class and segment (P = permutation of (ijk)):
+//   class c:  t2[k,i] x Gv[j] (P4)   t2[k,j] x GvT[i] (P5)   -H[j,k] x t2P[i] (P0)   -H[i,k] x t2Q[j] (P2)
+//   class a:  Gv[k] x t2[i,j] (P0)   GvT[j] x t2[i,k] (P1)   t2P[j] x -H[k,i] (P3)   t2Q[k] x -H[j,i] (P5)
+//   class b:  Gv[k] x t2[j,i] (P2)   GvT[i] x t2[j,k] (P3)   t2P[i] x -H[k,j] (P1)   t2Q[k] x -H[i,j] (P4)
+// with Gv[z][(b,c),d] = (bd|cz), GvT[z][(c,b),d] = Gv[z][(b,c),d],
+// t2P[x][(a,b),l] = t2[x,l,a,b], t2Q[x][(b,a),l] = t2[x,l,a,b] and
+// H[y,z][c,l] = (cz|yl).
 int CCEngine::triples(double *e4, double *e5, double *seconds) {
   const long long O = o, V = v;
   const long long V2 = V * V, V3 = V * V * V;
-  fill_tables();
   cudaEvent_t t0, t1e;
   ACES_CUDA(cudaEventCreate(&t0));
   ACES_CUDA(cudaEventCreate(&t1e));
@@ -144,16 +208,20 @@ int CCEngine::triples(double *e4, double *e5, double *seconds) {
   const long long sv[4] = {V * V * V, V * V, V, 1};      // I_ovvv[m,a,e,f]
   const long long s3[4] = {O * O * V, O * V, V, 1};      // I_ooov[m,n,i,e]
   const long long st2[4] = {O * V * V, V * V, V, 1};     // t2[i,j,a,b]
-  DBuf Gv, t2P, H, Wb, part, outp;
-  // Gv[k,b,c,d] = (bd|ck) = <bc|dk> = I_ovvv[k,d,c,b]
+  DBuf Gv, GvT, t2P, t2Q, Hn, Wb, part, outp;
+  // Gv[k,b,c,d] = (bd|ck) = <bc|dk> = I_ovvv[k,d,c,b]; GvT[k,c,b,d] = Gv[k,b,c,d]
   ACES_TRY(alloc(Gv, O * V3));
   ACES_TRY(perm(Gv.p, o, v, v, v, 0.0, {PermTerm{I_ovvv.p, 1.0, {sv[0], sv[3], sv[2], sv[1]}}}));
-  // t2P[i,a,b,l] = t2[i,l,a,b]
+  ACES_TRY(alloc(GvT, O * V3));
+  ACES_TRY(perm(GvT.p, o, v, v, v, 0.0, {PermTerm{I_ovvv.p, 1.0, {sv[0], sv[2], sv[3], sv[1]}}}));
+  // t2P[i,a,b,l] = t2[i,l,a,b]; t2Q[i,b,a,l] = t2[i,l,a,b]
   ACES_TRY(alloc(t2P, O * O * V2));
   ACES_TRY(perm(t2P.p, o, v, v, o, 0.0, {PermTerm{t2(), 1.0, {st2[0], st2[2], st2[3], st2[1]}}}));
-  // H[j,k,c,l] = (ck|jl) = I_ooov[l,k,j,c]
-  ACES_TRY(alloc(H, O * O * O * V));
-  ACES_TRY(perm(H.p, o, o, v, o, 0.0, {PermTerm{I_ooov.p, 1.0, {s3[2], s3[1], s3[3], s3[0]}}}));
+  ACES_TRY(alloc(t2Q, O * O * V2));
+  ACES_TRY(perm(t2Q.p, o, v, v, o, 0.0, {PermTerm{t2(), 1.0, {st2[0], st2[3], st2[2], st2[1]}}}));
+  // Hn[j,k,c,l] = -(ck|jl) = -I_ooov[l,k,j,c] (the second terms enter with a minus sign)
+  ACES_TRY(alloc(Hn, O * O * O * V));
+  ACES_TRY(perm(Hn.p, o, o, v, o, 0.0, {PermTerm{I_ooov.p, -1.0, {s3[2], s3[1], s3[3], s3[0]}}}));
   ACES_TRY(alloc(Wb, V3));
   // triplets i >= j >= k
   std::vector<int> trip;
@@ -161,49 +229,91 @@ int CCEngine::triples(double *e4, double *e5, double *seconds) {
     for (int j = 0; j <= i; ++j)
       for (int k = 0; k <= j; ++k) { trip.push_back(i); trip.push_back(j); trip.push_back(k); }
   const int ntrip = (int)trip.size() / 3;
-  const int nblk = std::min(v, 296);
+  const int nblk = 148 * 4;
   ACES_TRY(alloc(part, (size_t)ntrip * nblk * 2));
   ACES_TRY(alloc(outp, 2));
-  // split operands of the first-term contractions (constant over triplets)
   const bool use_split = prec == ACES_PREC_BF16X3 && v >= 128;
-  SplitOperand sT2, sGv;
+  SplitOperand sT2, sGv, sGvT, sHn, sT2P, sT2Q;
   if (use_split) {
-    ACES_TRY(split_pack(sT2, t2(), V, o * o * v, v, st));   // rows (x,y,alpha), K = d
-    ACES_TRY(split_pack(sGv, Gv.p, V, o * v * v, v, st));   // rows (z,beta,gamma), K = d
+    ACES_TRY(split_pack(sT2, t2(), V, o * o * v, v, st));       // rows (x,y,alpha), K = d
+    ACES_TRY(split_pack(sGv, Gv.p, V, o * v * v, v, st));       // rows (z,beta,gamma), K = d
+    ACES_TRY(split_pack(sGvT, GvT.p, V, o * v * v, v, st));     // rows (z,gamma,beta), K = d
+    ACES_TRY(split_pack(sHn, Hn.p, O, o * o * v, o, st));       // rows (y,z,gamma), K = l
+    ACES_TRY(split_pack(sT2P, t2P.p, O, o * v * v, o, st));     // rows (x,alpha,beta), K = l
+    ACES_TRY(split_pack(sT2Q, t2Q.p, O, o * v * v, o, st));     // rows (x,beta,alpha), K = l
+    // the FP64 copies are not read again
+    for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q}) {
+      ACES_CUDA(cudaStreamSynchronize(st));
+      cudaFree(b->p);
+      b->p = nullptr;
+    }
   }
-  const long long sW[3] = {V2, V, 1};  // W strides of the virtuals paired with i, j, k
-  for (int t = 0; t < ntrip; ++t) {
-    const int ti[3] = {trip[3 * t], trip[3 * t + 1], trip[3 * t + 2]};
-    // the 6 permutations (x,y,z) of positions (0,1,2)
-    const int P[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-    for (int pp = 0; pp < 6; ++pp) {
-      const int px = P[pp][0], py = P[pp][1], pz = P[pp][2];
-      const int x = ti[px], y = ti[py], z = ti[pz];
-      // first term: C[alpha, (beta,gamma)] = sum_d t2[x,y,alpha,d] Gv[z][(beta,gamma), d]
-      CView c1{Wb.p, kHugeView, 0, sW[px], V, sW[py], sW[pz]};
-      double beta1 = pp == 0 ? 0.0 : 1.0;
-      if (use_split) {
-        SplitOperand a = split_view(sT2, (x * o + y) * v, v);
-        SplitOperand b = split_view(sGv, z * v * v, v * v);
-        ACES_TRY(gemm_nt_bf16x3(a, b, v, v * v, 1.0, beta1, c1, st));
-      } else {
-        ACES_TRY(gemm_nt_f64(v, v * v, v, 1.0, t2() + ((long long)x * o + y) * V2, V,
-                             Gv.p + (long long)z * V3, V, beta1, c1, st));
+  // operand views: R = v rows of t2[x,y] or Hn[y,z]; Q = v^2 pair rows of Gv/GvT/t2P/t2Q[z]
+  struct Opd {
+    const SplitOperand *sp;
+    const double *p;
+    long long ld;
+    long long row0;
+    int rows;
+  };
+  auto T2r = [&](int x, int y) { return Opd{&sT2, t2(), V, ((long long)x * o + y) * V, v}; };
+  auto Hr = [&](int y, int z) { return Opd{&sHn, Hn.p, O, ((long long)y * o + z) * V, v}; };
+  auto Gq = [&](int z) { return Opd{&sGv, Gv.p, V, (long long)z * V2, v * v}; };
+  auto GTq = [&](int z) { return Opd{&sGvT, GvT.p, V, (long long)z * V2, v * v}; };
+  auto Pq = [&](int x) { return Opd{&sT2P, t2P.p, O, (long long)x * V2, v * v}; };
+  auto Qq = [&](int x) { return Opd{&sT2Q, t2Q.p, O, (long long)x * V2, v * v}; };
+  // one class: C(view) = beta C + sum_s A_s B_s^T
+  auto run_class = [&](const Opd (&A)[4], const Opd (&B)[4], int M, int N, const CView &cv,
+                       double beta) -> int {
+    if (use_split) {
+      SplitOperand a[4], b[4];
+      for (int g = 0; g < 4; ++g) {
+        a[g] = split_view(*A[g].sp, (int)A[g].row0, A[g].rows);
+        b[g] = split_view(*B[g].sp, (int)B[g].row0, B[g].rows);
       }
-      // second term: C[(alpha,beta), gamma] -= sum_l t2P[x][(alpha,beta), l] H[y,z][gamma, l]
-      CView c2{Wb.p, V, sW[px], sW[py], kHugeView, 0, sW[pz]};
-      ACES_TRY(gemm_nt_f64(v * v, v, o, -1.0, t2P.p + (long long)x * V2 * O, O,
-                           H.p + ((long long)y * O + z) * V * O, O, 1.0, c2, st));
+      return gemm_nt_bf16x3_multi(a, b, 4, M, N, 1.0, beta, cv, st);
+    }
+    for (int g = 0; g < 4; ++g) {
+      const int K = A[g].ld == V ? v : o;
+      ACES_TRY(gemm_nt_f64(M, N, K, 1.0, A[g].p + A[g].row0 * A[g].ld, A[g].ld,
+                           B[g].p + B[g].row0 * B[g].ld, B[g].ld, g == 0 ? beta : 1.0, cv, st));
+    }
+    return ACES_OK;
+  };
+  const CView vc{nullptr, kHugeView, 0, 1, V, V2, V};   // m = c, n = (a,b)
+  const CView va{nullptr, V, V, 1, kHugeView, 0, V2};   // m = (b,c), n = a
+  const CView vb{nullptr, V, V2, 1, kHugeView, 0, V};   // m = (a,c), n = b
+  for (int t = 0; t < ntrip; ++t) {
+    const int i = trip[3 * t], j = trip[3 * t + 1], k = trip[3 * t + 2];
+    CView cv = vc;
+    cv.p = Wb.p;
+    {
+      const Opd A[4] = {T2r(k, i), T2r(k, j), Hr(j, k), Hr(i, k)};
+      const Opd B[4] = {Gq(j), GTq(i), Pq(i), Qq(j)};
+      ACES_TRY(run_class(A, B, v, v * v, cv, 0.0));
+    }
+    cv = va;
+    cv.p = Wb.p;
+    {
+      const Opd A[4] = {Gq(k), GTq(j), Pq(j), Qq(k)};
+      const Opd B[4] = {T2r(i, j), T2r(i, k), Hr(k, i), Hr(j, i)};
+      ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
+    }
+    cv = vb;
+    cv.p = Wb.p;
+    {
+      const Opd A[4] = {Gq(k), GTq(i), Pq(i), Qq(k)};
+      const Opd B[4] = {T2r(j, i), T2r(j, k), Hr(k, j), Hr(i, j)};
+      ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
     }
     int mult = 1;
-    if (ti[0] == ti[1] && ti[1] == ti[2]) mult = 6;
-    else if (ti[0] == ti[1] || ti[1] == ti[2]) mult = 2;
-    k_triples_energy<<<nblk, 256, 0, st>>>(Wb.p, t1(), I_oovv.p, eo.p, ev.p, ti[0], ti[1], ti[2],
-                                           o, v, 1.0 / (3.0 * mult),
-                                           part.p + (size_t)t * nblk * 2);
+    if (i == j && j == k) mult = 6;
+    else if (i == j || j == k) mult = 2;
+    k_triples_energy<<<nblk, 256, 0, st>>>(Wb.p, t1(), I_oovv.p, eo.p, ev.p, i, j, k, o, v,
+                                           1.0 / (3.0 * mult), part.p + (size_t)t * nblk * 2);
     count_launch();
   }
-  k_sum_pairs<<<1, 32, 0, st>>>(outp.p, part.p, (long long)ntrip * nblk);
+  k_sum_pairs<<<1, 1024, 0, st>>>(outp.p, part.p, (long long)ntrip * nblk);
   count_launch();
   double h[2];
   ACES_CUDA(cudaMemcpyAsync(h, outp.p, 16, cudaMemcpyDeviceToHost, st));
@@ -220,12 +330,12 @@ int CCEngine::triples(double *e4, double *e5, double *seconds) {
   *e5 = h[1];
   cudaEventDestroy(t0);
   cudaEventDestroy(t1e);
-  for (DBuf *b : {&Gv, &t2P, &H, &Wb, &part, &outp}) {
-    cudaFree(b->p);
+  for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp}) {
+    if (b->p) cudaFree(b->p);
     b->p = nullptr;
   }
-  if (sT2.hi) cudaFree(sT2.hi);
-  if (sGv.hi) cudaFree(sGv.hi);
+  for (SplitOperand *sp : {&sT2, &sGv, &sGvT, &sHn, &sT2P, &sT2Q})
+    if (sp->hi) cudaFree(sp->hi);
   if (!std::isfinite(*e4) || !std::isfinite(*e5)) {
     set_error("(T): non-finite energy");
     return ACES_ERR_NAN;
