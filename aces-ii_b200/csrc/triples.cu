@@ -4,10 +4,11 @@
 // For every occupied triplet i >= j >= k the connected triples
 //   W_ijk^abc = sum over the 6 simultaneous permutations of (ia)(jb)(kc) of
 //     X_ijk^abc = sum_d t(ij,ad) (bd|ck) - sum_l t(il,ab) (ck|jl)
-// are built in one v^3 FP64 buffer by 12 contractions whose permuted outputs
-// land in place (two-level output views).  The energy kernel then sums, for
-// the distinct permutations of (i,j,k) and all orderings of every virtual set
-// {a>=b>=c}, the closed-shell expression
+// are built in one v^3 FP64 buffer by three tensor-core launches (the 12
+// contractions grouped by output orientation, four K segments each) whose
+// outputs land in place through coalesced two-level views.  The energy kernel
+// then sums, for the distinct permutations of (i,j,k) and all orderings of
+// every virtual set {a>=b>=c}, the closed-shell expression
 //   E[4]T  = 1/3 sum (4W_abc + W_bca + W_cab)(W_abc - W_cba)/D_ijk^abc
 //   E[5]ST = 1/3 sum (4W_abc + W_bca + W_cab)(V_abc - V_cba)/D_ijk^abc,
 //   V - W = t_i^a (jb|kc) + t_j^b (ia|kc) + t_k^c (ia|jb),

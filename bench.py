@@ -49,8 +49,9 @@ def args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64-compare", action="store_true")
     p.add_argument("--kernel-case", default=None,
-                   help="run one contraction shape through aces_xgemm and exit "
-                        "(small cases for ncu captures): ladder-small")
+                   help="run one small case for ncu captures and exit: a contraction "
+                        "shape through aces_xgemm (ladder-small, thin-t1, lowrank-t1) or "
+                        "CCSD(T) on a small system (triples-o10-v180)")
     return p.parse_args()
 
 
@@ -233,7 +234,10 @@ def run_ours(a, rank, world, local_rank):
                 "peak_source": f"bf16_tflops_sustained of {pk_src} MEASURED_PEAKS.json",
                 "algorithmic_flops_per_launch": launch_flops,
                 "executed_bf16_flops_per_launch": executed,
-                "seconds_per_launch": s_lad, "traffic": LADDER_TRAFFIC.get(a.workload)}
+                "seconds_per_launch": s_lad, "traffic": LADDER_TRAFFIC.get(a.workload),
+                "traffic_source": LADDER_TRAFFIC_SOURCE if a.workload in LADDER_TRAFFIC else None,
+                "algorithmic_bytes_per_launch": 4.0 * (v * v) * (v * v) + 4.0 * (o * o) * (v * v)
+                + 8.0 * (o * o) * (v * v)}
     else:
         roof = {"bound": "tensor", "kernel": "k_gemm_nt_f64 (particle-particle ladder)",
                 "achieved": launch_flops / s_lad / 1e12, "peak": None, "unit": "TFLOP/s",
@@ -272,7 +276,13 @@ def run_ours(a, rank, world, local_rank):
     return line
 
 
-LADDER_TRAFFIC = {}  # filled from profiles/ once an ncu capture exists
+# DRAM bytes (read + write) per ladder launch: the ncu capture of the
+# ladder-small case (919.4 MB read, 37.1 MB written at M = K = 14400, N = 400;
+# profiles/k_gemm_bf16x3_ladder_small.md) scaled by the A operand that
+# dominates it, (32400 / 14400)^2 for c2
+LADDER_TRAFFIC = {"c2": (919.4e6 + 37.1e6) * (32400.0 / 14400.0) ** 2}
+LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the ladder-small "
+                         "capture, scaled by (M*K) c2 / ladder-small")
 
 
 def accuracy(lib, wname, device):
@@ -401,6 +411,31 @@ KERNEL_CASES = {
     # accumulated into the existing output: M = o*o*v = 72000, N = v = 180, K = o = 20
     "lowrank-t1": dict(m=72000, n=180, k=20, beta=1.0),
 }
+# whole-program cases: a converged CCSD(T) on a small seeded system (ncu
+# captures of the (T) launches; B scaled by 0.25 so the amplitudes converge)
+PROGRAM_CASES = {
+    "triples-o10-v180": dict(nocc=10, nvir=180, naux=540, seed=5, bscale=0.25),
+}
+
+
+def run_program_case(a):
+    """CCSD (split precision, CC_CONV=7) and (T) on a PROGRAM_CASES system;
+    prints the (T) device time and energies."""
+    import torch
+    import acesb200 as ab
+    from acesb200.workloads import synthetic_df
+    wl = PROGRAM_CASES[a.kernel_case]
+    eps, B, _ = synthetic_df(**wl)
+    e, lists, o, v = _lists_from_df(eps, B, wl["nocc"], wl["nvir"], torch.device("cuda", 0))
+    lib = ab.load()
+    lib.init(0)
+    lib.sym_init([o], [v])
+    put_lists(lib, e, lists)
+    c = lib.xvcc(cc_conv=7, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3, triples=1)
+    print(json.dumps({"kernel_case": a.kernel_case, "e_ccsd": c.e_ccsd, "cycles": c.ncycle,
+                      "e_t4": c.e_t4, "e_st5": c.e_st5,
+                      "seconds_triples": c.seconds_triples}), flush=True)
+    lib.fin()
 
 
 def run_kernel_case(a):
@@ -408,6 +443,8 @@ def run_kernel_case(a):
     the same shape in FP64 (DMMA); prints device times (CUDA events)."""
     import torch
     import acesb200 as ab
+    if a.kernel_case in PROGRAM_CASES:
+        return run_program_case(a)
     c = KERNEL_CASES[a.kernel_case]
     m, n, k = c["m"], c["n"], c["k"]
     beta = c.get("beta", 0.0)
