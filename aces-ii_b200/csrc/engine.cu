@@ -37,9 +37,10 @@ void CCEngine::release() {
   tape.clear();
   active.clear();
   for (DBuf *b : registry()) {
-    if (b->p) cudaFree(b->p);
+    if (b->p && !b->borrowed) cudaFree(b->p);
     b->p = nullptr;
     b->n = 0;
+    b->borrowed = false;
   }
   for (auto &b : hx) if (b.p) cudaFree(b.p);
   for (auto &b : he) if (b.p) cudaFree(b.p);
@@ -62,6 +63,10 @@ void CCEngine::release() {
 
 int CCEngine::alloc(DBuf &b, size_t n) {
   if (b.p && b.n >= n) return ACES_OK;
+  if (b.borrowed) {
+    set_error("engine: a borrowed list buffer cannot be reallocated");
+    return ACES_ERR_ARG;
+  }
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.n = 0;
@@ -422,7 +427,23 @@ int CCEngine::load_from_lists() {
     ACES_TRY(perm(I_ovvv.p, o, v, v, v, 0.0, {PT(tmp4.p, 1.0, 1, O, V * O, V * V * O)}));
     ACES_CUDA(cudaStreamSynchronize(st));
   }
-  // list 233 (13,13): <Ab|Cd> -> I_vvvv[a,b,c,d]
+  // list 233 (13,13): <Ab|Cd> -> I_vvvv[a,b,c,d].  Without symmetry the list
+  // block is the full v^2 x v^2 matrix with pair index a + b*v; read as a C
+  // array it is L[d][c][b][a] = <ab|cd> = <dc|ba> (real orbitals: bra-ket and
+  // electron-label symmetry), i.e. exactly I_vvvv: the engine borrows the
+  // list's device memory instead of gathering a second copy (42.5 GB at
+  // o = 30, v = 270).
+  if (s.nirrep == 1 && aces_isytyp(1, 233) == 13 && aces_isytyp(2, 233) == 13) {
+    double *lp = aces_list_devptr(1, 233);
+    int nc = 0, nr = 0;
+    if (lp && aces_list_dims(1, 233, &nc, &nr) == ACES_OK && (long long)nr == V * V &&
+        (long long)nc == V * V) {
+      I_vvvv.p = lp;
+      I_vvvv.n = (size_t)(V * V) * (V * V);
+      I_vvvv.borrowed = true;
+      return ACES_OK;
+    }
+  }
   {
     DevMap dm;
     ACES_TRY(make_map(dm, 233, 13, 13, irr_o, irr_v, false));

@@ -17,6 +17,7 @@ namespace acesb200 {
 struct DBuf {
   double *p = nullptr;
   size_t n = 0;
+  bool borrowed = false;  // memory owned by the list store, never freed here
 };
 
 class CCEngine {

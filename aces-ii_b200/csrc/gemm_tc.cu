@@ -6,7 +6,7 @@
 // lo = bf16(x - hi).  The kernel accumulates hi*hi + hi*lo + lo*hi for every
 // K slice into one TMEM accumulator (the lo*lo term, ~2^-18 relative, is
 // dropped), which gives ~16 significant bits per product and FP32 sums that
-// are promoted to FP64 every CHUNK k tiles.
+// are promoted to FP64 every CHUNK k tiles (8, or fewer for very long K).
 //
 // Persistent kernel, one CTA per SM, output tile 128 x 128, k tile 64,
 // 3-stage mbarrier pipeline, 10 warps:
@@ -97,10 +97,12 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 
 namespace {
 constexpr int TBM = 128, TBN = 128, TBK = 64, STAGES = 3;
-#ifndef ACES_TC_CHUNK
-#define ACES_TC_CHUNK 8
-#endif
-constexpr int CHUNK = ACES_TC_CHUNK;                  // k tiles per FP32 accumulation chunk
+// k tiles per FP32 accumulation chunk, by the contraction length K
+inline int chunk_for(int kTilesTotal) {
+  if (kTilesTotal <= 576) return 8;   // K <= 36864
+  if (kTilesTotal <= 1152) return 4;  // K <= 73728
+  return 2;
+}
 constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
 constexpr int TILE_B = TBN * TBK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
@@ -204,7 +206,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // truncation bias of the tensor-core adders stays small instead of growing
 // with K.  The energy error of a CCSD solve grows linearly with CHUNK (o=20,
 // v=180: 1.4e-8 Eh at 2, 2.7e-8 at 4, 5.3e-8 at 8) while the drain cost per
-// product halves with every doubling; 8 keeps the error 20x inside 1e-6 Eh.
+// product halves with every doubling; it also grows with the contraction
+// length (o=30, v=270 with 8 throughout: 7.8e-7 Eh), so CHUNK is 8 up to
+// K = 36864 and smaller beyond (chunk_for).
 //
 // The kernel is persistent: gridDim.x <= #SMs CTAs walk the output tiles
 // t = blockIdx.x, blockIdx.x + gridDim.x, ... (n tile fastest, then m tile,
@@ -237,7 +241,7 @@ struct SegMaps {
 
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ SegMaps maps, int M, int N, TileSched sch, int nTiles,
-                  double alpha, double beta, CView C, double *__restrict__ part) {
+                  int chunk, double alpha, double beta, CView C, double *__restrict__ part) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int m0, n0, z, ktb, kTiles;
       sch.decode(t, m0, n0, z, ktb, kTiles);
       for (int kt = 0; kt < kTiles; ++kt) {
-        const int kin = kt % CHUNK, b = gc & 1;
+        const int kin = kt % chunk, b = gc & 1;
         if (kin == 0 && gc >= 2 &&
             !mbar_wait(smem_u32(&acc_empty[b]), ((gc >> 1) - 1) & 1)) {
           atomicExch(&g_tc_status, 5);
@@ -349,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         umma_commit(smem_u32(&empty[s]));
         ++it;
-        if (kin == CHUNK - 1 || kt == kTiles - 1) {
+        if (kin == chunk - 1 || kt == kTiles - 1) {
           umma_commit(smem_u32(&acc_full[b]));
           ++gc;
         }
@@ -370,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
       int m0, n0, z, ktb, kTiles;
       sch.decode(t, m0, n0, z, ktb, kTiles);
-      const int nChunks = (kTiles + CHUNK - 1) / CHUNK;
+      const int nChunks = (kTiles + chunk - 1) / chunk;
       const int ncol = min(kCols, N - (n0 + half * kCols));  // live columns (may be <= 0)
       double acc[kCols];
 #pragma unroll
@@ -565,7 +569,8 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
     return ACES_ERR_ARG;
   }
   const unsigned grid = (unsigned)std::min<long long>(nTiles, nsm);
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(maps, M, N, sch, (int)nTiles, alpha, beta, C,
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(maps, M, N, sch, (int)nTiles,
+                                                     chunk_for(sch.kTilesTotal), alpha, beta, C,
                                                      part);
   count_launch();
   ACES_CUDA(cudaGetLastError());

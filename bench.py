@@ -121,8 +121,19 @@ def host_lists(wl, device):
     from acesb200 import INTEGRAL_LISTS
     from acesb200.workloads import synthetic_df
 
-    eps, B, irr = synthetic_df(**wl)
     o, v = wl["nocc"], wl["nvir"]
+    # the six lists are staged in pinned host memory: refuse rather than drive
+    # the host out of memory
+    need = 8.0 * (v ** 4 + o * v ** 3 + 2 * o * o * v * v + o ** 3 * v + o ** 4)
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except ImportError:
+        avail = None
+    if avail is not None and avail < 2.0 * need:
+        raise SystemExit(f"workload {wl}: host lists need {need / 1e9:.1f} GB pinned, "
+                         f"only {avail / 1e9:.1f} GB available")
+    eps, B, irr = synthetic_df(**wl)
     return _lists_from_df(eps, B, o, v, device)
 
 
@@ -246,11 +257,11 @@ def run_ours(a, rank, world, local_rank):
                 "traffic": None}
 
     line = {
-        "metric": "CCSD s/iter, synthetic closed-shell o=20 v=180 naux=600 (split BF16x3 vs FP64 GPU)",
+        "metric": f"CCSD s/iter, synthetic closed-shell o={o} v={v} naux={wl['naux']} (split BF16x3 vs FP64 GPU)",
         "value": s_iter, "unit": "s/iter", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": s_iter * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16x3" if prec == ab.PREC_BF16X3 else "f64",
-        "data": "synthetic: seeded DF generator (acesb200.workloads c2)",
+        "data": f"synthetic: seeded DF generator (acesb200.workloads {a.workload})",
         "config": {"workload": f"{a.workload}: RHF-CCSD, C1, nocc={o}, nvir={v}, naux={wl['naux']}, "
                                f"seed={wl['seed']}",
                    "precision": a.precision, "cycles_timed": K, "diis_order": 5,
@@ -270,6 +281,7 @@ def run_ours(a, rank, world, local_rank):
     if fp64:
         line["fp64_gpu"] = fp64
     if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
+        del lists  # release the pinned host lists before the next workload's
         line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(a.workload, budget_s=90.0)
@@ -369,7 +381,7 @@ def run_reference(a, rank, world):
     cores = os.cpu_count()
     return {
         "impl": "reference",
-        "metric": "CCSD s/iter, synthetic closed-shell o=20 v=180 naux=600 (split BF16x3 vs FP64 GPU)",
+        "metric": f"CCSD s/iter, synthetic closed-shell o={wl['nocc']} v={wl['nvir']} naux={wl['naux']} (split BF16x3 vs FP64 GPU)",
         "value": v, "unit": "s/iter", "n_gpus": world, "steps": len(times), "warmup": W,
         "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded DF generator",
