@@ -209,9 +209,10 @@ class Lib:
                        verbose=verbose, timing_warmup=timing_warmup)
         return self._run("xvcc_run", cfg, allow_noconv)
 
-    def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0):
+    def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0,
+                timing_warmup=0):
         cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
-                       precision=precision, verbose=verbose)
+                       precision=precision, verbose=verbose, timing_warmup=timing_warmup)
         return self._run("xlambda_run", cfg)
 
     def xdens(self):

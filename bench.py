@@ -48,6 +48,8 @@ def args():
     p.add_argument("--workload", default=W_NAME)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64-compare", action="store_true")
+    p.add_argument("--no-lambda", action="store_true",
+                   help="skip the Lambda / density block (C4 system)")
     p.add_argument("--kernel-case", default=None,
                    help="run one small case for ncu captures and exit: a contraction "
                         "shape through aces_xgemm (ladder-small, thin-t1, lowrank-t1) or "
@@ -283,6 +285,8 @@ def run_ours(a, rank, world, local_rank):
     if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
         del lists  # release the pinned host lists before the next workload's
         line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank)
+    if prec == ab.PREC_BF16X3 and not a.no_lambda and a.workload == W_NAME:
+        line["lambda"] = lambda_block(lib, "c4conv", local_rank)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(a.workload, budget_s=90.0)
     return line
@@ -327,6 +331,71 @@ def accuracy(lib, wname, device):
                             - res["fp64"]["e_t4"] - res["fp64"]["e_st5"]),
             "speedup_per_iter": res["fp64"]["seconds_per_iter"] / res["bf16x3"]["seconds_per_iter"],
             "speedup_triples": res["fp64"]["seconds_triples"] / res["bf16x3"]["seconds_triples"]}
+
+
+def lambda_block(lib, wname, device, seed=4, delta=1e-4):
+    """Lambda equations + one-particle density on the convergent C4 system
+    (o=20, v=180, seed 3, B scaled by 1/4): Lambda s/iter for both precisions,
+    and dE/dx = Tr(D h') for f -> f + x h' (h' seeded, symmetric, N(0, 0.01^2)
+    entries) against a central finite difference (step delta) of FP64 CCSD
+    energies, and the split-precision density against the FP64 one."""
+    import time
+    import numpy as np
+    import torch
+    import acesb200 as ab
+    from acesb200.workloads import WORKLOADS, synthetic_df
+    wl = WORKLOADS[wname]
+    eps, B, irr = synthetic_df(**wl)
+    o, v = wl["nocc"], wl["nvir"]
+    n = o + v
+    lists = _lists_from_df(eps, B, o, v, torch.device("cuda", device))
+    rng = np.random.default_rng(seed)
+    hp = rng.normal(0.0, 0.01, (n, n))
+    hp = 0.5 * (hp + hp.T)
+    f0 = np.diag(eps)
+
+    def load(fock):
+        lib.init(device)
+        lib.sym_init([o], [v])
+        put_lists(lib, lists[0], lists[1])
+        lib.putrec("FOCKMAT", fock)
+
+    out = {"workload": f"{wname}: nocc={o}, nvir={v}, naux={wl['naux']}, seed={wl['seed']}, "
+                       f"B scaled by {wl.get('bscale', 1.0)}; h' seed {seed}",
+           "delta": delta}
+    dens = {}
+    # the split path's residual floor is ~5e-10 (CC_CONV 9); FP64 converges to 1e-10
+    for prec, name, conv in ((ab.PREC_FP64, "fp64", 10), (ab.PREC_BF16X3, "bf16x3", 9)):
+        load(f0)
+        c = lib.xvcc(cc_conv=conv, cc_maxcyc=80, cc_exporder=5, precision=prec)
+        t0 = time.perf_counter()
+        cl = lib.xlambda(cc_conv=conv, cc_maxcyc=80, cc_exporder=5, precision=prec,
+                         timing_warmup=1)
+        t1 = time.perf_counter()
+        lib.xdens()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        D = lib.getrec("DENSMAT", n * n).reshape(n, n)
+        dens[name] = D
+        out[name] = {"cc_conv": conv, "e_ccsd": c.e_ccsd, "ccsd_cycles": c.ncycle,
+                     "lambda_cycles": cl.ncycle, "lambda_converged": bool(cl.converged),
+                     "lambda_seconds_per_iter": cl.seconds_per_iter,
+                     "lambda_seconds_total": t1 - t0, "density_seconds": t2 - t1,
+                     "dE_dx_analytic": float(np.sum(D * hp))}
+    e = {}
+    for sgn in (+1, -1):
+        load(f0 + sgn * delta * hp)
+        e[sgn] = lib.xvcc(cc_conv=11, cc_maxcyc=100, cc_exporder=5, precision=ab.PREC_FP64).e_ccsd
+    fd = (e[+1] - e[-1]) / (2.0 * delta)
+    out["dE_dx_finite_difference_fp64"] = fd
+    out["abs_diff_analytic_fp64_vs_fd"] = abs(out["fp64"]["dE_dx_analytic"] - fd)
+    out["abs_diff_bf16x3_vs_fp64"] = abs(out["bf16x3"]["dE_dx_analytic"] -
+                                         out["fp64"]["dE_dx_analytic"])
+    out["max_abs_density_diff_bf16x3_vs_fp64"] = float(np.abs(dens["bf16x3"] - dens["fp64"]).max())
+    out["lambda_speedup_bf16x3_vs_fp64"] = (out["fp64"]["lambda_seconds_per_iter"] /
+                                            out["bf16x3"]["lambda_seconds_per_iter"])
+    lib.fin()
+    return out
 
 
 def cpu_baseline(wname, budget_s=90.0, steps=1):
