@@ -52,6 +52,7 @@ class CCConfig(C.Structure):
         ("seconds_per_iter", C.c_double), ("seconds_triples", C.c_double),
         ("seconds_ladder", C.c_double), ("flops_per_iter", C.c_double),
         ("launches_per_iter", C.c_longlong), ("seconds_setup", C.c_double),
+        ("triples_rank", C.c_int), ("triples_nranks", C.c_int),
     ]
 
 
@@ -203,10 +204,12 @@ class Lib:
         return cfg
 
     def xvcc(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, triples=0,
-             use_graph=0, verbose=0, allow_noconv=False, timing_warmup=0):
+             use_graph=0, verbose=0, allow_noconv=False, timing_warmup=0, triples_rank=0,
+             triples_nranks=1):
         cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
                        precision=precision, triples=triples, use_graph=use_graph,
-                       verbose=verbose, timing_warmup=timing_warmup)
+                       verbose=verbose, timing_warmup=timing_warmup, triples_rank=triples_rank,
+                       triples_nranks=triples_nranks)
         return self._run("xvcc_run", cfg, allow_noconv)
 
     def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0,

@@ -946,7 +946,12 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   }
   if (cfg->triples) {
     // (T) on the converged amplitudes (vcc/vcc.F:1215 -> trp/trps.F)
-    ACES_TRY(E.triples(&cfg->e_t4, &cfg->e_st5, &cfg->seconds_triples));
+    const int nr = cfg->triples_nranks > 0 ? cfg->triples_nranks : 1;
+    if (cfg->triples_rank < 0 || cfg->triples_rank >= nr) {
+      set_error("xvcc_run: triples_rank %d outside 0..%d", cfg->triples_rank, nr - 1);
+      return ACES_ERR_ARG;
+    }
+    ACES_TRY(E.triples(&cfg->e_t4, &cfg->e_st5, &cfg->seconds_triples, cfg->triples_rank, nr));
     aces_putrec("E4T", 8, &cfg->e_t4);
     aces_putrec("E5ST", 8, &cfg->e_st5);
   }

@@ -100,7 +100,8 @@ class CCEngine {
                 bool *extrap, bool lambda = false);
   int write_back();
   int write_amplitudes(const double *a1, const double *a2, int list1, int list2ab, int list2aa);
-  int triples(double *e4, double *e5, double *seconds);   // (T), trp/trps2.F
+  // (T), trp/trps2.F: the triplets t with t % nranks == rank (partial sums)
+  int triples(double *e4, double *e5, double *seconds, int rank = 0, int nranks = 1);
   void release();
 
   // contraction dispatch (FP64 DMMA or BF16x3 tcgen05)

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(1024) k_sum_pairs(double *out, const double *p
 // with Gv[z][(b,c),d] = (bd|cz), GvT[z][(c,b),d] = Gv[z][(b,c),d],
 // t2P[x][(a,b),l] = t2[x,l,a,b], t2Q[x][(b,a),l] = t2[x,l,a,b] and
 // H[y,z][c,l] = (cz|yl).
-int CCEngine::triples(double *e4, double *e5, double *seconds) {
+int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nranks) {
   const long long O = o, V = v;
   const long long V2 = V * V, V3 = V * V * V;
   cudaEvent_t t0, t1e;
@@ -224,11 +224,18 @@ int CCEngine::triples(double *e4, double *e5, double *seconds) {
   ACES_TRY(alloc(Hn, O * O * O * V));
   ACES_TRY(perm(Hn.p, o, o, v, o, 0.0, {PermTerm{I_ooov.p, -1.0, {s3[2], s3[1], s3[3], s3[0]}}}));
   ACES_TRY(alloc(Wb, V3));
-  // triplets i >= j >= k
+  // triplets i >= j >= k of this shard: index t (i, then j <= i, then k <= j)
+  // with t % nranks == rank
   std::vector<int> trip;
+  long long tix = 0;
   for (int i = 0; i < o; ++i)
     for (int j = 0; j <= i; ++j)
-      for (int k = 0; k <= j; ++k) { trip.push_back(i); trip.push_back(j); trip.push_back(k); }
+      for (int k = 0; k <= j; ++k, ++tix)
+        if (tix % nranks == rank) {
+          trip.push_back(i);
+          trip.push_back(j);
+          trip.push_back(k);
+        }
   const int ntrip = (int)trip.size() / 3;
   const int nblk = 148 * 4;
   ACES_TRY(alloc(part, (size_t)ntrip * nblk * 2));

@@ -284,7 +284,7 @@ def run_ours(a, rank, world, local_rank):
         line["fp64_gpu"] = fp64
     if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
         del lists  # release the pinned host lists before the next workload's
-        line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank)
+        line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank, rank, world)
     if prec == ab.PREC_BF16X3 and not a.no_lambda and a.workload == W_NAME:
         line["lambda"] = lambda_block(lib, "c4conv", local_rank)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -301,9 +301,12 @@ LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of th
                          "capture, scaled by (M*K) c2 / ladder-small")
 
 
-def accuracy(lib, wname, device):
+def accuracy(lib, wname, device, rank=0, world=1):
     """Split BF16x3 vs FP64 GPU on the convergent variant of the workload, both
-    converged to max|dT| < 1e-9 (CC_CONV=9): |dE| of the correlation energy."""
+    converged to max|dT| < 1e-9 (CC_CONV=9): |dE| of the correlation energy.
+    With several ranks the (T) triplets are split over them (each rank solves
+    the same CCSD) and the partial energies are all-reduced."""
+    from acesb200.parallel import sharded_triples
     import torch
     import acesb200 as ab
     from acesb200.workloads import WORKLOADS
@@ -317,14 +320,15 @@ def accuracy(lib, wname, device):
     put_lists(lib, eps, lists[1])
     res = {}
     for prec, name in ((ab.PREC_FP64, "fp64"), (ab.PREC_BF16X3, "bf16x3")):
-        c = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, precision=prec, allow_noconv=True,
-                     triples=1)
+        c = sharded_triples(lib, rank, world, cc_conv=9, cc_maxcyc=80, cc_exporder=5,
+                            precision=prec, allow_noconv=True)
         res[name] = {"e_corr": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
                      "seconds_per_iter": c.seconds_per_iter, "e_t4": c.e_t4, "e_st5": c.e_st5,
                      "seconds_triples": c.seconds_triples}
     lib.fin()
     return {"workload": f"{wname}: nocc={o}, nvir={v}, naux={wl['naux']}, seed={wl['seed']}, "
                         f"B scaled by {wl['bscale']} (convergent variant)",
+            "triples_ranks": world,
             "fp64": res["fp64"], "bf16x3": res["bf16x3"],
             "abs_dE": abs(res["bf16x3"]["e_corr"] - res["fp64"]["e_corr"]),
             "abs_dE_T": abs(res["bf16x3"]["e_t4"] + res["bf16x3"]["e_st5"]
@@ -474,11 +478,8 @@ def barrier(world):
 def max_over_ranks(x, world):
     if world == 1:
         return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from acesb200.parallel import allreduce_max
+    return allreduce_max(x)
 
 
 KERNEL_CASES = {
@@ -569,7 +570,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     try:
         line = run_ours(a, rank, world, local_rank)
         if rank == 0:

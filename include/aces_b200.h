@@ -175,6 +175,12 @@ typedef struct aces_cc_config {
   double flops_per_iter;     /* flops of all contractions of one cycle       */
   long long launches_per_iter; /* kernels launched in one timed cycle        */
   double seconds_setup;      /* device time reading lists and resorting integrals */
+  /* (T) over several GPUs (inputs): this call evaluates the occupied triplets
+   * i >= j >= k whose index t in the order (i, then j <= i, then k <= j)
+   * satisfies t % triples_nranks == triples_rank, and e_t4 / e_st5 are that
+   * shard's partial sums (add them over the ranks).  0 / 0 or 0 / 1: all. */
+  int triples_rank;
+  int triples_nranks;
 } aces_cc_config;
 
 /* PROGRAM VCC (vcc/vcc.F:9): RHF CCSD (and (T) when cfg->triples).  Reads

@@ -27,32 +27,64 @@ def _connected(t2, g_vvvo, g_ooov, i, j, k):
     return x
 
 
+class _Terms:
+    """The integral blocks and denominators of one (T) evaluation."""
+
+    def __init__(self, ham, t1, t2, eo=None, ev=None):
+        o, v = t1.shape
+        self.t1, self.t2 = t1, t2
+        self.g_vvvo = ham.chem("vvvo")   # (bd|ck) as [b,d,c,k]
+        self.g_ooov = ham.chem("ooov")   # (lj|kc) = (ck|jl) as [l,j,k,c]
+        self.g_ovov = ham.chem("ovov")   # (ia|jb) as [i,a,j,b]
+        if eo is None:
+            eps = ham.eps
+            eo, ev = eps[:o], eps[o:]
+        self.eo = eo
+        self.Dabc = ev[:, None, None] + ev[None, :, None] + ev[None, None, :]
+
+    def ordered(self, i, j, k):
+        """3 x the contribution of the ordered triplet (i, j, k) to (E[4]T, E[5]ST)."""
+        t1, t2, gv, go, gd = self.t1, self.t2, self.g_vvvo, self.g_ooov, self.g_ovov
+        W = (_connected(t2, gv, go, i, j, k)
+             + _connected(t2, gv, go, i, k, j).transpose(0, 2, 1)
+             + _connected(t2, gv, go, j, i, k).transpose(1, 0, 2)
+             + _connected(t2, gv, go, j, k, i).transpose(2, 0, 1)
+             + _connected(t2, gv, go, k, i, j).transpose(1, 2, 0)
+             + _connected(t2, gv, go, k, j, i).transpose(2, 1, 0))
+        Vd = (np.einsum("a,bc->abc", t1[i], gd[j, :, k, :])
+              + np.einsum("b,ac->abc", t1[j], gd[i, :, k, :])
+              + np.einsum("c,ab->abc", t1[k], gd[i, :, j, :]))
+        D = self.eo[i] + self.eo[j] + self.eo[k] - self.Dabc
+        Z = (4.0 * W + W.transpose(2, 0, 1) + W.transpose(1, 2, 0)) / D
+        return np.sum(Z * (W - W.transpose(2, 1, 0))), np.sum(Z * (Vd - Vd.transpose(2, 1, 0)))
+
+
 def triples(ham, t1, t2, eo=None, ev=None, return_parts=False):
     """Returns (E[4]T, E[5]ST) for converged closed-shell CCSD amplitudes."""
-    o, v = t1.shape
-    g_vvvo = ham.chem("vvvo")   # (bd|ck) as [b,d,c,k]
-    g_ooov = ham.chem("ooov")   # (lj|kc) = (ck|jl) as [l,j,k,c]
-    g_ovov = ham.chem("ovov")   # (ia|jb) as [i,a,j,b]
-    if eo is None:
-        eps = ham.eps
-        eo, ev = eps[:o], eps[o:]
-    Dabc = ev[:, None, None] + ev[None, :, None] + ev[None, None, :]
+    o = t1.shape[0]
+    T = _Terms(ham, t1, t2, eo, ev)
     e4 = 0.0
     e5 = 0.0
     for i in range(o):
         for j in range(o):
             for k in range(o):
-                W = (_connected(t2, g_vvvo, g_ooov, i, j, k)
-                     + _connected(t2, g_vvvo, g_ooov, i, k, j).transpose(0, 2, 1)
-                     + _connected(t2, g_vvvo, g_ooov, j, i, k).transpose(1, 0, 2)
-                     + _connected(t2, g_vvvo, g_ooov, j, k, i).transpose(2, 0, 1)
-                     + _connected(t2, g_vvvo, g_ooov, k, i, j).transpose(1, 2, 0)
-                     + _connected(t2, g_vvvo, g_ooov, k, j, i).transpose(2, 1, 0))
-                Vd = (np.einsum("a,bc->abc", t1[i], g_ovov[j, :, k, :])
-                      + np.einsum("b,ac->abc", t1[j], g_ovov[i, :, k, :])
-                      + np.einsum("c,ab->abc", t1[k], g_ovov[i, :, j, :]))
-                D = eo[i] + eo[j] + eo[k] - Dabc
-                Z = (4.0 * W + W.transpose(2, 0, 1) + W.transpose(1, 2, 0)) / D
-                e4 += np.sum(Z * (W - W.transpose(2, 1, 0)))
-                e5 += np.sum(Z * (Vd - Vd.transpose(2, 1, 0)))
+                a4, a5 = T.ordered(i, j, k)
+                e4 += a4
+                e5 += a5
+    return e4 / 3.0, e5 / 3.0
+
+
+def triples_unique(ham, t1, t2, triplets, eo=None, ev=None):
+    """(E[4]T, E[5]ST) restricted to the given triplets i >= j >= k, each
+    standing for its distinct orderings (the unit the engine distributes over
+    GPUs): summed over all triplets this equals `triples`."""
+    import itertools
+    T = _Terms(ham, t1, t2, eo, ev)
+    e4 = 0.0
+    e5 = 0.0
+    for (i, j, k) in triplets:
+        for p in set(itertools.permutations((i, j, k))):
+            a4, a5 = T.ordered(*p)
+            e4 += a4
+            e5 += a5
     return e4 / 3.0, e5 / 3.0

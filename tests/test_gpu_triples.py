@@ -52,3 +52,36 @@ def test_triples_split_matches_fp64(lib):
     assert abs(split.e_ccsd - exact.e_ccsd) < 1e-7
     assert abs(split.e_t4 - exact.e_t4) < 1e-8 + 1e-6 * abs(exact.e_t4)
     assert abs(split.e_st5 - exact.e_st5) < 1e-9 + 1e-6 * abs(exact.e_st5)
+
+
+@pytest.mark.parametrize("prec", [ab.PREC_FP64, ab.PREC_BF16X3])
+def test_triplet_shards_add_up_to_the_full_triples(lib, prec):
+    """The per-GPU (T) shards (triples_rank / triples_nranks), evaluated here one
+    after another on one GPU, sum to the unsharded energies; their union is
+    checked against the oracle's unique-triplet sum of the same shards."""
+    from acesb200.parallel import triplet_shard
+    from oracle.triples import triples_unique
+    ham = synthetic(5, 130, 48, seed=21, bscale=0.5)
+    setup_lists(lib, ham)
+    full = lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=prec)
+    for nranks in (2, 3):
+        e4 = e5 = 0.0
+        for r in range(nranks):
+            c = lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=prec, triples_rank=r,
+                         triples_nranks=nranks)
+            e4 += c.e_t4
+            e5 += c.e_st5
+        assert abs(e4 - full.e_t4) < 1e-13 + 1e-11 * abs(full.e_t4)
+        assert abs(e5 - full.e_st5) < 1e-14 + 1e-11 * abs(full.e_st5)
+    if prec == ab.PREC_FP64:
+        small = synthetic(4, 12, 20, seed=22)
+        setup_lists(lib, small)
+        ref = ccsd.run_ccsd(small, cc_conv=10, maxcyc=80, exporder=5)
+        s4, s5 = triples_unique(small, ref["t1"], ref["t2"], triplet_shard(4, 1, 3))
+        c = lib.xvcc(cc_conv=10, cc_maxcyc=80, triples=1, precision=prec, triples_rank=1,
+                     triples_nranks=3)
+        assert abs(c.e_t4 - s4) < 1e-12 + 1e-9 * abs(s4)
+        assert abs(c.e_st5 - s5) < 1e-13 + 1e-9 * abs(s5)
+    with pytest.raises(ab.AcesError):
+        lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=prec, triples_rank=3,
+                 triples_nranks=3)
