@@ -17,6 +17,13 @@ void set_error(const char *fmt, ...);
 // destroys the CC engine (amplitudes, intermediates, split caches) of this process
 void engine_reset();
 
+// caching device allocator (pool.cu): dev_free keeps the block for reuse by a
+// later dev_alloc of the same size class on the same device; pool_trim
+// returns every cached block to the driver
+cudaError_t dev_alloc(void **ptr, size_t bytes);
+void dev_free(void *ptr);
+void pool_trim();
+
 // number of kernels the library has launched (reported by the benchmarks)
 extern std::atomic<long long> g_launches;
 inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }

@@ -30,28 +30,28 @@ std::vector<DBuf *> CCEngine::registry() {
 }
 
 void CCEngine::release() {
-  for (auto &kv : adjoint) if (kv.second.p) cudaFree(kv.second.p);
+  for (auto &kv : adjoint) if (kv.second.p) dev_free(kv.second.p);
   adjoint.clear();
-  for (auto &kv : tcache) if (kv.second.p) cudaFree(kv.second.p);
+  for (auto &kv : tcache) if (kv.second.p) dev_free(kv.second.p);
   tcache.clear();
   tape.clear();
   active.clear();
   for (DBuf *b : registry()) {
-    if (b->p && !b->borrowed) cudaFree(b->p);
+    if (b->p && !b->borrowed) dev_free(b->p);
     b->p = nullptr;
     b->n = 0;
     b->borrowed = false;
   }
-  for (auto &b : hx) if (b.p) cudaFree(b.p);
-  for (auto &b : he) if (b.p) cudaFree(b.p);
+  for (auto &b : hx) if (b.p) dev_free(b.p);
+  for (auto &b : he) if (b.p) dev_free(b.p);
   hx.clear();
   he.clear();
   for (auto &e : split_cache) {
-    if (e.op.hi) cudaFree(e.op.hi);
+    if (e.op.hi) dev_free(e.op.hi);
   }
   split_cache.clear();
-  if (split_tmpA.hi) cudaFree(split_tmpA.hi);
-  if (split_tmpB.hi) cudaFree(split_tmpB.hi);
+  if (split_tmpA.hi) dev_free(split_tmpA.hi);
+  if (split_tmpB.hi) dev_free(split_tmpB.hi);
   split_tmpA = SplitOperand();
   split_tmpB = SplitOperand();
   if (ev_lad0) cudaEventDestroy(ev_lad0);
@@ -67,13 +67,13 @@ int CCEngine::alloc(DBuf &b, size_t n) {
     set_error("engine: a borrowed list buffer cannot be reallocated");
     return ACES_ERR_ARG;
   }
-  if (b.p) cudaFree(b.p);
+  if (b.p) dev_free(b.p);
   b.p = nullptr;
   b.n = 0;
   size_t bytes = (n ? n : 1) * sizeof(double);
-  if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+  if (dev_alloc((void **)&b.p, bytes) != cudaSuccess) {
     cudaGetLastError();
-    set_error("engine: cudaMalloc of %zu bytes failed", bytes);
+    set_error("engine: device allocation of %zu bytes failed", bytes);
     return ACES_ERR_NOMEM;
   }
   b.n = n;
@@ -247,15 +247,15 @@ struct DevMap {
   int *d_nrows = nullptr;
   DpdMap m;
   ~DevMap() {
-    cudaFree(d_rowidx); cudaFree(d_colidx); cudaFree(d_rowsgn); cudaFree(d_colsgn);
-    for (int k = 0; k < 4; ++k) cudaFree(d_irr[k]);
-    cudaFree(d_base); cudaFree(d_nrows);
+    dev_free(d_rowidx); dev_free(d_colidx); dev_free(d_rowsgn); dev_free(d_colsgn);
+    for (int k = 0; k < 4; ++k) dev_free(d_irr[k]);
+    dev_free(d_base); dev_free(d_nrows);
   }
 };
 
 template <class T>
 int upload(T **d, const std::vector<T> &h) {
-  ACES_CUDA(cudaMalloc(d, std::max<size_t>(1, h.size()) * sizeof(T)));
+  ACES_CUDA(dev_alloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T)));
   if (!h.empty()) ACES_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
   return ACES_OK;
 }
@@ -545,7 +545,7 @@ int CCEngine::setup_intermediates() {
   ACES_TRY(alloc(Bmat, 25 * 25));
   ACES_CUDA(cudaStreamSynchronize(st));
   // tmp4 is no longer needed
-  if (tmp4.p) { cudaFree(tmp4.p); tmp4.p = nullptr; tmp4.n = 0; }
+  if (tmp4.p) { dev_free(tmp4.p); tmp4.p = nullptr; tmp4.n = 0; }
   return ACES_OK;
 }
 
@@ -838,7 +838,7 @@ int CCEngine::write_amplitudes(const double *a1, const double *a2, int list1, in
           col[pair_index(s, 9, irr_v[a], lv[a], irr_o[i], lo[i])] = h1[(size_t)i * v + a];
     ACES_TRY(aces_putlst(col.data(), 1, 1, 1, list1));
   }
-  cudaFree(tmpb.p);
+  dev_free(tmpb.p);
   return ACES_OK;
 }
 

@@ -403,10 +403,10 @@ double *splitk_workspace(size_t doubles) {
   static double *ws = nullptr;
   static size_t cap = 0;
   if (doubles > cap) {
-    if (ws) cudaFree(ws);
+    if (ws) dev_free(ws);
     ws = nullptr;
     cap = 0;
-    if (cudaMalloc(&ws, doubles * sizeof(double)) != cudaSuccess) {
+    if (dev_alloc((void **)&ws, doubles * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }

@@ -63,13 +63,13 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
   int kp = (k + kSplitKPad - 1) / kSplitKPad * kSplitKPad;
   size_t need = (size_t)rp * kp * 2 * 2;
   if (!op.hi || op.cap < need) {
-    if (op.hi) cudaFree(op.hi);
+    if (op.hi) dev_free(op.hi);
     op.hi = op.lo = nullptr;
     op.cap = 0;
     void *p = nullptr;
-    if (cudaMalloc(&p, need) != cudaSuccess) {
+    if (dev_alloc((void **)&p, need) != cudaSuccess) {
       cudaGetLastError();
-      set_error("split_pack: cudaMalloc %zu failed", need);
+      set_error("split_pack: device allocation of %zu bytes failed", need);
       return ACES_ERR_NOMEM;
     }
     op.hi = p;

@@ -143,8 +143,8 @@ extern "C" int xlambda_run(aces_cc_config *cfg) {
   // initial multipliers: lambda = (dE/dT) / D
   launch_newt(E.L.p + ov, E.gE.p + ov, E.L.p, E.gE.p, E.eo.p, E.ev.p, E.o, E.v, E.st);
   ACES_CUDA(cudaGetLastError());
-  for (auto &b : E.hx) if (b.p) cudaFree(b.p);
-  for (auto &b : E.he) if (b.p) cudaFree(b.p);
+  for (auto &b : E.hx) if (b.p) dev_free(b.p);
+  for (auto &b : E.he) if (b.p) dev_free(b.p);
   E.hx.clear();
   E.he.clear();
   E.Bh.assign(625, 0.0);

@@ -36,7 +36,7 @@ void *DeviceArena::alloc(size_t bytes) {
     }
   size_t sz = bytes > chunk_bytes ? bytes : chunk_bytes;
   void *p = nullptr;
-  if (cudaMalloc(&p, sz) != cudaSuccess) {
+  if (dev_alloc((void **)&p, sz) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
@@ -45,7 +45,7 @@ void *DeviceArena::alloc(size_t bytes) {
 }
 
 void DeviceArena::release() {
-  for (auto &c : chunks) cudaFree(c.base);
+  for (auto &c : chunks) dev_free(c.base);
   chunks.clear();
 }
 
@@ -151,6 +151,7 @@ int aces_fin(void) {
   if (st.device >= 0) cudaDeviceSynchronize();
   engine_reset();
   st.arena.release();
+  pool_trim();  // cached device blocks go back to the driver
   st.lists.clear();
   st.isytyp.clear();
   st.records.clear();

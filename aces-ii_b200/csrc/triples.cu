@@ -252,7 +252,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
     // the FP64 copies are not read again
     for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q}) {
       ACES_CUDA(cudaStreamSynchronize(st));
-      cudaFree(b->p);
+      dev_free(b->p);
       b->p = nullptr;
     }
   }
@@ -339,11 +339,11 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   cudaEventDestroy(t0);
   cudaEventDestroy(t1e);
   for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp}) {
-    if (b->p) cudaFree(b->p);
+    if (b->p) dev_free(b->p);
     b->p = nullptr;
   }
   for (SplitOperand *sp : {&sT2, &sGv, &sGvT, &sHn, &sT2P, &sT2Q})
-    if (sp->hi) cudaFree(sp->hi);
+    if (sp->hi) dev_free(sp->hi);
   if (!std::isfinite(*e4) || !std::isfinite(*e5)) {
     set_error("(T): non-finite energy");
     return ACES_ERR_NAN;

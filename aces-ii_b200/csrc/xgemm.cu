@@ -12,7 +12,7 @@ namespace {
 // dst[r*cols + c] = src[r + c*ld]: column-major (rows x cols) -> row-major
 int to_kmajor(double **dst, const double *src, int rows, int cols, long long ld,
               cudaStream_t st) {
-  ACES_CUDA(cudaMalloc(dst, (size_t)rows * cols * 8 + 8));
+  ACES_CUDA(dev_alloc((void **)dst, (size_t)rows * cols * 8 + 8));
   PermSpec s;
   s.n[0] = 1; s.n[1] = 1; s.n[2] = rows; s.n[3] = cols;
   s.nterms = 1;
@@ -61,15 +61,15 @@ extern "C" int aces_xgemm(char transa, char transb, int m, int n, int k, double 
       if (status == ACES_OK) status = split_pack(sb, Bk, ldbk, n, k, st);
       if (status == ACES_OK) status = gemm_nt_bf16x3(sa, sb, m, n, alpha, beta, C, st);
       cudaStreamSynchronize(st);
-      if (sa.hi) cudaFree(sa.hi);
-      if (sb.hi) cudaFree(sb.hi);
+      if (sa.hi) dev_free(sa.hi);
+      if (sb.hi) dev_free(sb.hi);
     } else {
       status = gemm_nt_f64(m, n, k, alpha, Ak, ldak, Bk, ldbk, beta, C, st);
     }
   }
   cudaError_t e = cudaStreamSynchronize(st);
-  if (tA) cudaFree(tA);
-  if (tB) cudaFree(tB);
+  if (tA) dev_free(tA);
+  if (tB) dev_free(tB);
   if (status == ACES_OK && e != cudaSuccess) {
     set_error("aces_xgemm: %s", cudaGetErrorString(e));
     status = ACES_ERR_CUDA;

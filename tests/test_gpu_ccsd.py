@@ -161,3 +161,21 @@ def test_ccsd_errors_are_status_codes(lib):
     with pytest.raises(ab.AcesError) as e:
         lib.xvcc()
     assert e.value.status in (-2, -6)   # missing lists / SCFEVALA record
+
+
+def test_device_built_irrep_blocked_lists_match_oracle(lib):
+    """bench.put_lists_dpd (the 64-system batch's list builder: dense integrals
+    on the GPU, irrep blocks gathered there in the DPD pair order) gives the
+    same CCSD as the oracle on the same 8-irrep DF system."""
+    import torch
+    import bench
+    from acesb200.workloads import synthetic_df
+    o, v, naux, seed = 5, 31, 72, 1000
+    eps, B, irr = synthetic_df(o, v, naux, seed, irreps=8, bscale=0.25)
+    lib.init(0)
+    bench.put_lists_dpd(lib, eps, B, irr, o, v, torch.device("cuda", 0))
+    assert lib.nirrep == 8
+    cfg = lib.xvcc(cc_conv=10, cc_maxcyc=80, cc_exporder=5)
+    ref = ccsd.run_ccsd(synthetic(o, v, naux, seed, irreps=8, bscale=0.25), cc_conv=10, maxcyc=80,
+                        exporder=5)
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-10
