@@ -26,7 +26,7 @@ std::vector<DBuf *> CCEngine::registry() {
           &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
           &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
           &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec, &L, &Ln, &gE,
-          &lrhs, &bwdA, &bwdB, &bwdC, &bwdD};
+          &lrhs, &bwdA, &bwdB, &bwdC, &bwdD, &Up, &Um, &taup, &taum, &Sld, &Ald, &ladpairs};
 }
 
 void CCEngine::release() {
@@ -639,8 +639,13 @@ int CCEngine::residual() {
     ACES_CUDA(cudaEventCreate(&ev_lad1));
   }
   ACES_CUDA(cudaEventRecord(ev_lad0, st));
-  ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0, cview_colmajor(Z2.p, VV),
-             true));
+  if (recording) {
+    // the recorded (Lambda) pass keeps the dense form, whose adjoint the tape knows
+    ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0,
+               cview_colmajor(Z2.p, VV), true));
+  } else {
+    ACES_TRY(ladder_packed());
+  }
   ACES_CUDA(cudaEventRecord(ev_lad1, st));
 
   // ---- W(mbej) ABAB and ABBA (DWMBEJ, T1RING), layout W[j,b,m,e] ----
@@ -701,6 +706,52 @@ int CCEngine::residual() {
   ACES_TRY(perm(Z2.p, o, o, v, v, 1.0,
                 {PT(XP.p, 1.0, st2[0], st2[1], st2[2], st2[3]),
                  PT(XP.p, 1.0, st2[1], st2[0], st2[3], st2[2])}));
+  return ACES_OK;
+}
+
+// Particle-particle ladder Z2[ij,ab] += sum_cd <ab|cd> tau[ij,cd] on symmetric
+// and antisymmetric pair combinations (the reference's RHF a<=b packing,
+// vcc/ladab1.F:55-64 with SYMEXP4).  With <ba|dc> = <ab|cd>:
+//   S[ij,a<=b] = sum_{c<=d} U+[ab,cd] tau+[ij,cd],  U+ = (<ab|cd> + <ab|dc>)/2 (c<d), <ab|cc>
+//   A[ij,a<b]  = sum_{c<d}  U-[ab,cd] tau-[ij,cd],  U- = (<ab|cd> - <ab|dc>)/2
+//   tau+ = tau[cd] + tau[dc] (c<d), tau[cc];  tau- = tau[cd] - tau[dc]
+//   Z2[ab] += S + A,  Z2[ba] += S - A,  Z2[aa] += S
+// Two contractions of (v(v+1)/2)^2 and (v(v-1)/2)^2 x o^2 instead of v^4 x o^2:
+// half the flops.  U+/U- are built once from the dense <ab|cd> (or the list).
+int CCEngine::ladder_packed() {
+  const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2, oo = o * o;
+  if (!Up.p) {
+    // pair tables: p(c,d) = d(d+1)/2 + c (c <= d), m(c,d) = d(d-1)/2 + c (c < d)
+    std::vector<int> pr((size_t)2 * (np + nm));
+    for (int d = 0; d < v; ++d)
+      for (int c = 0; c <= d; ++c) {
+        const int p = d * (d + 1) / 2 + c;
+        pr[2 * p] = c;
+        pr[2 * p + 1] = d;
+        if (c < d) {
+          const int m = d * (d - 1) / 2 + c;
+          pr[2 * (np + m)] = c;
+          pr[2 * (np + m) + 1] = d;
+        }
+      }
+    ACES_TRY(alloc(ladpairs, (pr.size() + 1) / 2));
+    ACES_CUDA(cudaMemcpyAsync(ladpairs.p, pr.data(), pr.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, st));
+    ACES_TRY(alloc(Up, (size_t)np * np));
+    ACES_TRY(alloc(Um, (size_t)std::max(nm, 1) * std::max(nm, 1)));
+    launch_ladder_pack_v(Up.p, Um.p, I_vvvv.p, (const int *)ladpairs.p, v, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  ACES_TRY(alloc(taup, (size_t)oo * np));
+  ACES_TRY(alloc(taum, (size_t)oo * std::max(nm, 1)));
+  ACES_TRY(alloc(Sld, (size_t)oo * np));
+  ACES_TRY(alloc(Ald, (size_t)oo * std::max(nm, 1)));
+  launch_ladder_pack_tau(taup.p, taum.p, tau.p, (const int *)ladpairs.p, v, oo, st);
+  ACES_TRY(G(np, oo, np, 1.0, Up.p, np, taup.p, np, 0.0, cview_colmajor(Sld.p, np), true));
+  if (nm > 0)
+    ACES_TRY(G(nm, oo, nm, 1.0, Um.p, nm, taum.p, nm, 0.0, cview_colmajor(Ald.p, nm), true));
+  launch_ladder_unpack(Z2.p, Sld.p, Ald.p, v, oo, st);
+  ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
 

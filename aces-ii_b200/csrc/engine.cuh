@@ -48,6 +48,9 @@ class CCEngine {
   // temporaries
   DBuf tau, taut, tautP, tauT, U, Tp, Tpp, uT, wP, t2P, Y1, Y2, XnP, WA, WB, ZT, XP, Xmn, Wmnij,
       WmnT, t1T, Fae, Fmi, Fme, Fp, Fpp, FmiT, FppT, FmeT, tmp4;
+  // packed particle-particle ladder (symmetric / antisymmetric pair combinations)
+  DBuf Up, Um, taup, taum, Sld, Ald, ladpairs;
+  int ladder_packed();  // Z2 += <ab|cd> tau(ij,cd) at half the dense flops
   DBuf scratch, dev_small;  // reductions / DIIS scalars
   // DIIS history
   std::vector<DBuf> hx, he;

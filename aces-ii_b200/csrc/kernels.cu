@@ -598,4 +598,101 @@ void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st) {
   k_scatter<<<(unsigned)nb, 256, 0, st>>>(dense, m, total); count_launch();
 }
 
+// ---------------------------------------------------------------------------
+// Packed particle-particle ladder
+// ---------------------------------------------------------------------------
+// U+[p][q] = (V[ab,cd] + V[ab,dc]) / 2 (c < d), V[ab,cc];  U-[m][n] = (V[ab,cd] - V[ab,dc]) / 2
+// with (a,b) = pair p (or m), (c,d) = pair q (or n); one block row per output row
+__global__ void k_ladder_pack_v(double *__restrict__ Up, double *__restrict__ Um,
+                                const double *__restrict__ V, const int *__restrict__ pairs,
+                                int v) {
+  const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
+  const size_t vv = (size_t)v * v;
+  for (int r = blockIdx.x; r < np + nm; r += gridDim.x) {
+    const bool sym = r < np;
+    const int a = pairs[2 * r], b = pairs[2 * r + 1];
+    const double *row = V + ((size_t)a * v + b) * vv;
+    if (sym) {
+      double *out = Up + (size_t)r * np;
+      for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        const int c = pairs[2 * q], d = pairs[2 * q + 1];
+        out[q] = c == d ? row[(size_t)c * v + c]
+                        : 0.5 * (row[(size_t)c * v + d] + row[(size_t)d * v + c]);
+      }
+    } else {
+      double *out = Um + (size_t)(r - np) * nm;
+      for (int q = threadIdx.x; q < nm; q += blockDim.x) {
+        const int c = pairs[2 * (np + q)], d = pairs[2 * (np + q) + 1];
+        out[q] = 0.5 * (row[(size_t)c * v + d] - row[(size_t)d * v + c]);
+      }
+    }
+  }
+}
+
+void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pairs, int v,
+                          cudaStream_t st) {
+  const int rows = v * v;  // np + nm
+  k_ladder_pack_v<<<std::min(rows, 148 * 16), 256, 0, st>>>(Up, Um, V, pairs, v);
+  count_launch();
+}
+
+// tau+[ij][p(c,d)] = tau[ij][cd] + tau[ij][dc] (c < d), tau[ij][cc];
+// tau-[ij][m(c,d)] = tau[ij][cd] - tau[ij][dc]
+__global__ void k_ladder_pack_tau(double *__restrict__ tp, double *__restrict__ tm,
+                                  const double *__restrict__ tau, const int *__restrict__ pairs,
+                                  int v, int noo) {
+  const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
+  const size_t vv = (size_t)v * v;
+  for (int ij = blockIdx.y; ij < noo; ij += gridDim.y) {
+    const double *t = tau + (size_t)ij * vv;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np + nm; q += gridDim.x * blockDim.x) {
+      const int c = pairs[2 * q], d = pairs[2 * q + 1];
+      if (q < np)
+        tp[(size_t)ij * np + q] = c == d ? t[(size_t)c * v + c]
+                                         : t[(size_t)c * v + d] + t[(size_t)d * v + c];
+      else
+        tm[(size_t)ij * nm + (q - np)] = t[(size_t)c * v + d] - t[(size_t)d * v + c];
+    }
+  }
+}
+
+void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
+                            int noo, cudaStream_t st) {
+  const int n = v * v;
+  dim3 grid((unsigned)std::min((n + 255) / 256, 64), (unsigned)std::min(noo, 65535));
+  k_ladder_pack_tau<<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo);
+  count_launch();
+}
+
+// Z2[ij][a][b] += S[ij][p] + A[ij][m] (a < b), S - A (a > b), S[ij][p(a,a)] (a = b)
+__global__ void k_ladder_unpack(double *__restrict__ Z2, const double *__restrict__ S,
+                                const double *__restrict__ A, int v, int noo) {
+  const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
+  const size_t vv = (size_t)v * v;
+  for (int ij = blockIdx.y; ij < noo; ij += gridDim.y) {
+    double *z = Z2 + (size_t)ij * vv;
+    const double *s = S + (size_t)ij * np, *an = A + (size_t)ij * nm;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < v * v; e += gridDim.x * blockDim.x) {
+      const int a = e / v, b = e - a * v;
+      double x;
+      if (a == b) {
+        x = s[a * (a + 1) / 2 + a];
+      } else if (a < b) {
+        x = s[b * (b + 1) / 2 + a] + an[b * (b - 1) / 2 + a];
+      } else {
+        x = s[a * (a + 1) / 2 + b] - an[a * (a - 1) / 2 + b];
+      }
+      z[e] += x;
+    }
+  }
+}
+
+void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
+                          cudaStream_t st) {
+  const int n = v * v;
+  dim3 grid((unsigned)std::min((n + 255) / 256, 64), (unsigned)std::min(noo, 65535));
+  k_ladder_unpack<<<grid, 256, 0, st>>>(Z2, S, A, v, noo);
+  count_launch();
+}
+
 }  // namespace acesb200

@@ -72,4 +72,14 @@ struct DpdMap {
 void launch_gather(double *dense, const DpdMap &m, cudaStream_t st);
 void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st);
 
+// packed particle-particle ladder (engine.cu, ladder_packed): pairs[2p], pairs[2p+1]
+// = (c, d) of the symmetric pair p (np = v(v+1)/2 of them) followed by the
+// antisymmetric pairs (c < d)
+void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pairs, int v,
+                          cudaStream_t st);
+void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
+                            int noo, cudaStream_t st);
+void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
+                          cudaStream_t st);
+
 }  // namespace acesb200

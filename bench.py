@@ -342,11 +342,19 @@ def run_ours(a, rank, world, local_rank):
     lib.fin()
 
     pk, pk_src = peaks()
-    launch_flops = 2.0 * (o * o) * (v * v) * (v * v)
+    # the ladder runs packed (symmetric + antisymmetric pair blocks): its own
+    # contraction flops, and the reference's dense 2 o^2 v^4 for comparison
+    n_p, n_m = v * (v + 1) // 2, v * (v - 1) // 2
+    launch_flops = 2.0 * (o * o) * (n_p * n_p + n_m * n_m)
+    dense_flops = 2.0 * (o * o) * (v * v) * (v * v)
     if prec == ab.PREC_BF16X3:
         executed = 3.0 * launch_flops
         peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
-        roof = {"bound": "tensor", "kernel": "k_gemm_bf16x3 (particle-particle ladder)",
+        roof = {"bound": "tensor",
+                "kernel": "k_gemm_bf16x3 (particle-particle ladder, symmetric + antisymmetric "
+                          "pair blocks, with its pack/unpack kernels)",
+                "reference_dense_flops_per_launch": dense_flops,
+                "effective_dense_tflops": dense_flops / s_lad / 1e12,
                 "achieved": executed / s_lad / 1e12, "peak": peak, "unit": "TFLOP/s",
                 "frac": executed / s_lad / 1e12 / peak,
                 "peak_source": f"bf16_tflops_sustained of {pk_src} MEASURED_PEAKS.json",
@@ -354,8 +362,8 @@ def run_ours(a, rank, world, local_rank):
                 "executed_bf16_flops_per_launch": executed,
                 "seconds_per_launch": s_lad, "traffic": LADDER_TRAFFIC.get(a.workload),
                 "traffic_source": LADDER_TRAFFIC_SOURCE if a.workload in LADDER_TRAFFIC else None,
-                "algorithmic_bytes_per_launch": 4.0 * (v * v) * (v * v) + 4.0 * (o * o) * (v * v)
-                + 8.0 * (o * o) * (v * v)}
+                "algorithmic_bytes_per_launch": 4.0 * (n_p * n_p + n_m * n_m)
+                + 4.0 * (o * o) * (v * v) + 3 * 8.0 * (o * o) * (v * v)}
     else:
         roof = {"bound": "tensor", "kernel": "k_gemm_nt_f64 (particle-particle ladder)",
                 "achieved": launch_flops / s_lad / 1e12, "peak": None, "unit": "TFLOP/s",
@@ -397,13 +405,10 @@ def run_ours(a, rank, world, local_rank):
     return line
 
 
-# DRAM bytes (read + write) per ladder launch: the ncu capture of the
-# ladder-small case (919.4 MB read, 37.1 MB written at M = K = 14400, N = 400;
-# profiles/k_gemm_bf16x3_ladder_small.md) scaled by the A operand that
-# dominates it, (32400 / 14400)^2 for c2
-LADDER_TRAFFIC = {"c2": (919.4e6 + 37.1e6) * (32400.0 / 14400.0) ** 2}
-LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the ladder-small "
-                         "capture, scaled by (M*K) c2 / ladder-small")
+# DRAM bytes (read + write) of one packed ladder (its launches summed), from
+# the one-pass ncu launch list of the c2 bench (profiles/ccsd_cycle_c2_launches.md)
+LADDER_TRAFFIC = {}
+LADDER_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the ladder launches"
 
 
 def accuracy(lib, wname, device, rank=0, world=1):
