@@ -26,6 +26,14 @@ class CCEngine {
   int prec = ACES_PREC_FP64;
   cudaStream_t st = 0;
   bool nonhf = false;
+  // residual pass captured in a CUDA graph (use_graph): captured on the second
+  // cycle, when every buffer it touches exists, and replayed afterwards
+  bool use_graph = false;
+  cudaGraphExec_t residual_exec = nullptr;
+  long long residual_launches = 0;
+  double residual_flops = 0.0;
+  int residual_passes = 0;
+  int residual_run();
 
   // orbital data
   std::vector<double> eps_h;       // nmo, DPD order

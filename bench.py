@@ -48,6 +48,8 @@ def args():
     p.add_argument("--workload", default=W_NAME)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64-compare", action="store_true")
+    p.add_argument("--use-graph", type=int, default=0,
+                   help="1: replay each cycle's residual pass from a captured CUDA graph")
     p.add_argument("--batch-bscale", type=float, default=1.0,
                    help="scale of the DF factors of the 64-system batch (--workload c5)")
     p.add_argument("--no-lambda", action="store_true",
@@ -248,7 +250,7 @@ def run_batch(a):
         row = {"k": k, "nocc": o, "nvir": v}
         for prec, name in ((ab.PREC_BF16X3, "bf16x3"), (ab.PREC_FP64, "fp64")):
             c = lib.xvcc(cc_conv=7, cc_maxcyc=80, cc_exporder=5, precision=prec,
-                         allow_noconv=True)
+                         allow_noconv=True, use_graph=a.use_graph)
             t = c.seconds_setup + c.seconds_per_iter * c.ncycle
             tot[name] += t
             row[name] = {"e": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
@@ -262,7 +264,8 @@ def run_batch(a):
             "dtype": "bf16x3",
             "data": f"synthetic: acesb200.workloads.batch_systems, B x {a.batch_bscale}",
             "config": {"workload": "c5: 64 systems, nocc 4-24, nvir 30-220, 8 irreps, "
-                                   "seeds 1000-1063", "execution": "sequential xvcc_run calls"},
+                                   "seeds 1000-1063", "execution": "sequential xvcc_run calls",
+                       "use_graph": a.use_graph},
             "fp64_seconds": tot["fp64"], "speedup_split_vs_fp64": tot["fp64"] / tot["bf16x3"],
             "max_abs_dE": max(dE), "all_converged": all(r["bf16x3"]["converged"] and
                                                         r["fp64"]["converged"] for r in rows),
@@ -304,7 +307,7 @@ def run_ours(a, rank, world, local_rank):
     barrier(world)
     with Clocks(local_rank) as clk:
         cfg = lib.xvcc(cc_conv=30, cc_maxcyc=W + K, cc_exporder=5, precision=prec,
-                       timing_warmup=W, allow_noconv=True)
+                       timing_warmup=W, allow_noconv=True, use_graph=a.use_graph)
         torch.cuda.synchronize()
     barrier(world)
     s_iter = max_over_ranks(cfg.seconds_per_iter, world)
@@ -347,7 +350,11 @@ def run_ours(a, rank, world, local_rank):
     n_p, n_m = v * (v + 1) // 2, v * (v - 1) // 2
     launch_flops = 2.0 * (o * o) * (n_p * n_p + n_m * n_m)
     dense_flops = 2.0 * (o * o) * (v * v) * (v * v)
-    if prec == ab.PREC_BF16X3:
+    if s_lad <= 0.0:  # graph replay: the ladder is not timed separately
+        roof = {"bound": "tensor", "kernel": "k_gemm_bf16x3 (particle-particle ladder)",
+                "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
+                "traffic": None, "note": "not measured under --use-graph 1"}
+    elif prec == ab.PREC_BF16X3:
         executed = 3.0 * launch_flops
         peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
         roof = {"bound": "tensor",

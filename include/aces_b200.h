@@ -158,7 +158,9 @@ typedef struct aces_cc_config {
   int cc_exporder;    /* IFLAGS(12): DIIS subspace (<= 25)                   */
   int precision;      /* ACES_PREC_*                                         */
   int triples;        /* 1: run (T) after CCSD (CALC=CCSD(T))                */
-  int use_graph;      /* 1: capture one iteration in a CUDA graph             */
+  int use_graph;      /* 1: the residual pass of every cycle after the second
+                         is a replay of a CUDA graph captured on the second
+                         (seconds_ladder is then not measured)              */
   int verbose;        /* 1: per-iteration log on stdout (IFLAGS(1))          */
   int timing_warmup;  /* cycles excluded from the timing outputs             */
   /* outputs */

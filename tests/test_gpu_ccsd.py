@@ -179,3 +179,16 @@ def test_device_built_irrep_blocked_lists_match_oracle(lib):
     ref = ccsd.run_ccsd(synthetic(o, v, naux, seed, irreps=8, bscale=0.25), cc_conv=10, maxcyc=80,
                         exporder=5)
     assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-10
+
+
+@pytest.mark.parametrize("prec", [ab.PREC_FP64, ab.PREC_BF16X3])
+def test_residual_graph_replay_is_bitwise_identical(lib, prec):
+    """use_graph: the residual pass replayed from a captured CUDA graph runs the
+    same kernels in the same order, so every cycle's energy is identical."""
+    ham = synthetic(6, 130, 50, seed=17, bscale=0.5)
+    setup_lists(lib, ham)
+    plain = lib.xvcc(cc_conv=8, cc_maxcyc=40, cc_exporder=5, precision=prec)
+    graph = lib.xvcc(cc_conv=8, cc_maxcyc=40, cc_exporder=5, precision=prec, use_graph=1)
+    assert graph.ncycle == plain.ncycle and graph.converged == 1
+    assert graph.e_ccsd == plain.e_ccsd
+    assert graph.launches_per_iter == plain.launches_per_iter
