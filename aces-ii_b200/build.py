@@ -51,7 +51,8 @@ def build(verbose=False):
     objs = [o for o, _ in results]
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < newest:
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart",
+                                                               "-Xlinker", "--no-undefined"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -210,8 +210,9 @@ int CCEngine::backward() {
           // A_bar[m,k] += sum_n Cd[m,n] B[n,k]
           const double *Bt = transposed(op.B, op.N, op.K, op.ldb, !op.b_act, bwdB);
           if (!Bt) return ACES_ERR_NOMEM;
+          // a constant operand's transpose is cached, so its split is too
           ACES_TRY(G(op.M, op.K, op.N, 1.0, bwdC.p, op.N, Bt, op.N, 1.0,
-                     cview_rowmajor(adj(op.A), op.lda)));
+                     cview_rowmajor(adj(op.A), op.lda), false, !op.b_act));
         }
         if (op.b_act) {
           // B_bar[n,k] += sum_m Cd[m,n] A[m,k]
@@ -219,7 +220,7 @@ int CCEngine::backward() {
           const double *At = transposed(op.A, op.M, op.K, op.lda, !op.a_act, bwdA);
           if (!Cdt || !At) return ACES_ERR_NOMEM;
           ACES_TRY(G(op.N, op.K, op.M, 1.0, Cdt, op.M, At, op.M, 1.0,
-                     cview_rowmajor(adj(op.B), op.ldb)));
+                     cview_rowmajor(adj(op.B), op.ldb), false, !op.a_act));
         }
       }
       if (op.beta == 0.0)

@@ -52,6 +52,10 @@ void CCEngine::release() {
   split_cache.clear();
   if (split_tmpA.hi) dev_free(split_tmpA.hi);
   if (split_tmpB.hi) dev_free(split_tmpB.hi);
+  for (auto &t : split_tmpG) {
+    if (t.hi) dev_free(t.hi);
+    t = SplitOperand();
+  }
   split_tmpA = SplitOperand();
   split_tmpB = SplitOperand();
   if (residual_exec) cudaGraphExecDestroy(residual_exec);
@@ -183,26 +187,66 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
     std::swap(constA, constB);
     Cv = CView{C.p, C.ndiv, C.sn1, C.sn0, C.mdiv, C.sm1, C.sm0};
   }
-  auto get = [&](const double *src, long long ld, int rows, bool cst, SplitOperand &tmp,
-                 const SplitOperand **out) -> int {
-    if (cst) {
-      for (auto &e : split_cache)
-        if (e.src == src && e.op.rows == rows && e.op.k == K) { *out = &e.op; return ACES_OK; }
-      SplitEntry e;
-      e.src = src;
-      ACES_TRY(split_pack(e.op, src, ld, rows, K, st));
-      split_cache.push_back(e);
-      *out = &split_cache.back().op;
-      return ACES_OK;
-    }
-    ACES_TRY(split_pack(tmp, src, ld, rows, K, st));
-    *out = &tmp;
-    return ACES_OK;
-  };
   const SplitOperand *a = nullptr, *b = nullptr;
-  ACES_TRY(get(A, lda, M, constA, split_tmpA, &a));
-  ACES_TRY(get(B, ldb, N, constB, split_tmpB, &b));
+  ACES_TRY(split_get(A, lda, M, K, constA, split_tmpA, &a));
+  ACES_TRY(split_get(B, ldb, N, K, constB, split_tmpB, &b));
   return gemm_nt_bf16x3(*a, *b, M, N, alpha, beta, Cv, st);
+}
+
+int CCEngine::split_get(const double *src, long long ld, int rows, int K, bool cst,
+                        SplitOperand &tmp, const SplitOperand **out) {
+  if (cst) {
+    for (auto &e : split_cache)
+      if (e.src == src && e.op.rows == rows && e.op.k == K) {
+        *out = &e.op;
+        return ACES_OK;
+      }
+    split_cache.emplace_back();
+    SplitEntry &e = split_cache.back();
+    e.src = src;
+    ACES_TRY(split_pack(e.op, src, ld, rows, K, st));
+    *out = &e.op;
+    return ACES_OK;
+  }
+  ACES_TRY(split_pack(tmp, src, ld, rows, K, st));
+  *out = &tmp;
+  return ACES_OK;
+}
+
+int CCEngine::Ggroup(const GArgs *g, int n, double beta) {
+  bool grouped = prec == ACES_PREC_BF16X3 && !recording && n >= 2 && n <= 3;
+  for (int i = 0; i < n && grouped; ++i)
+    grouped = g[i].M >= 16 && g[i].N >= 16 && g[i].K >= 128 &&
+              (double)g[i].M * g[i].N * g[i].K >= 1.0e8;
+  if (!grouped) {
+    for (int i = 0; i < n; ++i)
+      ACES_TRY(G(g[i].M, g[i].N, g[i].K, 1.0, g[i].A, g[i].lda, g[i].B, g[i].ldb, beta, g[i].C,
+                 g[i].constA, g[i].constB));
+    return ACES_OK;
+  }
+  const SplitOperand *sa[3], *sb[3];
+  GroupedProblem pr[3];
+  for (int i = 0; i < n; ++i) {
+    GArgs q = g[i];
+    gemm_calls++;
+    gemm_flops += 2.0 * q.M * q.N * (double)q.K;
+    if (q.C.sm0 != 1 && q.C.sn0 == 1) {  // coalescing orientation, as in G
+      std::swap(q.M, q.N);
+      std::swap(q.A, q.B);
+      std::swap(q.lda, q.ldb);
+      std::swap(q.constA, q.constB);
+      q.C = CView{q.C.p, q.C.ndiv, q.C.sn1, q.C.sn0, q.C.mdiv, q.C.sm1, q.C.sm0};
+    }
+    ACES_TRY(split_get(q.A, q.lda, q.M, q.K, q.constA, split_tmpG[2 * i], &sa[i]));
+    ACES_TRY(split_get(q.B, q.ldb, q.N, q.K, q.constB, split_tmpG[2 * i + 1], &sb[i]));
+    pr[i].A = sa[i];
+    pr[i].B = sb[i];
+    pr[i].nseg = 1;
+    pr[i].M = q.M;
+    pr[i].N = q.N;
+    pr[i].C = q.C;
+  }
+  return gemm_nt_bf16x3_grouped(pr, n, 1.0, beta, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -749,9 +793,10 @@ int CCEngine::ladder_packed() {
   ACES_TRY(alloc(Sld, (size_t)oo * np));
   ACES_TRY(alloc(Ald, (size_t)oo * std::max(nm, 1)));
   launch_ladder_pack_tau(taup.p, taum.p, tau.p, (const int *)ladpairs.p, v, oo, st);
-  ACES_TRY(G(np, oo, np, 1.0, Up.p, np, taup.p, np, 0.0, cview_colmajor(Sld.p, np), true));
-  if (nm > 0)
-    ACES_TRY(G(nm, oo, nm, 1.0, Um.p, nm, taum.p, nm, 0.0, cview_colmajor(Ald.p, nm), true));
+  // both products in one grouped launch (their tiles fill each other's last wave)
+  const GArgs g[2] = {{np, oo, np, Up.p, np, taup.p, np, cview_colmajor(Sld.p, np), true, false},
+                      {nm, oo, nm, Um.p, nm, taum.p, nm, cview_colmajor(Ald.p, nm), true, false}};
+  ACES_TRY(Ggroup(g, nm > 0 ? 2 : 1, 0.0));
   launch_ladder_unpack(Z2.p, Sld.p, Ald.p, v, oo, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;

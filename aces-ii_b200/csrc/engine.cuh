@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <map>
 #include <vector>
 
@@ -68,8 +69,23 @@ class CCEngine {
 
   // split-precision operand cache (constant integrals)
   struct SplitEntry { const double *src; SplitOperand op; };
-  std::vector<SplitEntry> split_cache;
-  SplitOperand split_tmpA, split_tmpB;
+  std::deque<SplitEntry> split_cache;  // a deque: entries keep their address
+  SplitOperand split_tmpA, split_tmpB, split_tmpG[6];
+  // split operand of src (rows x K, leading dimension ld): cached when cst
+  int split_get(const double *src, long long ld, int rows, int K, bool cst, SplitOperand &tmp,
+                const SplitOperand **out);
+  // several contractions C_g = A_g B_g^T + beta C_g in one grouped tensor-core
+  // launch when all take the split path (else one G call each)
+  struct GArgs {
+    int M, N, K;
+    const double *A;
+    long long lda;
+    const double *B;
+    long long ldb;
+    CView C;
+    bool constA, constB;
+  };
+  int Ggroup(const GArgs *g, int n, double beta);
 
   // Lambda (adjoint) state: lambda = [l1 | l2] like X, dE/dT, tape
   DBuf L, Ln, gE, lrhs;

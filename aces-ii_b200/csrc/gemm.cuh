@@ -120,6 +120,18 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
 int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
                          double alpha, double beta, const CView &C, cudaStream_t st);
 
+// Up to 3 independent products in one persistent launch (no split K):
+// C_g = alpha sum_s A_g[s] B_g[s]^T + beta C_g.  The tiles of all problems are
+// scheduled together, so products whose own tile counts leave SMs idle in
+// their last wave fill each other's.
+struct GroupedProblem {
+  const SplitOperand *A, *B;  // nseg operands each
+  int nseg, M, N;
+  CView C;
+};
+int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha, double beta,
+                           cudaStream_t st);
+
 // Rows [row0, row0 + rows) of a split operand (no copy).  The view's tensor
 // map ends at the parent's padded rows; rows past the view inside it belong
 // to the next slice and only reach output rows that callers discard.

@@ -216,32 +216,49 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // k-tile sequence straight across tile boundaries (stage and TMEM-buffer
 // parities are global counters), so the loads and products of the next tile
 // overlap the epilogue of the current one.
-struct TileSched {
-  int tilesN, tilesM, ktc, kTilesTotal;
-  __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &ktb,
-                                         int &kTiles) const {
-    const int tn = t % tilesN, r = t / tilesN;
-    const int tm = r % tilesM;
-    z = r / tilesM;
-    m0 = tm * TBM;
-    n0 = tn * TBN;
-    ktb = z * ktc;
-    kTiles = max(0, min(ktc, kTilesTotal - ktb));
-  }
+// One launch computes up to kMaxProb independent products (a grouped launch
+// keeps every SM busy where one product has too few tiles for whole waves),
+// each C_g = alpha * sum_s A_gs B_gs^T + beta C_g over up to kMaxSeg K
+// segments with their own tensor maps.  Tiles are numbered problem by
+// problem; within a problem n tile fastest, then m tile, then split-K slice.
+constexpr int kMaxSeg = 4, kMaxProb = 3;
+struct Problem {
+  CView C;
+  int M, N, tilesM, tilesN;
+  int ktc, kTilesTotal;  // k tiles per split-K slice, in total
+  int tile0;             // first tile of this problem
+  int nseg, chunk;
+  int kt0[kMaxSeg + 1];  // segment s owns global k tiles [kt0[s], kt0[s+1])
 };
-
-// K segments: C = alpha * sum_s A_s B_s^T + beta C, segment s owning the
-// global k tiles [kt0[s], kt0[s+1]) with its own tensor maps
-constexpr int kMaxSeg = 4;
-struct SegMaps {
-  CUtensorMap ah[kMaxSeg], al[kMaxSeg], bh[kMaxSeg], bl[kMaxSeg];
-  int kt0[kMaxSeg + 1];
-  int nseg;
+struct Launch {
+  CUtensorMap ah[kMaxProb][kMaxSeg], al[kMaxProb][kMaxSeg];
+  CUtensorMap bh[kMaxProb][kMaxSeg], bl[kMaxProb][kMaxSeg];
+  Problem prob[kMaxProb];
+  int nprob, nTiles;
 };
+struct TileRef {
+  int g, m0, n0, z, ktb, kTiles;
+};
+__device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
+  TileRef r;
+  r.g = 0;
+  while (r.g + 1 < L.nprob && t >= L.prob[r.g + 1].tile0) ++r.g;
+  const Problem &P = L.prob[r.g];
+  const int tl = t - P.tile0;
+  const int tn = tl % P.tilesN, q = tl / P.tilesN;
+  const int tm = q % P.tilesM;
+  r.z = q / P.tilesM;
+  r.m0 = tm * TBM;
+  r.n0 = tn * TBN;
+  r.ktb = r.z * P.ktc;
+  r.kTiles = max(0, min(P.ktc, P.kTilesTotal - r.ktb));
+  return r;
+}
 
 __global__ void __launch_bounds__(kThreads, 1)
-    k_gemm_bf16x3(const __grid_constant__ SegMaps maps, int M, int N, TileSched sch, int nTiles,
-                  int chunk, double alpha, double beta, CView C, double *__restrict__ part) {
+    k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
+                  double *__restrict__ part) {
+  const int nTiles = L.nTiles;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -284,8 +301,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     int it = 0;  // k tiles issued by this CTA
     bool stop = false;
     for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
-      int m0, n0, z, ktb, kTiles;
-      sch.decode(t, m0, n0, z, ktb, kTiles);
+      const TileRef T = decode_tile(L, t);
+      const Problem &P = L.prob[T.g];
+      const int m0 = T.m0, n0 = T.n0, ktb = T.ktb, kTiles = T.kTiles;
       for (int kt = 0; kt < kTiles; ++kt) {
         const int s = it % STAGES;
         if (it >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((it / STAGES) - 1) & 1)) {
@@ -301,14 +319,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t fb = smem_u32(&full[s]);
         unsigned char *st = smem + s * STAGE_BYTES;
         mbar_expect_tx(fb, STAGE_BYTES);
-        const int g = ktb + kt;  // global k tile -> segment and its local k offset
+        const int gk = ktb + kt;  // global k tile -> segment and its local k offset
         int sg = 0;
-        while (sg + 1 < maps.nseg && g >= maps.kt0[sg + 1]) ++sg;
-        const int kx = (g - maps.kt0[sg]) * TBK;
-        tma_load_2d(smem_u32(st), &maps.ah[sg], kx, m0, fb);
-        tma_load_2d(smem_u32(st + TILE_A), &maps.al[sg], kx, m0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A), &maps.bh[sg], kx, n0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &maps.bl[sg], kx, n0, fb);
+        while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
+        const int kx = (gk - P.kt0[sg]) * TBK;
+        tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, m0, fb);
+        tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, m0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, n0, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &L.bl[T.g][sg], kx, n0, fb);
         ++it;
       }
     }
@@ -321,8 +339,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     int it = 0, gc = 0;  // k tiles consumed, accumulation chunks started
     bool stop = false;
     for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
-      int m0, n0, z, ktb, kTiles;
-      sch.decode(t, m0, n0, z, ktb, kTiles);
+      const TileRef T = decode_tile(L, t);
+      const int kTiles = T.kTiles, chunk = L.prob[T.g].chunk;
       for (int kt = 0; kt < kTiles; ++kt) {
         const int kin = kt % chunk, b = gc & 1;
         if (kin == 0 && gc >= 2 &&
@@ -367,14 +385,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
     const int half = (warp - 2) >> 2;      // which kCols accumulator columns
     const int row = q * 32 + lane;
-    // lanes are consecutive output rows: with unit m stride a warp's stores coalesce
-    const bool coalesced = C.sm0 == 1;
     int gc = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
-      int m0, n0, z, ktb, kTiles;
-      sch.decode(t, m0, n0, z, ktb, kTiles);
-      const int nChunks = (kTiles + chunk - 1) / chunk;
+      const TileRef T = decode_tile(L, t);
+      const Problem &P = L.prob[T.g];
+      const CView &C = P.C;
+      const int M = P.M, N = P.N, m0 = T.m0, n0 = T.n0, z = T.z;
+      // lanes are consecutive output rows: with unit m stride a warp's stores coalesce
+      const bool coalesced = C.sm0 == 1;
+      const int nChunks = (T.kTiles + P.chunk - 1) / P.chunk;
       const int ncol = min(kCols, N - (n0 + half * kCols));  // live columns (may be <= 0)
       double acc[kCols];
 #pragma unroll
@@ -507,13 +527,44 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
 }
 }  // namespace
 
-int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
-                         double alpha, double beta, const CView &C, cudaStream_t st) {
-  if (M <= 0 || N <= 0) return ACES_OK;
+namespace {
+// fills problem g of a launch (maps, dims, chunk); tiles and split-K are set by the caller
+int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, int nseg, int M,
+                int N, const CView &C) {
   if (nseg < 1 || nseg > kMaxSeg) {
     set_error("gemm_nt_bf16x3: %d K segments (1..%d)", nseg, kMaxSeg);
     return ACES_ERR_ARG;
   }
+  Problem &P = L.prob[g];
+  P.C = C;
+  P.M = M;
+  P.N = N;
+  P.nseg = nseg;
+  P.kt0[0] = 0;
+  for (int s = 0; s < nseg; ++s) {
+    const SplitOperand &a = A[s], &b = B[s];
+    if (a.k_pad != b.k_pad || a.rows < M || b.rows < N || a.k_pad % TBK || a.rows_pad < M ||
+        b.rows_pad < N || a.k_pad == 0) {
+      set_error("gemm_nt_bf16x3: operand shapes of segment %d do not match (%d/%d, %d, %d)", s,
+                a.k_pad, b.k_pad, a.rows, b.rows);
+      return ACES_ERR_ARG;
+    }
+    ACES_TRY(make_map(&L.ah[g][s], a.hi, a.rows_pad, a.k_pad, TBM));
+    ACES_TRY(make_map(&L.al[g][s], a.lo, a.rows_pad, a.k_pad, TBM));
+    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, TBN));
+    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, TBN));
+    P.kt0[s + 1] = P.kt0[s] + a.k_pad / TBK;
+  }
+  for (int s = nseg + 1; s <= kMaxSeg; ++s) P.kt0[s] = P.kt0[nseg];
+  P.kTilesTotal = P.kt0[nseg];
+  P.ktc = P.kTilesTotal;
+  P.chunk = chunk_for(P.kTilesTotal);
+  P.tilesM = (M + TBM - 1) / TBM;
+  P.tilesN = (N + TBN - 1) / TBN;
+  return ACES_OK;
+}
+
+int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -522,40 +573,32 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
     attr = true;
   }
-  SegMaps maps;
-  memset(&maps, 0, sizeof(maps));
-  maps.nseg = nseg;
-  maps.kt0[0] = 0;
-  for (int g = 0; g < nseg; ++g) {
-    const SplitOperand &a = A[g], &b = B[g];
-    if (a.k_pad != b.k_pad || a.rows < M || b.rows < N || a.k_pad % TBK || a.rows_pad < M ||
-        b.rows_pad < N || a.k_pad == 0) {
-      set_error("gemm_nt_bf16x3: operand shapes of segment %d do not match (%d/%d, %d, %d)", g,
-                a.k_pad, b.k_pad, a.rows, b.rows);
-      return ACES_ERR_ARG;
-    }
-    ACES_TRY(make_map(&maps.ah[g], a.hi, a.rows_pad, a.k_pad, TBM));
-    ACES_TRY(make_map(&maps.al[g], a.lo, a.rows_pad, a.k_pad, TBM));
-    ACES_TRY(make_map(&maps.bh[g], b.hi, b.rows_pad, b.k_pad, TBN));
-    ACES_TRY(make_map(&maps.bl[g], b.lo, b.rows_pad, b.k_pad, TBN));
-    maps.kt0[g + 1] = maps.kt0[g] + a.k_pad / TBK;
-  }
-  for (int g = nseg + 1; g <= kMaxSeg; ++g) maps.kt0[g] = maps.kt0[nseg];
-  TileSched sch;
-  sch.tilesN = (N + TBN - 1) / TBN;
-  sch.tilesM = (M + TBM - 1) / TBM;
-  sch.kTilesTotal = maps.kt0[nseg];
-  sch.ktc = sch.kTilesTotal;
+  const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
+  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(L, alpha, beta, part);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+}  // namespace
+
+int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
+                         double alpha, double beta, const CView &C, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return ACES_OK;
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.nprob = 1;
+  ACES_TRY(set_problem(L, 0, A, B, nseg, M, N, C));
+  Problem &P = L.prob[0];
   // split K when the output has too few tiles to fill the SMs
-  const long long tiles = (long long)sch.tilesN * sch.tilesM;
+  const long long tiles = (long long)P.tilesN * P.tilesM;
   const int nsm = num_sms();
   int Z = 1;
   double *part = nullptr;
-  if (tiles < nsm && sch.kTilesTotal >= 8) {
-    Z = (int)std::min<long long>((nsm + tiles - 1) / tiles, sch.kTilesTotal / 4);
+  if (tiles < nsm && P.kTilesTotal >= 8) {
+    Z = (int)std::min<long long>((nsm + tiles - 1) / tiles, P.kTilesTotal / 4);
     if (Z > 1) {
-      sch.ktc = (sch.kTilesTotal + Z - 1) / Z;
-      Z = (sch.kTilesTotal + sch.ktc - 1) / sch.ktc;
+      P.ktc = (P.kTilesTotal + Z - 1) / Z;
+      Z = (P.kTilesTotal + P.ktc - 1) / P.ktc;
       part = splitk_workspace((size_t)Z * M * N);
       if (!part) {
         set_error("gemm_nt_bf16x3: split-K workspace allocation failed");
@@ -568,14 +611,39 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
     set_error("gemm_nt_bf16x3: %lld output tiles exceed the scheduler range", nTiles);
     return ACES_ERR_ARG;
   }
-  const unsigned grid = (unsigned)std::min<long long>(nTiles, nsm);
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(maps, M, N, sch, (int)nTiles,
-                                                     chunk_for(sch.kTilesTotal), alpha, beta, C,
-                                                     part);
-  count_launch();
-  ACES_CUDA(cudaGetLastError());
+  P.tile0 = 0;
+  L.nTiles = (int)nTiles;
+  ACES_TRY(launch_prepared(L, alpha, beta, part, st));
   if (part) return splitk_reduce(C, part, M, N, Z, alpha, beta, st, true);
   return ACES_OK;
+}
+
+int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha, double beta,
+                           cudaStream_t st) {
+  if (nprob < 1 || nprob > kMaxProb) {
+    set_error("gemm_nt_bf16x3_grouped: %d problems (1..%d)", nprob, kMaxProb);
+    return ACES_ERR_ARG;
+  }
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  long long tiles = 0;
+  int n = 0;
+  for (int g = 0; g < nprob; ++g) {
+    const GroupedProblem &q = probs[g];
+    if (q.M <= 0 || q.N <= 0) continue;
+    ACES_TRY(set_problem(L, n, q.A, q.B, q.nseg, q.M, q.N, q.C));
+    L.prob[n].tile0 = (int)tiles;
+    tiles += (long long)L.prob[n].tilesM * L.prob[n].tilesN;
+    ++n;
+  }
+  if (n == 0) return ACES_OK;
+  if (tiles > (1LL << 31) - 1) {
+    set_error("gemm_nt_bf16x3_grouped: %lld output tiles exceed the scheduler range", tiles);
+    return ACES_ERR_ARG;
+  }
+  L.nprob = n;
+  L.nTiles = (int)tiles;
+  return launch_prepared(L, alpha, beta, nullptr, st);
 }
 
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,

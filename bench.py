@@ -614,6 +614,8 @@ KERNEL_CASES = {
 # captures of the (T) launches; B scaled by 0.25 so the amplitudes converge)
 PROGRAM_CASES = {
     "triples-o10-v180": dict(nocc=10, nvir=180, naux=540, seed=5, bscale=0.25),
+    # Lambda + density on the convergent C4 system (split precision)
+    "lambda-c4": dict(nocc=20, nvir=180, naux=600, seed=3, bscale=0.25, lam=True),
 }
 
 
@@ -623,17 +625,27 @@ def run_program_case(a):
     import torch
     import acesb200 as ab
     from acesb200.workloads import synthetic_df
-    wl = PROGRAM_CASES[a.kernel_case]
+    wl = dict(PROGRAM_CASES[a.kernel_case])
+    lam = wl.pop("lam", False)
     eps, B, _ = synthetic_df(**wl)
     e, lists, o, v = _lists_from_df(eps, B, wl["nocc"], wl["nvir"], torch.device("cuda", 0))
     lib = ab.load()
     lib.init(0)
     lib.sym_init([o], [v])
     put_lists(lib, e, lists)
-    c = lib.xvcc(cc_conv=7, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3, triples=1)
-    print(json.dumps({"kernel_case": a.kernel_case, "e_ccsd": c.e_ccsd, "cycles": c.ncycle,
-                      "e_t4": c.e_t4, "e_st5": c.e_st5,
-                      "seconds_triples": c.seconds_triples}), flush=True)
+    if lam:
+        c = lib.xvcc(cc_conv=9, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3)
+        cl = lib.xlambda(cc_conv=9, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3,
+                         timing_warmup=1)
+        lib.xdens()
+        print(json.dumps({"kernel_case": a.kernel_case, "e_ccsd": c.e_ccsd, "cycles": c.ncycle,
+                          "lambda_cycles": cl.ncycle,
+                          "lambda_seconds_per_iter": cl.seconds_per_iter}), flush=True)
+    else:
+        c = lib.xvcc(cc_conv=7, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3, triples=1)
+        print(json.dumps({"kernel_case": a.kernel_case, "e_ccsd": c.e_ccsd, "cycles": c.ncycle,
+                          "e_t4": c.e_t4, "e_st5": c.e_st5,
+                          "seconds_triples": c.seconds_triples}), flush=True)
     lib.fin()
 
 
