@@ -874,11 +874,11 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
       ACES_TRY(alloc(he[k], len));
     }
   ACES_TRY(copy(hx[idimr].p, cur, len));
-  launch_diff(he[idimr].p, nxt, cur, len, st);
-  launch_absmax(d + 3, he[idimr].p, o, v, scratch.p, st);
   std::vector<const double *> hp(ndimr);
   for (int k = 0; k < ndimr; ++k) hp[k] = he[k].p;
-  ACES_TRY(launch_diis_dots(d + 8, he[idimr].p, hp.data(), ndimr, o, v, scratch.p, st));
+  // error vector, its largest element and its DIIS dots in one pass
+  ACES_TRY(launch_diff_stats(he[idimr].p, nxt, cur, hp.data(), ndimr, idimr, o, v, scratch.p,
+                             d + 3, d + 8, st));
   double hd[40];
   ACES_CUDA(cudaMemcpyAsync(hd, d, 40 * 8, cudaMemcpyDeviceToHost, st));
   ACES_CUDA(cudaStreamSynchronize(st));

@@ -277,6 +277,49 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Split-K reduction with many slices and few outputs: one warp per output,
+// lane k adds slices k, k+32, ..., then a fixed shuffle tree (deterministic).
+// layout 0: part[z][m][n]; 1: part[z][n][m]; 2 / 3: part[z][l][s] of the thin
+// kernel with (m, n) = (l, s) / (s, l) and S the short dimension.
+__global__ void k_reduce_warp(CView C, const double *__restrict__ part, int M, int N, int Z,
+                              double alpha, double beta, int layout, int S) {
+  const long long total = (long long)M * N;
+  const int lane = threadIdx.x & 31;
+  for (long long idx = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; idx < total;
+       idx += ((long long)gridDim.x * blockDim.x) >> 5) {
+    double sum = 0.0;
+    for (int z = lane; z < Z; z += 32) sum += part[(size_t)z * total + idx];
+    for (int off = 16; off; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+    if (lane == 0) {
+      int m, n;
+      if (layout == 0) {
+        m = (int)(idx / N);
+        n = (int)(idx % N);
+      } else if (layout == 1) {
+        m = (int)(idx % M);
+        n = (int)(idx / M);
+      } else {  // thin partials: idx = l * S + s
+        const int l = (int)(idx / S), sidx = (int)(idx % S);
+        m = layout == 3 ? sidx : l;
+        n = layout == 3 ? l : sidx;
+      }
+      double *cp = C.p + cview_off(C, m, n);
+      double v = alpha * sum;
+      if (beta != 0.0) v += beta * *cp;
+      *cp = v;
+    }
+  }
+}
+
+static void launch_reduce_warp(const CView &C, const double *part, int M, int N, int Z,
+                               double alpha, double beta, int layout, int S, cudaStream_t st) {
+  const long long total = (long long)M * N;
+  long long nb = (total + 7) / 8;  // 8 warps per block
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_reduce_warp<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, layout, S);
+  count_launch();
+}
+
 // reduce thin split-K partials part[z][l][s] into C
 __global__ void k_thin_reduce(CView C, const double *__restrict__ part, int L, int S, int Z,
                               double alpha, double beta, bool s_is_m) {
@@ -418,6 +461,12 @@ double *splitk_workspace(size_t doubles) {
 int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
                   double beta, cudaStream_t st, bool mfast) {
   long long total = (long long)M * N;
+  if (Z >= 24 && total <= 16384) {
+    // few outputs, many slices: a warp per output instead of a serial loop
+    launch_reduce_warp(C, part, M, N, Z, alpha, beta, mfast ? 1 : 0, 0, st);
+    ACES_CUDA(cudaGetLastError());
+    return ACES_OK;
+  }
   long long nb = (total + 255) / 256;
   if (nb > 148 * 16) nb = 148 * 16;
   k_splitk_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, mfast);
@@ -473,7 +522,10 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
                                        Z > 1 ? part : nullptr);
     count_launch();
     ACES_CUDA(cudaGetLastError());
-    if (Z > 1) {
+    if (Z >= 24 && (long long)L * S <= 16384) {
+      launch_reduce_warp(C, part, M, N, Z, alpha, beta, s_is_m ? 3 : 2, S, st);
+      ACES_CUDA(cudaGetLastError());
+    } else if (Z > 1) {
       long long total = (long long)L * S;
       long long nb = (total + 255) / 256;
       if (nb > 148 * 16) nb = 148 * 16;

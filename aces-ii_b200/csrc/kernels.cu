@@ -48,6 +48,41 @@ __global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long 
   }
 }
 
+// The gather of k_permute_naive for outputs whose innermost extent is a
+// multiple of 4 (every source has unit stride along it): a thread owns 4
+// consecutive outputs of one row, splits its index once and issues 4
+// independent loads per term and two 16-byte stores.
+__global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long quads) {
+  for (long long qd = blockIdx.x * (long long)blockDim.x + threadIdx.x; qd < quads;
+       qd += (long long)gridDim.x * blockDim.x) {
+    const long long idx = qd * 4;
+    unsigned r = (unsigned)idx, q;
+    q = a.fd3.div(r); const int i3 = (int)(r - q * a.fd3.d); r = q;
+    q = a.fd2.div(r); const int i2 = (int)(r - q * a.fd2.d); r = q;
+    q = a.fd1.div(r); const int i1 = (int)(r - q * a.fd1.d);
+    const int i0 = (int)q;
+    double acc[4];
+    if (a.beta == 0.0) {
+      acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+    } else {
+      const double2 o0 = *reinterpret_cast<const double2 *>(out + idx);
+      const double2 o1 = *reinterpret_cast<const double2 *>(out + idx + 2);
+      acc[0] = a.beta * o0.x; acc[1] = a.beta * o0.y;
+      acc[2] = a.beta * o1.x; acc[3] = a.beta * o1.y;
+    }
+    for (int t = 0; t < a.nterms; ++t) {
+      const double *src = a.src[t] + i0 * a.s[t][0] + i1 * a.s[t][1] + i2 * a.s[t][2] + i3;
+      double x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = __ldg(src + u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] += a.alpha[t] * x[u];
+    }
+    *reinterpret_cast<double2 *>(out + idx) = make_double2(acc[0], acc[1]);
+    *reinterpret_cast<double2 *>(out + idx + 2) = make_double2(acc[2], acc[3]);
+  }
+}
+
 // 32x32 shared-memory tiles over (i3, i_d) where every term reads i_d with
 // unit stride: reads coalesced along i_d, writes coalesced along i3.
 template <int D>
@@ -141,7 +176,13 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
   } else {
     long long nb = (total + 255) / 256;
     if (nb > 148 * 64) nb = 148 * 64;
-    if (total < (1LL << 31))
+    const bool rows4 = all_unit3 && a.n[3] % 4 == 0 && total < (1LL << 31) &&
+                       ((uintptr_t)out & 15) == 0;
+    if (rows4) {
+      long long nq = (total / 4 + 255) / 256;
+      if (nq > 148 * 64) nq = 148 * 64;
+      k_permute_rows4<<<(unsigned)nq, 256, 0, st>>>(out, a, total / 4);
+    } else if (total < (1LL << 31))
       k_permute_naive<false><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
     else
       k_permute_naive<true><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
@@ -467,6 +508,98 @@ void launch_absmax(double *out, const double *x, int o, int v, double *scratch, 
                                        FastDiv((unsigned)v), FastDiv((unsigned)o));
   count_launch();
   k_absmax_final<<<1, 32, 0, st>>>(out, pv, pi, kRedBlocks); count_launch();
+}
+
+// One pass over the new DIIS error vector e = xnew - xold: writes e, its
+// signed absmax over T1, T2(AB) and packed T2(AA) (as k_absmax) and its dots
+// with the n history error vectors (as k_diis_dots; history slot `self` is e
+// itself, taken from registers).  The [j,i,a,b] partner of a T2 element is
+// recomputed from xnew and xold, never read back from e.
+__global__ void k_diff_stats(double *__restrict__ e, const double *__restrict__ xnew,
+                             const double *__restrict__ xold, HistPtrs h, int nh, int self,
+                             int o, int v, FastDiv fvv, FastDiv fv, FastDiv fo,
+                             double *__restrict__ part, double *__restrict__ pv,
+                             long long *__restrict__ pi) {
+  double s[25];
+  for (int k = 0; k < 25; ++k) s[k] = 0.0;
+  const long long n1 = (long long)o * v;
+  const long long n2 = (long long)o * o * v * v;
+  const long long vv = (long long)v * v;
+  double bv = 0.0;
+  long long bi = 0x7fffffffffffffffLL;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const double x = xnew[idx] - xold[idx];
+    e[idx] = x;
+    amax_merge(bv, bi, x, idx);
+    long long tix = -1;
+    double xp = 0.0;
+    if (idx >= n1) {
+      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
+      if (q.i < q.j) {
+        tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;  // [j,i,a,b]
+        xp = xnew[tix] - xold[tix];
+        if (q.a < q.b) amax_merge(bv, bi, x - xp, n1 + n2 + idx);
+      }
+    }
+    for (int k = 0; k < nh; ++k) {
+      const double y = k == self ? x : h.p[k][idx];
+      double acc = x * y;
+      if (tix >= 0) acc += x * (y - (k == self ? xp : h.p[k][tix]));
+      s[k] += acc;
+    }
+  }
+  // dots: same block reduction as k_diis_dots
+  __shared__ double sh[25][8];
+  __shared__ double sv[8];
+  __shared__ long long si[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 0; k < nh; ++k) {
+    double x = s[k];
+    for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+    if (lane == 0) sh[k][wid] = x;
+  }
+  for (int off = 16; off; off >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffff, bv, off);
+    const long long oi = __shfl_down_sync(0xffffffff, bi, off);
+    amax_merge(bv, bi, ov, oi);
+  }
+  if (lane == 0) {
+    sv[wid] = bv;
+    si[wid] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x < nh) {
+    double x = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+    part[(long long)blockIdx.x * 25 + threadIdx.x] = x;
+  }
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax_merge(bv, bi, sv[w], si[w]);
+    pv[blockIdx.x] = bv;
+    pi[blockIdx.x] = bi;
+  }
+}
+
+int launch_diff_stats(double *e, const double *xnew, const double *xold,
+                      const double *const *hist, int nh, int self, int o, int v,
+                      double *scratch, double *absmax_out, double *dots_out, cudaStream_t st) {
+  if (nh < 1 || nh > 25 || self < 0 || self >= nh) return ACES_ERR_ARG;
+  HistPtrs h;
+  for (int k = 0; k < 25; ++k) h.p[k] = k < nh ? hist[k] : nullptr;
+  double *part = scratch;                   // [kRedBlocks][25]
+  double *pv = scratch + kRedBlocks * 25;   // [kRedBlocks]
+  long long *pi = (long long *)(scratch + kRedBlocks * 26);
+  k_diff_stats<<<kRedBlocks, 256, 0, st>>>(e, xnew, xold, h, nh, self, o, v,
+                                           FastDiv((unsigned)(v * v)), FastDiv((unsigned)v),
+                                           FastDiv((unsigned)o), part, pv, pi);
+  count_launch();
+  k_absmax_final<<<1, 32, 0, st>>>(absmax_out, pv, pi, kRedBlocks);
+  count_launch();
+  k_final_sum<<<nh, 32, 0, st>>>(dots_out, part, kRedBlocks, 25);
+  count_launch();
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
 }
 
 // Bordered DIIS system [[0,-1..],[-1,B]] (lam,c) = (-1,0,..) by LU with

@@ -43,6 +43,12 @@ void launch_energy(double *out2, const double *t2, const double *t1, const doubl
 int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
                      int o, int v, double *scratch, cudaStream_t st);
 void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st);
+// e = xnew - xold (T1 + T2 of a pair-symmetric vector) with, in the same pass,
+// absmax_out[0] = signed absmax (as launch_absmax) and dots_out[k] = <e, hist[k]>
+// (as launch_diis_dots; hist[self] is e); scratch holds >= 592 * 27 doubles
+int launch_diff_stats(double *e, const double *xnew, const double *xold,
+                      const double *const *hist, int nh, int self, int o, int v,
+                      double *scratch, double *absmax_out, double *dots_out, cudaStream_t st);
 // signed absmax over [t1 | t2 | packed AA(t2)]
 void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st);
 // solve the bordered DIIS system for n <= 25 on the device (libr/dodiis.F);
