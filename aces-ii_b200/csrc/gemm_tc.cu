@@ -111,7 +111,11 @@ constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadran
 constexpr int kCols = 4 * TBN / kEpiWarps;            // accumulator columns per epilogue thread
 static_assert(kCols % 32 == 0 && kCols >= 32, "epilogue column span");
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr int kTmemCols = 2 * TBN;                    // two ping-pong accumulators
+#ifndef ACES_TC_NACC
+#define ACES_TC_NACC 2
+#endif
+constexpr int kNAcc = ACES_TC_NACC;                   // TMEM accumulators in rotation
+constexpr int kTmemCols = kNAcc * TBN;
 constexpr unsigned long long kWaitNs = 4000000000ULL;  // 4 s bound on any wait
 
 __device__ int g_tc_status;
@@ -264,10 +268,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
   uint64_t *full = bars;                      // [STAGES] TMA -> MMA
   uint64_t *empty = bars + STAGES;            // [STAGES] MMA -> TMA
-  uint64_t *acc_full = bars + 2 * STAGES;     // [2] MMA -> epilogue
-  uint64_t *acc_empty = bars + 2 * STAGES + 2;  // [2] epilogue -> MMA
-  uint64_t *mma_done = bars + 2 * STAGES + 4;   // all products retired (teardown)
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
+  uint64_t *acc_full = bars + 2 * STAGES;             // [kNAcc] MMA -> epilogue
+  uint64_t *acc_empty = bars + 2 * STAGES + kNAcc;    // [kNAcc] epilogue -> MMA
+  uint64_t *mma_done = bars + 2 * STAGES + 2 * kNAcc;  // all products retired (teardown)
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 2 * kNAcc + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kNAcc; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
       mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);
     }
@@ -342,9 +346,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       const TileRef T = decode_tile(L, t);
       const int kTiles = T.kTiles, chunk = L.prob[T.g].chunk;
       for (int kt = 0; kt < kTiles; ++kt) {
-        const int kin = kt % chunk, b = gc & 1;
-        if (kin == 0 && gc >= 2 &&
-            !mbar_wait(smem_u32(&acc_empty[b]), ((gc >> 1) - 1) & 1)) {
+        const int kin = kt % chunk, b = gc % kNAcc;
+        if (kin == 0 && gc >= kNAcc &&
+            !mbar_wait(smem_u32(&acc_empty[b]), ((gc / kNAcc) - 1) & 1)) {
           atomicExch(&g_tc_status, 5);
           *(volatile int *)abort_flag = 1;
           stop = true;
@@ -400,8 +404,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int j = 0; j < kCols; ++j) acc[j] = 0.0;
       for (int c = 0; c < nChunks; ++c, ++gc) {
-        const int b = gc & 1;
-        const bool w = mbar_wait(smem_u32(&acc_full[b]), (gc >> 1) & 1);
+        const int b = gc % kNAcc;
+        const bool w = mbar_wait(smem_u32(&acc_full[b]), (gc / kNAcc) & 1);
         if (!w) atomicExch(&g_tc_status, 4);
         ok = __all_sync(0xffffffffu, w && !*(volatile int *)abort_flag);
         if (!ok) break;
