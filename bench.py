@@ -56,7 +56,8 @@ def args():
                    help="skip the Lambda / density block (C4 system)")
     p.add_argument("--kernel-case", default=None,
                    help="run one small case for ncu captures and exit: a contraction "
-                        "shape through aces_xgemm (ladder-small, thin-t1, lowrank-t1) or "
+                        "shape through aces_xgemm (ladder-small, ladder-packed, thin-t1, "
+                        "lowrank-t1) or "
                         "CCSD(T) on a small system (triples-o10-v180)")
     return p.parse_args()
 
@@ -609,6 +610,9 @@ KERNEL_CASES = {
     # T1-dressing rank-o update W(jbm,e) += sum_n t(n,e) X(jbm,n) at o=20, v=180,
     # accumulated into the existing output: M = o*o*v = 72000, N = v = 180, K = o = 20
     "lowrank-t1": dict(m=72000, n=180, k=20, beta=1.0),
+    # symmetric block of the packed particle-particle ladder at o=20, v=180:
+    # M = K = v(v+1)/2 = 16290, N = o^2 = 400
+    "ladder-packed": dict(m=16290, n=400, k=16290),
 }
 # whole-program cases: a converged CCSD(T) on a small seeded system (ncu
 # captures of the (T) launches; B scaled by 0.25 so the amplitudes converge)
