@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -599,7 +600,19 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
   int Z = 1;
   double *part = nullptr;
   if (tiles < nsm && P.kTilesTotal >= 8) {
-    Z = (int)std::min<long long>((nsm + tiles - 1) / tiles, P.kTilesTotal / 4);
+    // the slice count (at least 4 k tiles each, at most ~4 waves of tiles)
+    // whose tiles fill the SMs' waves best; ties go to fewer slices (less
+    // partial traffic)
+    double best = 0.0;
+    const long long zmax = std::min<long long>(P.kTilesTotal / 4, (4LL * nsm + tiles - 1) / tiles);
+    for (int z = 2; z <= zmax; ++z) {
+      const double waves = (double)(tiles * z) / nsm;
+      const double eff = waves / std::ceil(waves);
+      if (eff > best + 1e-9) {
+        best = eff;
+        Z = z;
+      }
+    }
     if (Z > 1) {
       P.ktc = (P.kTilesTotal + Z - 1) / Z;
       Z = (P.kTilesTotal + P.ktc - 1) / P.ktc;

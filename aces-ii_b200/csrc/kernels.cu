@@ -734,29 +734,55 @@ void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Packed particle-particle ladder
 // ---------------------------------------------------------------------------
-// U+[p][q] = (V[ab,cd] + V[ab,dc]) / 2 (c < d), V[ab,cc];  U-[m][n] = (V[ab,cd] - V[ab,dc]) / 2
-// with (a,b) = pair p (or m), (c,d) = pair q (or n); one block row per output row
-__global__ void k_ladder_pack_v(double *__restrict__ Up, double *__restrict__ Um,
-                                const double *__restrict__ V, const int *__restrict__ pairs,
-                                int v) {
+// U+[p(a,b)][p(c,d)] = (V[ab,cd] + V[ab,dc]) / 2 (c < d), V[ab,cc];
+// U-[m(a,b)][m(c,d)] = (V[ab,cd] - V[ab,dc]) / 2, p(c,d) = d(d+1)/2 + c,
+// m(c,d) = d(d-1)/2 + c.  One block per (row a <= b, 32 x 32 tile pair of
+// (c, d) with the c tile <= the d tile): the [c][d] and [d][c] tiles of the
+// row's v x v block are read coalesced, the second through a shared-memory
+// transpose, and the packed outputs (consecutive c for one d) coalesce.
+__global__ void __launch_bounds__(256)
+    k_ladder_pack_v(double *__restrict__ Up, double *__restrict__ Um,
+                    const double *__restrict__ V, const int *__restrict__ pairs, int v,
+                    int ntile) {
+  __shared__ double t1[32][33];  // [c][d]
+  __shared__ double t2[32][33];  // [c][d] = V[ab][d][c]
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
+  const int npairs_t = ntile * (ntile + 1) / 2;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const size_t vv = (size_t)v * v;
-  for (int r = blockIdx.x; r < np + nm; r += gridDim.x) {
-    const bool sym = r < np;
+  for (long long blk = blockIdx.x; blk < (long long)np * npairs_t; blk += gridDim.x) {
+    const int r = (int)(blk / npairs_t);
+    int tp = (int)(blk - (long long)r * npairs_t);
+    // tile pair tp -> (tc <= td)
+    int td = 0;
+    while ((td + 1) * (td + 2) / 2 <= tp) ++td;
+    const int tc = tp - td * (td + 1) / 2;
     const int a = pairs[2 * r], b = pairs[2 * r + 1];
     const double *row = V + ((size_t)a * v + b) * vv;
-    if (sym) {
-      double *out = Up + (size_t)r * np;
-      for (int q = threadIdx.x; q < np; q += blockDim.x) {
-        const int c = pairs[2 * q], d = pairs[2 * q + 1];
-        out[q] = c == d ? row[(size_t)c * v + c]
-                        : 0.5 * (row[(size_t)c * v + d] + row[(size_t)d * v + c]);
-      }
-    } else {
-      double *out = Um + (size_t)(r - np) * nm;
-      for (int q = threadIdx.x; q < nm; q += blockDim.x) {
-        const int c = pairs[2 * (np + q)], d = pairs[2 * (np + q) + 1];
-        out[q] = 0.5 * (row[(size_t)c * v + d] - row[(size_t)d * v + c]);
+    const int c0 = tc * 32, d0 = td * 32;
+    __syncthreads();  // the previous tile's reads of t1/t2 are done
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int cl = ty + 8 * k;
+      const int c = c0 + cl, d = d0 + tx;
+      t1[cl][tx] = (c < v && d < v) ? row[(size_t)c * v + d] : 0.0;  // along d
+      const int dl = ty + 8 * k;
+      const int dd = d0 + dl, cc = c0 + tx;
+      t2[tx][dl] = (cc < v && dd < v) ? row[(size_t)dd * v + cc] : 0.0;  // along c
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int dl = ty + 8 * k, cl = tx;
+      const int c = c0 + cl, d = d0 + dl;
+      if (c >= v || d >= v || c > d) continue;
+      const double x = t1[cl][dl], y = t2[cl][dl];
+      if (c == d) {
+        Up[(size_t)r * np + (size_t)d * (d + 1) / 2 + c] = x;
+      } else {
+        Up[(size_t)r * np + (size_t)d * (d + 1) / 2 + c] = 0.5 * (x + y);
+        if (a < b) Um[(size_t)(b * (b - 1) / 2 + a) * nm + (size_t)d * (d - 1) / 2 + c] =
+            0.5 * (x - y);
       }
     }
   }
@@ -764,8 +790,10 @@ __global__ void k_ladder_pack_v(double *__restrict__ Up, double *__restrict__ Um
 
 void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pairs, int v,
                           cudaStream_t st) {
-  const int rows = v * v;  // np + nm
-  k_ladder_pack_v<<<std::min(rows, 148 * 16), 256, 0, st>>>(Up, Um, V, pairs, v);
+  const int ntile = (v + 31) / 32;
+  const long long blocks = (long long)(v * (v + 1) / 2) * (ntile * (ntile + 1) / 2);
+  k_ladder_pack_v<<<(unsigned)std::min<long long>(blocks, 148 * 64), 256, 0, st>>>(
+      Up, Um, V, pairs, v, ntile);
   count_launch();
 }
 

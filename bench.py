@@ -438,8 +438,9 @@ def accuracy(lib, wname, device, rank=0, world=1):
     put_lists(lib, eps, lists[1])
     res = {}
     for prec, name in ((ab.PREC_FP64, "fp64"), (ab.PREC_BF16X3, "bf16x3")):
+        # cycle 1 (integral splits, packed ladder matrices) is setup, not an iteration
         c = sharded_triples(lib, rank, world, cc_conv=9, cc_maxcyc=80, cc_exporder=5,
-                            precision=prec, allow_noconv=True)
+                            precision=prec, allow_noconv=True, timing_warmup=1)
         res[name] = {"e_corr": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
                      "seconds_per_iter": c.seconds_per_iter, "e_t4": c.e_t4, "e_st5": c.e_st5,
                      "seconds_triples": c.seconds_triples}
