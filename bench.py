@@ -368,7 +368,10 @@ def run_ours(a, rank, world, local_rank):
                 "peak_source": f"bf16_tflops_sustained of {pk_src} MEASURED_PEAKS.json",
                 "algorithmic_flops_per_launch": launch_flops,
                 "executed_bf16_flops_per_launch": executed,
-                "seconds_per_launch": s_lad, "traffic": LADDER_TRAFFIC.get(a.workload),
+                "seconds_per_launch": s_lad,
+                "seconds_note": "CUDA events around the packed ladder: the grouped launch "
+                                "plus its pack/unpack kernels (~0.16 ms at c2)",
+                "traffic": LADDER_TRAFFIC.get(a.workload),
                 "traffic_source": LADDER_TRAFFIC_SOURCE if a.workload in LADDER_TRAFFIC else None,
                 "algorithmic_bytes_per_launch": 4.0 * (n_p * n_p + n_m * n_m)
                 + 4.0 * (o * o) * (v * v) + 3 * 8.0 * (o * o) * (v * v)}
@@ -415,8 +418,9 @@ def run_ours(a, rank, world, local_rank):
 
 # DRAM bytes (read + write) of one packed ladder (its launches summed), from
 # the one-pass ncu launch list of the c2 bench (profiles/ccsd_cycle_c2_launches.md)
-LADDER_TRAFFIC = {}
-LADDER_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the ladder launches"
+LADDER_TRAFFIC = {"c2": 2637.7e6 + 98.1e6}
+LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped ladder "
+                         "launch in the c2 cycle (one-pass launch list)")
 
 
 def accuracy(lib, wname, device, rank=0, world=1):
