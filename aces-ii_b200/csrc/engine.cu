@@ -684,7 +684,10 @@ int CCEngine::residual() {
     ACES_CUDA(cudaEventCreate(&ev_lad0));
     ACES_CUDA(cudaEventCreate(&ev_lad1));
   }
-  ACES_CUDA(cudaEventRecord(ev_lad0, st));
+  // inside a graph capture the records become external event nodes, which
+  // record the events again on every replay (the ladder stays timed)
+  const unsigned evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  ACES_CUDA(cudaEventRecordWithFlags(ev_lad0, st, evflag));
   if (recording) {
     // the recorded (Lambda) pass keeps the dense form, whose adjoint the tape knows
     ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0,
@@ -692,7 +695,7 @@ int CCEngine::residual() {
   } else {
     ACES_TRY(ladder_packed());
   }
-  ACES_CUDA(cudaEventRecord(ev_lad1, st));
+  ACES_CUDA(cudaEventRecordWithFlags(ev_lad1, st, evflag));
 
   // ---- W(mbej) ABAB and ABBA (DWMBEJ, T1RING), layout W[j,b,m,e] ----
   ACES_TRY(copy(WA.p, WA0.p, (size_t)OO * VV));
@@ -819,7 +822,9 @@ int CCEngine::residual_run() {
   const double f0 = gemm_flops;
   cudaGraph_t graph = nullptr;
   ACES_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  capturing = true;
   const int s = residual();
+  capturing = false;
   const cudaError_t ce = cudaStreamEndCapture(st, &graph);
   if (s != ACES_OK) {
     if (graph) cudaGraphDestroy(graph);
@@ -1047,8 +1052,7 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
     ACES_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f, msl = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    // the ladder events are graph nodes when the residual is replayed: no time
-    if (!E.residual_exec && cudaEventElapsedTime(&msl, E.ev_lad0, E.ev_lad1) != cudaSuccess) {
+    if (cudaEventElapsedTime(&msl, E.ev_lad0, E.ev_lad1) != cudaSuccess) {
       cudaGetLastError();
       msl = 0.f;
     }

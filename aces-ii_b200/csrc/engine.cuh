@@ -34,6 +34,7 @@ class CCEngine {
   long long residual_launches = 0;
   double residual_flops = 0.0;
   int residual_passes = 0;
+  bool capturing = false;  // the residual pass is being captured into a graph
   int residual_run();
 
   // orbital data

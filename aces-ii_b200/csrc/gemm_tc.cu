@@ -6,10 +6,10 @@
 // lo = bf16(x - hi).  The kernel accumulates hi*hi + hi*lo + lo*hi for every
 // K slice into one TMEM accumulator (the lo*lo term, ~2^-18 relative, is
 // dropped), which gives ~16 significant bits per product and FP32 sums that
-// are promoted to FP64 every CHUNK k tiles (8, or fewer for very long K).
+// are promoted to FP64 every CHUNK = 512 K elements (fewer for very long K).
 //
-// Persistent kernel, one CTA per SM, output tile 128 x 128, k tile 64,
-// 3-stage mbarrier pipeline, 10 warps:
+// Persistent kernel, one CTA per SM, output tile 128 x 128, k tile 64, 3-stage
+// mbarrier pipeline (128-byte swizzle), 10 warps:
 //   warp 0  TMA producer (one elected lane)
 //   warp 1  TMEM allocator + MMA issuer (one elected lane)
 //   warps 2-9 epilogue: two warps per TMEM lane quadrant, each thread one
@@ -97,17 +97,31 @@ int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int 
 }
 
 namespace {
-constexpr int TBM = 128, TBN = 128, TBK = 64, STAGES = 3;
-// k tiles per FP32 accumulation chunk, by the contraction length K
-inline int chunk_for(int kTilesTotal) {
-  if (kTilesTotal <= 576) return 8;   // K <= 36864
-  if (kTilesTotal <= 1152) return 4;  // K <= 73728
-  return 2;
-}
+// k tile: 64 BF16 (128-byte rows, 128-byte swizzle, 3 stages), or 32 BF16
+// (64-byte rows, 64-byte swizzle), which fits 7 stages in shared memory but
+// measured slower on B200 (packed ladder M = K = 16290, N = 400: 1.08 ms
+// against 0.82 ms, tensor pipe 42 % against 57 % of active cycles).
+#ifndef ACES_TC_TBK
+#define ACES_TC_TBK 64
+#endif
+constexpr int TBM = 128, TBN = 128, TBK = ACES_TC_TBK;
+static_assert(TBK == 32 || TBK == 64, "k tile of 32 or 64 BF16");
+constexpr int kRowBytes = TBK * 2;                    // one swizzled smem row
+constexpr int kUnit = 64 / TBK;                       // k tiles per 64 K elements
 constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
 constexpr int TILE_B = TBN * TBK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
+constexpr int kSmemLimit = 227 * 1024;
+constexpr int STAGES = (kSmemLimit - 1024 - 256) / STAGE_BYTES;  // 3 (TBK 64) or 6/7 (TBK 32)
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment + barriers
+static_assert(SMEM_BYTES <= kSmemLimit && STAGES >= 3, "pipeline depth");
+// k tiles per FP32 accumulation chunk, by the contraction length K: 512 K
+// elements up to K = 36864, 256 up to 73728, 128 beyond
+inline int chunk_for(int kTilesTotal) {
+  if (kTilesTotal <= 576 * kUnit) return 8 * kUnit;
+  if (kTilesTotal <= 1152 * kUnit) return 4 * kUnit;
+  return 2 * kUnit;
+}
 constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
 constexpr int kCols = 4 * TBN / kEpiWarps;            // accumulator columns per epilogue thread
 static_assert(kCols % 32 == 0 && kCols >= 32, "epilogue column span");
@@ -139,13 +153,16 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
+// try_wait with a suspend-time hint: a waiting thread sleeps until the phase
+// completes (or 20 us pass) instead of re-polling, which leaves the issue
+// slots of its SM sub-partition to the MMA and TMA threads
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(20000u)
       : "memory");
   return ok != 0;
 }
@@ -166,15 +183,16 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
       : "memory");
 }
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), LBO unused (1), sm100 descriptor version 1.
+// UMMA shared-memory descriptor: K-major, swizzled rows of kRowBytes (128- or
+// 64-byte swizzle, layout type 2 or 4), 8-row groups 8 * kRowBytes apart (SBO),
+// LBO unused (1), sm100 descriptor version 1.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
   d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)((8 * kRowBytes) >> 4) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
+  d |= (uint64_t)(kRowBytes == 128 ? 2 : 4) << 61;
   return d;
 }
 // instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, N>>3, M>>4
@@ -204,15 +222,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       : "r"(taddr));
 }
 
-// The MMA warp accumulates CHUNK k tiles at a time in FP32 into one of two TMEM
-// accumulators (ping-pong); the epilogue warps drain every finished chunk into
-// FP64 registers while the next chunk is computed.  This bounds the number of
-// FP32 tensor-core accumulations any partial sum sees to 12*CHUNK, so the
+// The MMA warp accumulates CHUNK K elements at a time in FP32 into one of two
+// TMEM accumulators (ping-pong); the epilogue warps drain every finished chunk
+// into FP64 registers while the next chunk is computed.  This bounds the number
+// of FP32 tensor-core accumulations any partial sum sees to 3*CHUNK/16, so the
 // truncation bias of the tensor-core adders stays small instead of growing
 // with K.  The energy error of a CCSD solve grows linearly with CHUNK (o=20,
-// v=180: 1.4e-8 Eh at 2, 2.7e-8 at 4, 5.3e-8 at 8) while the drain cost per
-// product halves with every doubling; it also grows with the contraction
-// length (o=30, v=270 with 8 throughout: 7.8e-7 Eh), so CHUNK is 8 up to
+// v=180: 1.4e-8 Eh at 128, 2.7e-8 at 256, 5.3e-8 at 512) while the drain cost
+// per product halves with every doubling; it also grows with the contraction
+// length (o=30, v=270 with 512 throughout: 7.8e-7 Eh), so CHUNK is 512 up to
 // K = 36864 and smaller beyond (chunk_for).
 //
 // The kernel is persistent: gridDim.x <= #SMs CTAs walk the output tiles
@@ -366,13 +384,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
         const uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + TILE_B;
         const uint32_t acc_t = tmem + (uint32_t)(b * TBN);
+        // the start address is the descriptor's low field (address >> 4): the
+        // 32-byte K step (16 BF16) inside a swizzled row adds 2 to it
+        const uint64_t dah = umma_desc(ah), dal = umma_desc(al), dbh = umma_desc(bh),
+                       dbl = umma_desc(bl);
 #pragma unroll
         for (int kk = 0; kk < TBK / 16; ++kk) {
-          const uint32_t off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzled row
+          const uint64_t o = 2 * kk;
           const uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
-          umma(acc_t, umma_desc(ah + off), umma_desc(bh + off), acc);
-          umma(acc_t, umma_desc(ah + off), umma_desc(bl + off), 1u);
-          umma(acc_t, umma_desc(al + off), umma_desc(bh + off), 1u);
+          umma(acc_t, dah + o, dbh + o, acc);
+          umma(acc_t, dah + o, dbl + o, 1u);
+          umma(acc_t, dal + o, dbh + o, 1u);
         }
         umma_commit(smem_u32(&empty[s]));
         ++it;
@@ -522,7 +544,8 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
   cuuint32_t box[2] = {(cuuint32_t)TBK, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  kRowBytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -599,12 +622,13 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
   const int nsm = num_sms();
   int Z = 1;
   double *part = nullptr;
-  if (tiles < nsm && P.kTilesTotal >= 8) {
-    // the slice count (at least 4 k tiles each, at most ~4 waves of tiles)
-    // whose tiles fill the SMs' waves best; ties go to fewer slices (less
-    // partial traffic)
+  if (tiles < nsm && P.kTilesTotal >= 8 * kUnit) {
+    // the slice count (at least 256 K elements each, at most ~4 waves of
+    // tiles) whose tiles fill the SMs' waves best; ties go to fewer slices
+    // (less partial traffic)
     double best = 0.0;
-    const long long zmax = std::min<long long>(P.kTilesTotal / 4, (4LL * nsm + tiles - 1) / tiles);
+    const long long zmax =
+        std::min<long long>(P.kTilesTotal / (4 * kUnit), (4LL * nsm + tiles - 1) / tiles);
     for (int z = 2; z <= zmax; ++z) {
       const double waves = (double)(tiles * z) / nsm;
       const double eff = waves / std::ceil(waves);

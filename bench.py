@@ -48,8 +48,9 @@ def args():
     p.add_argument("--workload", default=W_NAME)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64-compare", action="store_true")
-    p.add_argument("--use-graph", type=int, default=0,
-                   help="1: replay each cycle's residual pass from a captured CUDA graph")
+    p.add_argument("--use-graph", type=int, default=1,
+                   help="1: replay each cycle's residual pass from a CUDA graph captured on "
+                        "the second cycle (0: launch every kernel from the host)")
     p.add_argument("--batch-bscale", type=float, default=1.0,
                    help="scale of the DF factors of the 64-system batch (--workload c5)")
     p.add_argument("--no-lambda", action="store_true",
@@ -319,7 +320,7 @@ def run_ours(a, rank, world, local_rank):
     fp64 = None
     if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
         c64 = lib.xvcc(cc_conv=30, cc_maxcyc=W + K, cc_exporder=5, precision=ab.PREC_FP64,
-                       timing_warmup=W, allow_noconv=True)
+                       timing_warmup=W, allow_noconv=True, use_graph=a.use_graph)
         fp64 = {"seconds_per_iter": c64.seconds_per_iter, "e_corr": c64.e_ccsd,
                 "dE_split_minus_fp64": e_split - c64.e_ccsd,
                 "speedup_split_vs_fp64": c64.seconds_per_iter / cfg.seconds_per_iter}
@@ -332,7 +333,8 @@ def run_ours(a, rank, world, local_rank):
     lib.sym_init([o], [v])
     h2d = put_lists(lib, eps, lists)
     tp = time.perf_counter()
-    ce = lib.xvcc(cc_conv=30, cc_maxcyc=K, cc_exporder=5, precision=prec, allow_noconv=True)
+    ce = lib.xvcc(cc_conv=30, cc_maxcyc=K, cc_exporder=5, precision=prec, allow_noconv=True,
+                  use_graph=a.use_graph)
     tx = time.perf_counter()
     nr, nc = lib.list_dims(1, 46)
     t2 = lib.getlst(1, nc, 1, 46)
@@ -351,11 +353,7 @@ def run_ours(a, rank, world, local_rank):
     n_p, n_m = v * (v + 1) // 2, v * (v - 1) // 2
     launch_flops = 2.0 * (o * o) * (n_p * n_p + n_m * n_m)
     dense_flops = 2.0 * (o * o) * (v * v) * (v * v)
-    if s_lad <= 0.0:  # graph replay: the ladder is not timed separately
-        roof = {"bound": "tensor", "kernel": "k_gemm_bf16x3 (particle-particle ladder)",
-                "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
-                "traffic": None, "note": "not measured under --use-graph 1"}
-    elif prec == ab.PREC_BF16X3:
+    if prec == ab.PREC_BF16X3:
         executed = 3.0 * launch_flops
         peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
         roof = {"bound": "tensor",
@@ -369,8 +367,9 @@ def run_ours(a, rank, world, local_rank):
                 "algorithmic_flops_per_launch": launch_flops,
                 "executed_bf16_flops_per_launch": executed,
                 "seconds_per_launch": s_lad,
-                "seconds_note": "CUDA events around the packed ladder: the grouped launch "
-                                "plus its pack/unpack kernels (~0.16 ms at c2)",
+                "seconds_note": "CUDA events around the packed ladder (external event nodes "
+                                "of the replayed residual graph under --use-graph 1): the "
+                                "grouped launch plus its pack/unpack kernels (~0.16 ms at c2)",
                 "traffic": LADDER_TRAFFIC.get(a.workload),
                 "traffic_source": LADDER_TRAFFIC_SOURCE if a.workload in LADDER_TRAFFIC else None,
                 "algorithmic_bytes_per_launch": 4.0 * (n_p * n_p + n_m * n_m)
@@ -392,7 +391,8 @@ def run_ours(a, rank, world, local_rank):
                                f"seed={wl['seed']}",
                    "precision": a.precision, "cycles_timed": K, "diis_order": 5,
                    "l2": "inputs larger than L2 (<ab|cd> 8.4 GB read every step)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "residual_graph": bool(a.use_graph)},
         "e2e": {"value": e2e, "unit": "s/iter", "h2d_bytes_per_step": h2d // K,
                 "d2h_bytes_per_step": d2h // K,
                 "note": "PUTLST of all lists + xvcc_run(K cycles) + GETLST T2, wall clock / K",
@@ -408,7 +408,8 @@ def run_ours(a, rank, world, local_rank):
         line["fp64_gpu"] = fp64
     if prec == ab.PREC_BF16X3 and not a.no_fp64_compare:
         del lists  # release the pinned host lists before the next workload's
-        line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank, rank, world)
+        line["accuracy"] = accuracy(lib, a.workload + "conv", local_rank, rank, world,
+                                    use_graph=a.use_graph)
     if prec == ab.PREC_BF16X3 and not a.no_lambda and a.workload == W_NAME:
         line["lambda"] = lambda_block(lib, "c4conv", local_rank)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -423,7 +424,7 @@ LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of th
                          "launch in the c2 cycle (one-pass launch list)")
 
 
-def accuracy(lib, wname, device, rank=0, world=1):
+def accuracy(lib, wname, device, rank=0, world=1, use_graph=1):
     """Split BF16x3 vs FP64 GPU on the convergent variant of the workload, both
     converged to max|dT| < 1e-9 (CC_CONV=9): |dE| of the correlation energy.
     With several ranks the (T) triplets are split over them (each rank solves
@@ -444,7 +445,8 @@ def accuracy(lib, wname, device, rank=0, world=1):
     for prec, name in ((ab.PREC_FP64, "fp64"), (ab.PREC_BF16X3, "bf16x3")):
         # cycle 1 (integral splits, packed ladder matrices) is setup, not an iteration
         c = sharded_triples(lib, rank, world, cc_conv=9, cc_maxcyc=80, cc_exporder=5,
-                            precision=prec, allow_noconv=True, timing_warmup=1)
+                            precision=prec, allow_noconv=True, timing_warmup=1,
+                            use_graph=use_graph)
         res[name] = {"e_corr": c.e_ccsd, "cycles": c.ncycle, "converged": bool(c.converged),
                      "seconds_per_iter": c.seconds_per_iter, "e_t4": c.e_t4, "e_st5": c.e_st5,
                      "seconds_triples": c.seconds_triples}

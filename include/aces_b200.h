@@ -160,7 +160,8 @@ typedef struct aces_cc_config {
   int triples;        /* 1: run (T) after CCSD (CALC=CCSD(T))                */
   int use_graph;      /* 1: the residual pass of every cycle after the second
                          is a replay of a CUDA graph captured on the second
-                         (seconds_ladder is then not measured)              */
+                         (the ladder stays timed through external event
+                         nodes of the graph)                                 */
   int verbose;        /* 1: per-iteration log on stdout (IFLAGS(1))          */
   int timing_warmup;  /* cycles excluded from the timing outputs             */
   /* outputs */
