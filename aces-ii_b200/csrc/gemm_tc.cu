@@ -234,8 +234,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // K = 36864 and smaller beyond (chunk_for).
 //
 // The kernel is persistent: gridDim.x <= #SMs CTAs walk the output tiles
-// t = blockIdx.x, blockIdx.x + gridDim.x, ... (n tile fastest, then m tile,
-// then the split-K slice z).  The TMA producer and the MMA issuer run their
+// t = blockIdx.x, blockIdx.x + gridDim.x, ... (the side with fewer tiles
+// fastest, then the other, then the split-K slice z).  The TMA producer and
+// the MMA issuer run their
 // k-tile sequence straight across tile boundaries (stage and TMEM-buffer
 // parities are global counters), so the loads and products of the next tile
 // overlap the epilogue of the current one.
@@ -243,13 +244,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // keeps every SM busy where one product has too few tiles for whole waves),
 // each C_g = alpha * sum_s A_gs B_gs^T + beta C_g over up to kMaxSeg K
 // segments with their own tensor maps.  Tiles are numbered problem by
-// problem; within a problem n tile fastest, then m tile, then split-K slice.
+// problem; within a problem as above.
 constexpr int kMaxSeg = 4, kMaxProb = 3;
 struct Problem {
   CView C;
   int M, N, tilesM, tilesN;
   int ktc, kTilesTotal;  // k tiles per split-K slice, in total
   int tile0;             // first tile of this problem
+  int mfast;             // tile order: m tile fastest (else n tile fastest)
   int nseg, chunk;
   int kt0[kMaxSeg + 1];  // segment s owns global k tiles [kt0[s], kt0[s+1])
 };
@@ -268,9 +270,18 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   while (r.g + 1 < L.nprob && t >= L.prob[r.g + 1].tile0) ++r.g;
   const Problem &P = L.prob[r.g];
   const int tl = t - P.tile0;
-  const int tn = tl % P.tilesN, q = tl / P.tilesN;
-  const int tm = q % P.tilesM;
-  r.z = q / P.tilesM;
+  int tm, tn;
+  if (P.mfast) {
+    tm = tl % P.tilesM;
+    const int q = tl / P.tilesM;
+    tn = q % P.tilesN;
+    r.z = q / P.tilesN;
+  } else {
+    tn = tl % P.tilesN;
+    const int q = tl / P.tilesN;
+    tm = q % P.tilesM;
+    r.z = q / P.tilesM;
+  }
   r.m0 = tm * TBM;
   r.n0 = tn * TBN;
   r.ktb = r.z * P.ktc;
@@ -589,6 +600,10 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
   P.chunk = chunk_for(P.kTilesTotal);
   P.tilesM = (M + TBM - 1) / TBM;
   P.tilesN = (N + TBN - 1) / TBN;
+  // the side with fewer tiles runs fastest, so the CTAs working at the same
+  // time share the row block of the larger operand (read from DRAM once,
+  // then from L2): with a few m tiles and many n tiles, B is the large operand
+  P.mfast = P.tilesM < P.tilesN ? 1 : 0;
   return ACES_OK;
 }
 
