@@ -11,11 +11,16 @@ the engine's xvcc_run entry point.  Printed JSON line:
   value      device time per iteration (CUDA events on the engine stream,
              inputs resident in HBM, W warm-up cycles excluded), BF16x3 split
              contractions on tcgen05 (default) or FP64 (--precision fp64);
+             from the third cycle on, the residual pass is the replay of a
+             CUDA graph captured on the second (--use-graph 0 launches every
+             kernel from the host);
   e2e        the same metric through the C-ABI with HOST lists: PUTLST of the
              six integral lists from pinned memory, xvcc_run for K cycles and
              GETLST of T2, all inside the timed region, divided by K;
-  roofline   the particle-particle ladder contraction (2 o^2 v^4 flops, 3 BF16
-             products each) against the measured bf16 peak;
+  roofline   the packed particle-particle ladder (2 o^2 (np^2 + nm^2) flops
+             for the symmetric and antisymmetric pair blocks, 3 BF16 products
+             each), timed by CUDA events around it inside every cycle,
+             against the measured sustained bf16 peak;
   cpu_baseline  the FP64 numpy restatement of the reference (oracle/) on the
              host cores, one CCSD iteration of the same system.
 
@@ -48,9 +53,10 @@ def args():
     p.add_argument("--workload", default=W_NAME)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64-compare", action="store_true")
-    p.add_argument("--use-graph", type=int, default=1,
+    p.add_argument("--use-graph", type=int, default=None,
                    help="1: replay each cycle's residual pass from a CUDA graph captured on "
-                        "the second cycle (0: launch every kernel from the host)")
+                        "the second cycle, 0: launch every kernel from the host (default 1, "
+                        "and 0 for the c5 batch, whose short solves do not amortise a capture)")
     p.add_argument("--batch-bscale", type=float, default=1.0,
                    help="scale of the DF factors of the 64-system batch (--workload c5)")
     p.add_argument("--no-lambda", action="store_true",
@@ -60,7 +66,10 @@ def args():
                         "shape through aces_xgemm (ladder-small, ladder-packed, thin-t1, "
                         "lowrank-t1) or "
                         "CCSD(T) on a small system (triples-o10-v180)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.use_graph is None:
+        a.use_graph = 0 if a.workload == "c5" else 1
+    return a
 
 
 def peaks():
