@@ -196,14 +196,20 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return d;
 }
 // instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, N>>3, M>>4
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) |
-                            ((uint32_t)(TBM >> 4) << 24);
+// (the N field, bits 17-22, is set per tile: a ragged last n tile multiplies
+// only its live columns rounded up to 16, the granularity of N at M = 128)
+constexpr uint32_t kIdescMK = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBM >> 4) << 24);
+__device__ __forceinline__ uint32_t idesc_for(int n_live) {
+  const int n = min(TBN, (n_live + 15) & ~15);
+  return kIdescMK | ((uint32_t)(n >> 3) << 17);
+}
 
-__device__ __forceinline__ void umma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t acc) {
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                     uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-      "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -375,6 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
       const TileRef T = decode_tile(L, t);
       const int kTiles = T.kTiles, chunk = L.prob[T.g].chunk;
+      const uint32_t idesc = idesc_for(L.prob[T.g].N - T.n0);
       for (int kt = 0; kt < kTiles; ++kt) {
         const int kin = kt % chunk, b = gc % kNAcc;
         if (kin == 0 && gc >= kNAcc &&
@@ -403,9 +410,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int kk = 0; kk < TBK / 16; ++kk) {
           const uint64_t o = 2 * kk;
           const uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
-          umma(acc_t, dah + o, dbh + o, acc);
-          umma(acc_t, dah + o, dbl + o, 1u);
-          umma(acc_t, dal + o, dbh + o, 1u);
+          umma(acc_t, dah + o, dbh + o, idesc, acc);
+          umma(acc_t, dah + o, dbl + o, idesc, 1u);
+          umma(acc_t, dal + o, dbh + o, idesc, 1u);
         }
         umma_commit(smem_u32(&empty[s]));
         ++it;
