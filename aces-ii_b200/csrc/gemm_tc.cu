@@ -23,6 +23,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <mutex>
+#include <unordered_map>
 
 #include "common.cuh"
 #include "gemm.cuh"
@@ -551,7 +554,45 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// Encoded maps by their only variable inputs: a map is a pure function of
+// (address, rows, k, box rows), so a cached map is exactly what a new encode
+// would produce, even for a freed and reused address.  (T) asks for the same
+// operand views for every triplet: 16 maps per launch without the cache.
+struct MapKey {
+  const void *base;
+  int rows_pad, k_pad, box_rows;
+  bool operator==(const MapKey &o) const {
+    return base == o.base && rows_pad == o.rows_pad && k_pad == o.k_pad &&
+           box_rows == o.box_rows;
+  }
+};
+struct MapKeyHash {
+  size_t operator()(const MapKey &k) const {
+    size_t h = std::hash<const void *>()(k.base);
+    h ^= ((size_t)k.rows_pad * 0x9E3779B97F4A7C15ULL) + ((size_t)k.k_pad << 20) + k.box_rows;
+    return h;
+  }
+};
+struct MapCache {
+  std::mutex mu;
+  std::unordered_map<MapKey, CUtensorMap, MapKeyHash> maps;
+};
+MapCache &map_cache() {
+  static MapCache *c = new MapCache();
+  return *c;
+}
+
 int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) {
+  const MapKey key{base, rows_pad, k_pad, box_rows};
+  MapCache &mc = map_cache();
+  {
+    std::lock_guard<std::mutex> lk(mc.mu);
+    auto it = mc.maps.find(key);
+    if (it != mc.maps.end()) {
+      *m = it->second;
+      return ACES_OK;
+    }
+  }
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -569,6 +610,9 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
     return ACES_ERR_CUDA;
   }
+  std::lock_guard<std::mutex> lk(mc.mu);
+  if (mc.maps.size() >= 16384) mc.maps.clear();
+  mc.maps.emplace(key, *m);
   return ACES_OK;
 }
 }  // namespace
