@@ -197,6 +197,36 @@ def residual(B, t1, t2):
     return Z1, Z2
 
 
+def ladder_packed(vvvv, tt):
+    """The particle-particle ladder sum_ef <ab|ef> tau(ij,ef) in the RHF a<=b
+    packing of vcc/ladab1.F:55-64 (pair blocks + SYMEXP4), in the symmetric /
+    antisymmetric form the engine evaluates: with <ba|dc> = <ab|cd> and
+    tau(ji,dc) = tau(ij,cd),
+      U+[ab,cd] = (<ab|cd> + <ab|dc>)/2 (c<d), <ab|cc> (c=d);  tau+ = tau[cd] + tau[dc] (c<d), tau[cc]
+      U-[ab,cd] = (<ab|cd> - <ab|dc>)/2 (c<d);                 tau- = tau[cd] - tau[dc]
+      S[ij,a<=b] = sum_{c<=d} U+ tau+,  A[ij,a<b] = sum_{c<d} U- tau-
+      Z[ab] = S + A,  Z[ba] = S - A,  Z[aa] = S.
+    Returns Z[i,j,a,b] (the dense contraction's value)."""
+    o, v = tt.shape[0], tt.shape[2]
+    iu, ju = np.triu_indices(v)          # pairs c <= d (upper triangle incl. diagonal)
+    im, jm = np.triu_indices(v, 1)       # pairs c < d
+    diag = iu == ju
+    Up = 0.5 * (vvvv[:, :, iu, ju] + vvvv[:, :, ju, iu])
+    Up = Up[iu, ju]                      # rows a <= b
+    Um = 0.5 * (vvvv[:, :, im, jm] - vvvv[:, :, jm, im])[im, jm]
+    tp = tt[:, :, iu, ju] + tt[:, :, ju, iu]
+    tp[:, :, diag] *= 0.5                # the diagonal pair once
+    tm = tt[:, :, im, jm] - tt[:, :, jm, im]
+    S = np.einsum("ijq,pq->ijp", tp, Up, optimize=True)
+    A = np.einsum("ijq,pq->ijp", tm, Um, optimize=True)
+    Z = np.zeros((o, o, v, v))
+    Z[:, :, iu, ju] += S
+    Z[:, :, ju, iu] += S * (~diag)       # Z[ba] = S - A below; the diagonal once
+    Z[:, :, im, jm] += A
+    Z[:, :, jm, im] -= A
+    return Z
+
+
 def _ovoo(B):
     """<mb|ij> as [m,b,i,j]; with real orbitals <mb|ij> = <ij|mb> = ooov[i,j,m,b]."""
     return _tr(B.ooov, 2, 3, 0, 1)

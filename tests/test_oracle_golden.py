@@ -130,3 +130,25 @@ def test_triples_equals_spin_orbital():
     e4, e5 = triples(ham, t1, t2)
     assert abs(e4 - np.sum(t3c * D * t3c) / 36) < 1e-16
     assert abs(e5 - np.sum(t3c * D * t3d) / 36) < 1e-18
+
+
+def test_packed_ladder_equals_dense_ladder(h2o035):
+    """The a<=b packed particle-particle ladder (vcc/ladab1.F:55-64) in the
+    symmetric/antisymmetric form the engine runs equals the dense
+    sum_ef <ab|ef> tau(ij,ef), on the real H2O/DZP integrals at the MP2
+    amplitudes and on a synthetic DF system with T1 in tau."""
+    B = ccsd.Blocks(h2o035)
+    t1, t2 = ccsd.mp2_guess(B)
+    tt = ccsd.tau(t1, t2)
+    dense = np.einsum("ijef,abef->ijab", tt, B.vvvv, optimize=True)
+    np.testing.assert_allclose(ccsd.ladder_packed(B.vvvv, tt), dense, rtol=0, atol=1e-14)
+    ham = synthetic(4, 13, 30, seed=9)
+    Bs = ccsd.Blocks(ham)
+    rng = np.random.default_rng(3)
+    t1 = rng.normal(0.0, 0.05, (4, 13))
+    t2 = rng.normal(0.0, 0.05, (4, 4, 13, 13))
+    t2 = 0.5 * (t2 + t2.transpose(1, 0, 3, 2))
+    tt = ccsd.tau(t1, t2)
+    dense = np.einsum("ijef,abef->ijab", tt, Bs.vvvv, optimize=True)
+    np.testing.assert_allclose(ccsd.ladder_packed(Bs.vvvv, tt), dense,
+                               rtol=0, atol=1e-13 * np.abs(dense).max())
