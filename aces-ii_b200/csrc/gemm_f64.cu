@@ -442,20 +442,26 @@ static int launch_lowrank(int M, int N, int K, double alpha, const double *A, lo
   return ACES_OK;
 }
 
+// split-K partials of the current device (one buffer per device, grown on demand)
 double *splitk_workspace(size_t doubles) {
-  static double *ws = nullptr;
-  static size_t cap = 0;
-  if (doubles > cap) {
-    if (ws) dev_free(ws);
-    ws = nullptr;
-    cap = 0;
-    if (dev_alloc((void **)&ws, doubles * sizeof(double)) != cudaSuccess) {
+  static double *ws[64] = {nullptr};
+  static size_t cap[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (doubles > cap[dev]) {
+    if (ws[dev]) dev_free(ws[dev]);
+    ws[dev] = nullptr;
+    cap[dev] = 0;
+    if (dev_alloc((void **)&ws[dev], doubles * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
-    cap = doubles;
+    cap[dev] = doubles;
   }
-  return ws;
+  return ws[dev];
 }
 
 int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, double alpha,
@@ -535,13 +541,19 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
     }
     return ACES_OK;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[64] = {false};  // the shared-memory opt-in is per device
+  int dev = 0;
+  ACES_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("gemm_nt_f64: device %d outside 0..63", dev);
+    return ACES_ERR_ARG;
+  }
+  if (!attr_set[dev]) {
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_nt_f64<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSmemBytes));
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_nt_f64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSmemBytes));
-    attr_set = true;
+    attr_set[dev] = true;
   }
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   if (grid.y > 65535) {

@@ -659,13 +659,20 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
 }
 
 int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
+  // the shared-memory opt-in and the status word are per device
+  static bool attr[64] = {false};
+  int dev = 0;
+  ACES_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("gemm_nt_bf16x3: device %d outside 0..63", dev);
+    return ACES_ERR_ARG;
+  }
+  if (!attr[dev]) {
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    SMEM_BYTES));
     int zero = 0;
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
-    attr = true;
+    attr[dev] = true;
   }
   const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
   k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(L, alpha, beta, part);

@@ -16,6 +16,7 @@
 // (triplet, block) and reduced in a fixed order: the FP64 energy sum is
 // deterministic.
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "engine.cuh"
@@ -202,14 +203,31 @@ __global__ void __launch_bounds__(1024) k_sum_pairs(double *out, const double *p
 int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nranks) {
   const long long O = o, V = v;
   const long long V2 = V * V, V3 = V * V * V;
-  cudaEvent_t t0, t1e;
+  cudaEvent_t t0 = nullptr, t1e = nullptr;
+  DBuf Gv, GvT, t2P, t2Q, Hn, Wb, part, outp;
+  SplitOperand sT2, sGv, sGvT, sHn, sT2P, sT2Q;
+  // every exit, the error returns included, gives back the scratch and events
+  struct Release {
+    std::function<void()> f;
+    ~Release() { f(); }
+  } release_scratch{[&] {
+    for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp}) {
+      if (b->p) dev_free(b->p);
+      b->p = nullptr;
+    }
+    for (SplitOperand *sp : {&sT2, &sGv, &sGvT, &sHn, &sT2P, &sT2Q}) {
+      if (sp->hi) dev_free(sp->hi);
+      sp->hi = sp->lo = nullptr;
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1e) cudaEventDestroy(t1e);
+  }};
   ACES_CUDA(cudaEventCreate(&t0));
   ACES_CUDA(cudaEventCreate(&t1e));
   ACES_CUDA(cudaEventRecord(t0, st));
   const long long sv[4] = {V * V * V, V * V, V, 1};      // I_ovvv[m,a,e,f]
   const long long s3[4] = {O * O * V, O * V, V, 1};      // I_ooov[m,n,i,e]
   const long long st2[4] = {O * V * V, V * V, V, 1};     // t2[i,j,a,b]
-  DBuf Gv, GvT, t2P, t2Q, Hn, Wb, part, outp;
   // Gv[k,b,c,d] = (bd|ck) = <bc|dk> = I_ovvv[k,d,c,b]; GvT[k,c,b,d] = Gv[k,b,c,d]
   ACES_TRY(alloc(Gv, O * V3));
   ACES_TRY(perm(Gv.p, o, v, v, v, 0.0, {PermTerm{I_ovvv.p, 1.0, {sv[0], sv[3], sv[2], sv[1]}}}));
@@ -241,7 +259,6 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   ACES_TRY(alloc(part, (size_t)ntrip * nblk * 2));
   ACES_TRY(alloc(outp, 2));
   const bool use_split = prec == ACES_PREC_BF16X3 && v >= 128;
-  SplitOperand sT2, sGv, sGvT, sHn, sT2P, sT2Q;
   if (use_split) {
     ACES_TRY(split_pack(sT2, t2(), V, o * o * v, v, st));       // rows (x,y,alpha), K = d
     ACES_TRY(split_pack(sGv, Gv.p, V, o * v * v, v, st));       // rows (z,beta,gamma), K = d
@@ -336,14 +353,6 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   *seconds = ms * 1e-3;
   *e4 = h[0];
   *e5 = h[1];
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1e);
-  for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp}) {
-    if (b->p) dev_free(b->p);
-    b->p = nullptr;
-  }
-  for (SplitOperand *sp : {&sT2, &sGv, &sGvT, &sHn, &sT2P, &sT2Q})
-    if (sp->hi) dev_free(sp->hi);
   if (!std::isfinite(*e4) || !std::isfinite(*e5)) {
     set_error("(T): non-finite energy");
     return ACES_ERR_NAN;
