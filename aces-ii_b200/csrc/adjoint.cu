@@ -239,6 +239,14 @@ int CCEngine::backward() {
       double *dbar = adj(op.dst);
       if (is_active(op.src)) launch_axpy(adj(op.src), dbar, 1.0, (long long)op.count, st);
       launch_scale(dbar, 0.0, (long long)op.count, st);
+    } else if (op.kind == TapeOp::LADDER) {
+      // out += V in with V = <ab|cd> symmetric: in_bar += V out_bar, the same
+      // packed ladder (out_bar is not changed: the forward accumulates)
+      if (is_active(op.src)) {
+        double *ob = adj(op.dst), *ib = adj(op.src);
+        if (!ob || !ib) return ACES_ERR_NOMEM;
+        ACES_TRY(ladder_packed(ob, ib));
+      }
     } else if (op.kind == TapeOp::TAU) {
       double *tb = adj(op.tau);
       launch_tau_adjoint(adj(op.t2), adj(op.t1), tb, op.t1, op.c, o, v, st);

@@ -18,7 +18,7 @@
 namespace acesb200 {
 
 struct TapeOp {
-  enum Kind { GEMM, PERM, COPY, TAU } kind;
+  enum Kind { GEMM, PERM, COPY, TAU, LADDER } kind;
   // GEMM: C(view) = alpha * A B^T + beta * C
   int M = 0, N = 0, K = 0;
   double alpha = 0, beta = 0;
@@ -31,6 +31,7 @@ struct TapeOp {
   PermSpec spec{};
   bool t_act[4] = {false, false, false, false};
   // COPY: dst <- src (count doubles)
+  // LADDER: dst[ij,ab] += sum_cd <ab|cd> src[ij,cd] (the packed pp ladder)
   double *dst = nullptr;
   const double *src = nullptr;
   size_t count = 0;

@@ -689,11 +689,21 @@ int CCEngine::residual() {
   const unsigned evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   ACES_CUDA(cudaEventRecordWithFlags(ev_lad0, st, evflag));
   if (recording) {
-    // the recorded (Lambda) pass keeps the dense form, whose adjoint the tape knows
-    ACES_TRY(G(v * v, o * o, v * v, 1.0, I_vvvv.p, VV, tau.p, VV, 1.0,
-               cview_colmajor(Z2.p, VV), true));
-  } else {
-    ACES_TRY(ladder_packed());
+    // one tape entry for the whole ladder: its adjoint is the same packed
+    // ladder applied to the output's adjoint (<ab|cd> = <cd|ab>)
+    TapeOp op;
+    op.kind = TapeOp::LADDER;
+    op.src = tau.p;
+    op.dst = Z2.p;
+    if (is_active(tau.p)) mark_active(Z2.p);
+    tape.push_back(op);
+  }
+  {
+    const bool rec = recording;
+    recording = false;  // the ladder's own products and kernels are not taped
+    const int ls = ladder_packed(tau.p, Z2.p);
+    recording = rec;
+    ACES_TRY(ls);
   }
   ACES_CUDA(cudaEventRecordWithFlags(ev_lad1, st, evflag));
 
@@ -767,7 +777,9 @@ int CCEngine::residual() {
 //   Z2[ab] += S + A,  Z2[ba] += S - A,  Z2[aa] += S
 // Two contractions of (v(v+1)/2)^2 and (v(v-1)/2)^2 x o^2 instead of v^4 x o^2:
 // half the flops.  U+/U- are built once from the dense <ab|cd> (or the list).
-int CCEngine::ladder_packed() {
+// The map is linear in tau and needs no symmetry of it, so the Lambda
+// backward pass calls it with (Z2 adjoint, tau adjoint) for in and out.
+int CCEngine::ladder_packed(const double *in, double *out) {
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2, oo = o * o;
   if (!Up.p) {
     // pair tables: p(c,d) = d(d+1)/2 + c (c <= d), m(c,d) = d(d-1)/2 + c (c < d)
@@ -795,12 +807,12 @@ int CCEngine::ladder_packed() {
   ACES_TRY(alloc(taum, (size_t)oo * std::max(nm, 1)));
   ACES_TRY(alloc(Sld, (size_t)oo * np));
   ACES_TRY(alloc(Ald, (size_t)oo * std::max(nm, 1)));
-  launch_ladder_pack_tau(taup.p, taum.p, tau.p, (const int *)ladpairs.p, v, oo, st);
+  launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st);
   // both products in one grouped launch (their tiles fill each other's last wave)
   const GArgs g[2] = {{np, oo, np, Up.p, np, taup.p, np, cview_colmajor(Sld.p, np), true, false},
                       {nm, oo, nm, Um.p, nm, taum.p, nm, cview_colmajor(Ald.p, nm), true, false}};
   ACES_TRY(Ggroup(g, nm > 0 ? 2 : 1, 0.0));
-  launch_ladder_unpack(Z2.p, Sld.p, Ald.p, v, oo, st);
+  launch_ladder_unpack(out, Sld.p, Ald.p, v, oo, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }

@@ -60,7 +60,8 @@ class CCEngine {
       WmnT, t1T, Fae, Fmi, Fme, Fp, Fpp, FmiT, FppT, FmeT, tmp4;
   // packed particle-particle ladder (symmetric / antisymmetric pair combinations)
   DBuf Up, Um, taup, taum, Sld, Ald, ladpairs;
-  int ladder_packed();  // Z2 += <ab|cd> tau(ij,cd) at half the dense flops
+  // out[ij,ab] += <ab|cd> in[ij,cd] at half the dense flops
+  int ladder_packed(const double *in, double *out);
   DBuf scratch, dev_small;  // reductions / DIIS scalars
   // DIIS history
   std::vector<DBuf> hx, he;
