@@ -124,6 +124,17 @@ def test_ccsd_h2o_dzp_matches_oracle_and_reference(lib):
     np.testing.assert_allclose(aa, ref["t2"] - ref["t2"].transpose(0, 1, 3, 2), atol=1e-11)
 
 
+def test_ccsd_h2o_dzp_026_matches_reference(lib):
+    """Second golden geometry, out.zmat.026 (R=0.96 A, A=104 deg): the same
+    11 iterations and the converged CCSD energy of :677."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat026.npz"))
+    setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=7, cc_maxcyc=50, cc_exporder=5)
+    assert cfg.converged == 1 and cfg.ncycle == 11
+    assert abs(cfg.e_ccsd - (-0.226261749882)) < 1e-10
+    assert abs(ham.e_scf + cfg.e_ccsd - (-76.272545457483)) < 1e-10
+
+
 @pytest.mark.parametrize("o,v,naux,seed", [(6, 24, 40, 5), (9, 41, 60, 11)])
 def test_ccsd_synthetic_c1_matches_oracle(lib, o, v, naux, seed):
     ham = synthetic(o, v, naux, seed)

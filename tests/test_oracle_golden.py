@@ -32,6 +32,22 @@ GOLD_035_DRES = [0.80606944e-02, 0.24718504e-02, 0.86146781e-03, 0.86891628e-04,
                  0.24698868e-06, 0.61904624e-07, 0.10316917e-07]
 
 
+# out.zmat.026 (H2O/DZP, R=0.96 A, A=104 deg, the CCSD of the first-order
+# properties job): "Summary of iterative solution of CC equations" :665-677,
+# per-iteration maxima :570-632, amplitude norms :646/:658, MP2 :530-545
+GOLD_026_ITER = [
+    -0.217208070842, -0.221613733226, -0.225105466772, -0.225882139977, -0.226238701153,
+    -0.226259784917, -0.226261880533, -0.226261678232, -0.226261750159, -0.226261766032,
+    -0.226261752235, -0.226261749882,
+]
+GOLD_026_RES = [0.81020837e-02, 0.23343131e-02, 0.11138743e-02, 0.17013937e-03,
+                0.13042336e-03, 0.43938616e-04, 0.16929190e-04, 0.24720746e-05,
+                0.39616913e-06, 0.10378036e-06, 0.17358044e-07]
+GOLD_026_DRES = [0.81020837e-02, 0.25114774e-02, 0.87657768e-03, 0.88183039e-04,
+                 0.83485227e-04, 0.18278810e-04, 0.50242777e-05, 0.82730424e-06,
+                 0.25734839e-06, 0.62318640e-07, 0.10602429e-07]
+
+
 @pytest.fixture(scope="module")
 def h2o035():
     return from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat035.npz"))
@@ -152,3 +168,24 @@ def test_packed_ladder_equals_dense_ladder(h2o035):
     dense = np.einsum("ijef,abef->ijab", tt, Bs.vvvv, optimize=True)
     np.testing.assert_allclose(ccsd.ladder_packed(Bs.vvvv, tt), dense,
                                rtol=0, atol=1e-13 * np.abs(dense).max())
+
+
+def test_ccsd_026_matches_reference():
+    """A third geometry (out.zmat.026): SCF, MP2, every CCSD iteration's energy
+    and residual maxima, the converged energy and amplitude norms."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat026.npz"))
+    # E(SCF) :451, nuclear repulsion 9.16938 a.u. (z-matrix analysis)
+    assert abs(ham.e_scf - (-76.0462837076)) < 1e-10
+    B = ccsd.Blocks(ham)
+    t1, t2 = ccsd.mp2_guess(B)
+    eaa, eab, etot = ccsd.energy(B, t1, t2)
+    assert abs(eaa - (-0.025991950000)) < 1e-10 and abs(eab - (-0.165224170842)) < 1e-10
+    assert abs(np.linalg.norm(t2) - 0.1987656990) < 1e-9
+    h = ccsd.run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5)
+    assert h["converged"] and h["ncycle"] == 11
+    np.testing.assert_allclose(h["energies"], GOLD_026_ITER, atol=1e-10)
+    np.testing.assert_allclose(np.abs(h["res"]), GOLD_026_RES, rtol=2e-7)
+    np.testing.assert_allclose(np.abs(h["dres"]), GOLD_026_DRES, rtol=2e-7)
+    assert abs(h["e_final"] - (-0.226261749882)) < 1e-10
+    assert abs(np.linalg.norm(h["t1"]) - 0.0193257962) < 1e-9
+    assert abs(np.linalg.norm(h["t2"]) - 0.2200706819) < 1e-9
