@@ -97,6 +97,70 @@ def solve_lambda(B, t1, t2, symmetric=True):
     return lam[:n1].reshape(o, v), lam[n1:].reshape(o, o, v, v)
 
 
+def lambda_to_reference(l1, l2):
+    """The reference's closed-shell multipliers (lists 190 and 146, the
+    alpha-beta block) from this module's: lambda = dL/dr for the spin-adapted
+    residual r of oracle.ccsd, l1 = 2 L1 and l2 = 2 L2 - L2~ (L2~: virtuals
+    swapped), so L1 = l1 / 2 and L2 = (2 l2 + l2~) / 3."""
+    return 0.5 * l1, (2.0 * l2 + l2.transpose(0, 1, 3, 2)) / 3.0
+
+
+def lambda_from_reference(L1, L2):
+    """Inverse of lambda_to_reference."""
+    return 2.0 * L1, 2.0 * L2 - L2.transpose(0, 1, 3, 2)
+
+
+def iterate_lambda(B, t1, t2, cc_conv=7, maxcyc=50, exporder=5):
+    """The xlambda cycle (lambda/vlamcc.F:597-927) as the reference runs it:
+    multipliers kept in the reference's convention (lambda_to_reference),
+    started from the converged amplitudes (the lists 190/146/144 initialised
+    from 90/46/44, as the copies of vlamcc.F:533-546), each cycle
+    lambda <- (dE/dT + (dZ/dT)^T lambda) / D (NEWT2, :756) with the pair
+    symmetrisation of the amplitude solver, convergence on the largest element
+    of the change (DRTSTS, :791) and the DIIS of the amplitude solver over the
+    reference's vector L1 + L2(AB) + packed L2(AA) (DODIIS0, :812).
+
+    Returns dict(res, dres, converged, ncycle, L1, L2 (reference convention),
+    l1, l2 (this module's))."""
+    import torch
+    from .diis import ReferenceDIIS
+    TB = TorchBlocks(B, torch)
+    o, v = B.o, B.v
+    t1t = torch.tensor(t1, dtype=torch.float64, requires_grad=True)
+    t2t = torch.tensor(t2, dtype=torch.float64, requires_grad=True)
+    g1, g2 = torch.autograd.grad(_energy(TB, t1t, t2t), [t1t, t2t])
+    g1, g2 = g1.numpy(), g2.numpy()
+    Z1, Z2 = ccsd.residual(TB, t1t, t2t)
+    D1, D2 = TB.Dov.detach().numpy(), TB.Doovv.detach().numpy()
+
+    def jtv(l1, l2):
+        a, b = torch.autograd.grad([Z1, Z2], [t1t, t2t], [torch.tensor(l1), torch.tensor(l2)],
+                                   retain_graph=True)
+        return a.numpy(), b.numpy()
+
+    L1, L2 = np.array(t1, dtype=float), ccsd.symmetrize_t2(np.array(t2, dtype=float))
+    dii = ReferenceDIIS(exporder)
+    hist = dict(res=[], dres=[])
+    converged = False
+    for icycle in range(1, maxcyc + 1):
+        l1, l2 = lambda_from_reference(L1, L2)
+        a, b = jtv(l1, l2)
+        n1, n2 = lambda_to_reference((g1 + a) / D1, ccsd.symmetrize_t2((g2 + b) / D2))
+        res, dres, ext = dii.step(icycle, ccsd.diis_vector(L1, L2), ccsd.diis_vector(n1, n2))
+        hist["res"].append(res)
+        hist["dres"].append(dres)
+        if abs(res) < 10.0 ** (-cc_conv):
+            converged = True
+            break
+        if ext is not None:
+            L1, L2 = (x.copy() for x in ccsd.split_vector(ext, o, v))
+        else:
+            L1, L2 = n1, n2
+    l1, l2 = lambda_from_reference(L1, L2)
+    hist.update(converged=converged, ncycle=icycle, L1=L1, L2=L2, l1=l1, l2=l2)
+    return hist
+
+
 def density(B, t1, t2, l1, l2):
     """D_pq = dL/df_pq (occupied-occupied, virtual-virtual, occupied-virtual
     blocks; the engine reads f_ov only, so D_vo = 0)."""
