@@ -188,7 +188,23 @@ extern "C" int xlambda_run(aces_cc_config *cfg) {
   cfg->last_residual = res;
   cfg->seconds_per_iter = ntimed ? ms_total * 1e-3 / ntimed : 0.0;
   // L1 -> list 190, L2(AB) -> list 146, L2(AA) -> list 144 (vcc/vcc.F:622-626 list map)
-  ACES_TRY(E.write_amplitudes(E.L.p, E.L.p + ov, 190, 146, 144));
+  // in the reference's convention: the engine iterates the Lagrange multipliers
+  // l of its spin-adapted residual, l1 = 2 L1 and l2 = 2 L2 - L2~ (L2~: the
+  // virtual indices swapped), so the lists get L1 = l1 / 2, L2 = (2 l2 + l2~) / 3
+  {
+    DBuf r;
+    ACES_TRY(E.alloc(r, len));
+    const long long st2[4] = {O * V * V, V * V, V, 1};
+    int ws = E.perm(r.p, 1, 1, E.o, E.v, 0.0, {PermTerm{E.L.p, 0.5, {0, 0, V, 1}}});
+    if (ws == ACES_OK)
+      ws = E.perm(r.p + ov, E.o, E.o, E.v, E.v, 0.0,
+                  {PermTerm{E.L.p + ov, 2.0 / 3.0, {st2[0], st2[1], st2[2], st2[3]}},
+                   PermTerm{E.L.p + ov, 1.0 / 3.0, {st2[0], st2[1], st2[3], st2[2]}}});
+    if (ws == ACES_OK) ws = E.write_amplitudes(r.p, r.p + ov, 190, 146, 144);
+    ACES_CUDA(cudaStreamSynchronize(E.st));
+    dev_free(r.p);
+    ACES_TRY(ws);
+  }
   if (!converged) {
     set_error("Lambda equations did not converge in %d cycles", cfg->cc_maxcyc);
     return ACES_ERR_NOCONV;

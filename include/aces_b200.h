@@ -194,7 +194,10 @@ typedef struct aces_cc_config {
 int xvcc_run(aces_cc_config *cfg);
 
 /* PROGRAM VLAMCC (lambda/vlamcc.F): Lambda equations for the amplitudes left
- * by xvcc_run; writes L1 to list 190 (irrep 1) and L2(AB) to list 146. */
+ * by xvcc_run; writes L1 to list 190 (irrep 1), L2(AB) to list 146 and
+ * L2(AA) = L2 - L2~ to list 144, in the reference's convention (the
+ * multipliers its own xlambda leaves there: L1 = l1/2, L2 = (2 l2 + l2~)/3 of
+ * the Lagrange multipliers l of the spin-adapted residual). */
 int xlambda_run(aces_cc_config *cfg);
 
 /* DENSOO/DENSVV/DENSVO (dens/densoo.F, densvv.F, densvo.F): the CCSD

@@ -58,8 +58,10 @@ def test_lambda_and_density_match_autograd_oracle(lib, o, v, naux, seed, irreps)
     t1, t2 = read_amplitudes(lib, dpd, o, v)
     l1, l2 = read_lambda(lib, dpd, o, v)
     rl1, rl2 = lambda_ad.solve_lambda(B, t1, t2)
-    np.testing.assert_allclose(l1, rl1, atol=1e-10)
-    np.testing.assert_allclose(l2, rl2, atol=1e-10)
+    # lists 190/146 hold the reference's multipliers (lambda_ad.lambda_to_reference)
+    L1, L2 = lambda_ad.lambda_to_reference(rl1, rl2)
+    np.testing.assert_allclose(l1, L1, atol=1e-10)
+    np.testing.assert_allclose(l2, L2, atol=1e-10)
     D = lib.getrec("DENSMAT", (o + v) ** 2).reshape(o + v, o + v)
     np.testing.assert_allclose(D, lambda_ad.density(B, t1, t2, rl1, rl2), atol=1e-10)
 
@@ -89,6 +91,13 @@ def test_lambda_h2o_dzp_symmetry_blocked(lib):
     lib.xdens()
     t1, t2 = read_amplitudes(lib, dpd, ham.nocc, ham.nvir)
     l1, l2 = read_lambda(lib, dpd, ham.nocc, ham.nvir)
+    # the reference's Lambda cycle (pinned to out.zmat.026's xlambda history
+    # in tests/test_oracle_lambda.py) converges to the lists' multipliers
+    h = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
+    r = lambda_ad.iterate_lambda(h["blocks"], h["t1"], h["t2"], cc_conv=9, maxcyc=60)
+    assert r["converged"]
+    np.testing.assert_allclose(l1, r["L1"], atol=5e-8)
+    np.testing.assert_allclose(l2, r["L2"], atol=5e-8)
     # lambda2 is the pair-symmetric multiplier of T2; its norm is of the size of T2's
     assert np.abs(l2 - l2.transpose(1, 0, 3, 2)).max() < 1e-12
     assert 0.5 < np.linalg.norm(l2) / np.linalg.norm(t2) < 2.0
