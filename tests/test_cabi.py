@@ -85,3 +85,30 @@ def test_bad_arguments_return_status(lib):
     assert lib.h.aces_irpdpd(2, 13) < 0
     assert lib.h.aces_irpdpd(1, 23) < 0
     assert lib.h.aces_getlst(None, 1, 1, 9, 1) < 0
+
+
+def test_header_is_c99_and_config_layout_matches_ctypes(tmp_path):
+    """include/aces_b200.h compiles as C99 (a Fortran/C host includes it as
+    is), and the aces_cc_config layout a C compiler gives (size and every
+    field offset) is the one acesb200.CCConfig passes through ctypes."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    fields = [f for f, _ in ab.CCConfig._fields_]
+    src = tmp_path / "layout.c"
+    body = "\n".join(f'  printf("%s %zu\\n", "{f}", offsetof(aces_cc_config, {f}));' for f in fields)
+    src.write_text(
+        "#include <stddef.h>\n#include <stdio.h>\n#include \"aces_b200.h\"\n"
+        "int main(void) {\n"
+        '  printf("sizeof %zu\\n", sizeof(aces_cc_config));\n' + body + "\n  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True, text=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True,
+                                                       text=True, check=True).stdout.split("\n")
+               if line)
+    assert int(out["sizeof"]) == ctypes.sizeof(ab.CCConfig)
+    for f in fields:
+        assert int(out[f]) == getattr(ab.CCConfig, f).offset, f
