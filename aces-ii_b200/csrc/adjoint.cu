@@ -3,6 +3,7 @@
 
 #include "adjoint.cuh"
 #include "engine.cuh"
+#include "perm_plan.cuh"
 
 namespace acesb200 {
 
@@ -230,9 +231,21 @@ int CCEngine::backward() {
     } else if (op.kind == TapeOp::PERM) {
       double *obar = adj(op.out);
       if (!obar) return ACES_ERR_NOMEM;
-      for (int t = 0; t < op.spec.nterms; ++t)
-        if (op.t_act[t]) launch_perm_scatter_add(adj(op.spec.t[t].src), obar, op.spec.t[t],
-                                                 op.spec.n, st);
+      for (int t = 0; t < op.spec.nterms; ++t) {
+        if (!op.t_act[t]) continue;
+        const PermTerm &pt = op.spec.t[t];
+        double *sbar = adj(pt.src);
+        if (!sbar) return ACES_ERR_NOMEM;
+        int m[4];
+        long long ts[4];
+        if (inverse_perm_plan(op.spec.n, pt.s, m, ts)) {
+          // a dense bijection: the inverse resort, accumulated (beta = 1)
+          ACES_TRY(perm(sbar, m[0], m[1], m[2], m[3], 1.0,
+                        {PermTerm{obar, pt.alpha, {ts[0], ts[1], ts[2], ts[3]}}}));
+        } else {
+          launch_perm_scatter_add(sbar, obar, pt, op.spec.n, st);
+        }
+      }
       long long total = (long long)op.spec.n[0] * op.spec.n[1] * op.spec.n[2] * op.spec.n[3];
       if (op.spec.beta != 1.0) launch_scale(obar, op.spec.beta, total, st);
     } else if (op.kind == TapeOp::COPY) {
