@@ -32,7 +32,7 @@ PREC_BF16X3 = 1
 
 # exported C-ABI symbols (include/aces_b200.h)
 SYMBOLS = [
-    "aces_init", "aces_fin", "aces_last_error", "aces_sym_init", "aces_irpdpd",
+    "aces_init", "aces_fin", "aces_last_error", "aces_pool_stats", "aces_sym_init", "aces_irpdpd",
     "aces_isymoff", "aces_dirprd", "aces_list_touch", "aces_updmoi", "aces_inipck",
     "aces_isytyp", "aces_list_dims", "aces_getlst", "aces_putlst", "aces_getlst_dev",
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
@@ -104,6 +104,14 @@ class Lib:
 
     def error(self):
         return self.h.aces_last_error().decode()
+
+    def pool_stats(self):
+        """(device buffers requested, cudaMalloc calls, cached bytes) of the
+        library's caching allocator since load."""
+        a, d, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._chk("aces_pool_stats",
+                  self.h.aces_pool_stats(C.byref(a), C.byref(d), C.byref(c)))
+        return a.value, d.value, c.value
 
     # ---- runtime / symmetry -------------------------------------------------
     def init(self, device=0):

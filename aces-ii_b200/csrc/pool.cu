@@ -7,6 +7,7 @@
 // solves such as the 64-system batch.  Released blocks are therefore kept per
 // device and size class and handed out again; they return to the driver only
 // when an allocation would otherwise fail, or at aces_fin.
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -37,6 +38,8 @@ size_t cache_cap(Pool &P, int dev) {
   P.cap[dev] = c;
   return c;
 }
+// every dev_alloc call, and the ones the cache could not serve (cudaMalloc)
+std::atomic<long long> g_alloc_calls{0}, g_driver_allocs{0};
 Pool &pool() {
   static Pool *p = new Pool();  // never destroyed: blocks may be released at exit
   return *p;
@@ -67,6 +70,7 @@ cudaError_t dev_alloc(void **ptr, size_t bytes) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   const size_t cls = size_class(bytes);
+  g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
   Pool &P = pool();
   std::lock_guard<std::mutex> lk(P.mu);
   // smallest cached block of this device that fits without wasting more than
@@ -80,6 +84,7 @@ cudaError_t dev_alloc(void **ptr, size_t bytes) {
     P.free_blocks.erase(it);
     return cudaSuccess;
   }
+  g_driver_allocs.fetch_add(1, std::memory_order_relaxed);
   e = cudaMalloc(ptr, cls);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -137,3 +142,18 @@ void pool_trim() {
 }
 
 }  // namespace acesb200
+
+extern "C" int aces_pool_stats(long long *alloc_calls, long long *driver_allocs,
+                               long long *cached_bytes) {
+  using namespace acesb200;
+  if (alloc_calls) *alloc_calls = g_alloc_calls.load();
+  if (driver_allocs) *driver_allocs = g_driver_allocs.load();
+  if (cached_bytes) {
+    Pool &P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    long long c = 0;
+    for (auto &kv : P.cached) c += (long long)kv.second;
+    *cached_bytes = c;
+  }
+  return ACES_OK;
+}

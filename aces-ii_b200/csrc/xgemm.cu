@@ -1,5 +1,6 @@
 // xgemm.cu -- the reference's XGEMM boundary (tools/xgemm.F:10-49) on device
 // pointers, routed to the engine's contraction kernels.
+#include <algorithm>
 #include <cctype>
 
 #include "common.cuh"
@@ -35,6 +36,11 @@ extern "C" int aces_xgemm(char transa, char transb, int m, int n, int k, double 
   if ((long long)m * n == 0) return ACES_OK;  // quick return (tools/xgemm.F)
   if (ldc < (m > 1 ? m : 1)) {
     set_error("aces_xgemm: ldc < m");
+    return ACES_ERR_ARG;
+  }
+  // leading dimensions as DGEMM checks them: op(A) is m x k, op(B) is k x n
+  if (lda < std::max(1, ta == 'N' ? m : k) || ldb < std::max(1, tb == 'N' ? k : n)) {
+    set_error("aces_xgemm: lda %d or ldb %d below the operand's row count", lda, ldb);
     return ACES_ERR_ARG;
   }
   cudaStream_t st = 0;

@@ -19,6 +19,7 @@
 // array: calls that overlap on the GPU (several host threads, or several
 // streams) race on it.  Each call writes every scratch element it reads
 // before reading it, so nothing has to start at zero.
+#include <algorithm>
 #include <cctype>
 #include <map>
 #include <mutex>
@@ -90,6 +91,11 @@ extern "C" int aces_xgemm_static(char transa, char transb, int m, int n, int k, 
   if ((long long)m * n == 0) return ACES_OK;
   if (ldc < (m > 1 ? m : 1)) {
     set_error("aces_xgemm_static: ldc < m");
+    return ACES_ERR_ARG;
+  }
+  // leading dimensions as DGEMM checks them: op(A) is m x k, op(B) is k x n
+  if (lda < std::max(1, ta == 'N' ? m : k) || ldb < std::max(1, tb == 'N' ? k : n)) {
+    set_error("aces_xgemm_static: lda %d or ldb %d below the operand's row count", lda, ldb);
     return ACES_ERR_ARG;
   }
   size_t need = (ta == 'N' ? (size_t)m * k : 0) + (tb == 'T' ? (size_t)n * k : 0);

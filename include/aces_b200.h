@@ -55,6 +55,13 @@ int aces_init(int device);
 int aces_fin(void);
 /* Last error message (static storage). */
 const char *aces_last_error(void);
+/* Device-memory accounting of the library's caching allocator (no
+ * counterpart in the reference, whose ICORE heap is one up-front malloc,
+ * acescore/aces_malloc.c:48): alloc_calls counts every device buffer the
+ * library has requested since load, driver_allocs the requests the cache
+ * could not serve (cudaMalloc calls), cached_bytes the released memory held
+ * for reuse.  Any pointer may be NULL. */
+int aces_pool_stats(long long *alloc_calls, long long *driver_allocs, long long *cached_bytes);
 
 /* ---- symmetry / DPD metadata ------------------------------------------- */
 

@@ -119,14 +119,34 @@ def hermite_R(L, alpha, PC):
     return {(t, u, v): Rn[(t, u, v, 0)] for (t, u, v, n) in Rn if n == 0}
 
 
+# Real solid harmonics of degree 2 as combinations of the normalised
+# Cartesian components (xx, xy, xz, yy, yz, zz), each normalised by itself:
+# with x^2 = sqrt(3) g_xx (up to the common radial norm) the five pure-d
+# polynomials xy, xz, yz, x^2 - y^2, 2z^2 - x^2 - y^2 are spanned without the
+# r^2 (s-type) combination.  Scale factors do not matter (energies are
+# invariant to the normalisation of each AO).  The second entry is a
+# representative exponent triple whose parities under x -> -x and y -> -y are
+# the function's own (used to classify molecular orbitals by irrep).
+_SPH_D = [
+    ([0.0, 1.0, 0.0, 0.0, 0.0, 0.0], (1, 1, 0)),                 # xy
+    ([0.0, 0.0, 1.0, 0.0, 0.0, 0.0], (1, 0, 1)),                 # xz
+    ([0.0, 0.0, 0.0, 0.0, 1.0, 0.0], (0, 1, 1)),                 # yz
+    ([math.sqrt(3.0), 0.0, 0.0, -math.sqrt(3.0), 0.0, 0.0], (2, 0, 0)),   # x^2 - y^2
+    ([-math.sqrt(3.0), 0.0, 0.0, -math.sqrt(3.0), 0.0, 2.0 * math.sqrt(3.0)], (0, 0, 2)),
+]
+
+
 class Basis:
     """Primitive Cartesian functions and their contraction into AO functions.
 
     shells: list of (center(3,), l, exps(np), coefs(np, ncontr)) per atom shell
-    block as read from GENBAS.
+    block as read from GENBAS.  With ``spherical`` the d shells contribute the
+    five real solid harmonics instead of the six Cartesian components (the
+    reference's SPHERICAL=ON, its default for the correlation-consistent
+    sets); s and p shells are the same either way.
     """
 
-    def __init__(self, shells):
+    def __init__(self, shells, spherical=False):
         self.prim_shells = []  # (center, l, alpha)
         self.prim_funcs = []   # (prim_shell_index, (lx,ly,lz))
         rows = []              # contraction entries (prim_func, ao, coef)
@@ -160,6 +180,30 @@ class Basis:
         D = np.zeros((self.nprim, nao))
         for p, ao, c in rows:
             D[p, ao] += c
+        if spherical:
+            # Cartesian AO -> spherical AO, shell by shell in generation order
+            cols, centers, ls = [], [], []
+            k = 0
+            for center, l, exps, coefs in shells:
+                ncomp = len(cart_components(l))
+                for ic in range(coefs.shape[1]):
+                    if l < 2:
+                        for ci in range(ncomp):
+                            e = np.zeros(nao); e[k + ci] = 1.0
+                            cols.append(e)
+                            centers.append(self.ao_center[k + ci]); ls.append(self.ao_l[k + ci])
+                    elif l == 2:
+                        for w, rep in _SPH_D:
+                            e = np.zeros(nao); e[k:k + 6] = w
+                            cols.append(e)
+                            centers.append(self.ao_center[k]); ls.append(rep)
+                    else:
+                        raise NotImplementedError("spherical functions above d")
+                    k += ncomp
+            Tcs = np.array(cols).T
+            D = D @ Tcs
+            self.nao = Tcs.shape[1]
+            self.ao_center, self.ao_l = centers, ls
         self.D = D
 
     # ---- primitive-level integrals, grouped by angular-momentum class ----

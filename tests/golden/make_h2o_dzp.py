@@ -1,27 +1,36 @@
-"""Generate the H2O/DZP molecular-orbital fixtures that pin the CCSD oracle.
+"""Generate the H2O molecular-orbital fixtures that pin the CCSD oracle.
 
-Run in a container that holds the reference tree (it reads the DZP basis from
-the reference's basis library, test/KEEP/GENBAS, and nothing else):
+Run in a container that holds the reference tree (it reads the DZP and
+cc-pVDZ basis sets from the reference's basis library, test/KEEP/GENBAS, and
+nothing else); the reference root is a required argument:
 
-    python tests/golden/make_h2o_dzp.py /root/reference
+    python tests/golden/make_h2o_dzp.py <reference root> [tag ...]
 
-Writes tests/golden/h2o_dzp_<tag>.npz for the geometries of the reference's
-regression inputs:
+Writes tests/golden/<file> for the geometries of the reference's regression
+inputs and for the cc-pVDZ benchmark system:
 
-  * ``zmat035``: test/zmat.035.ccsd (R=0.957 A, A=104.5 deg), golden CCSD
+  * ``zmat035``: test/zmat.035.ccsd (R=0.957 A, A=104.5 deg), DZP, golden CCSD
     iteration energies in test/OUTPUT/out.zmat.035.ccsd:555-650;
-  * ``zmat020``: test/zmat.020 (R=1.0 A, A=104 deg), golden CCSD and (T)
+  * ``zmat020``: test/zmat.020 (R=1.0 A, A=104 deg), DZP, golden CCSD and (T)
     energies in test/OUTPUT/out.zmat.020:650-688;
-  * ``zmat026``: test/zmat.026 (R=0.96 A, A=104 deg), CCSD first-order
-    properties.
+  * ``zmat026``: test/zmat.026 (R=0.96 A, A=104 deg), DZP, CCSD first-order
+    properties;
+  * ``zmat046``: test/zmat.046 (R=0.95720197 A, A=104.52 deg), DZP with
+    Cartesian d (SPHERICAL=OFF); the reference runs a UHF-CCSD on this closed
+    shell, whose SCF, MP2 and converged CCSD energies equal the RHF ones
+    (test/OUTPUT/out.zmat.046:461,605-608,745);
+  * ``ccpvdz``: H2O at R=0.9572 A, A=104.52 deg in cc-pVDZ with spherical d
+    functions (24 basis functions, 5 occupied / 19 virtual, C2v), the
+    plain-FP64 benchmark system; the reference has no output for it, so it
+    is pinned through the oracle only.
 
 Each file holds: orbital energies (occupied then virtual, each block sorted by
 irrep as the reference's DPD lists order them), the irrep populations
 (pop, vrt), the MO two-electron integrals (pq|rs) packed with 8-fold symmetry,
 the MO dipole integrals, E(SCF) and the nuclear repulsion energy.
 
-The SCF energies must reproduce the reference's SCFENEG records; the script
-asserts that.
+Where the reference prints them, the SCF and nuclear repulsion energies must
+reproduce its records; the script asserts that.
 """
 from __future__ import annotations
 
@@ -34,10 +43,17 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from _gto import BOHR_ANGSTROM, Basis  # noqa: E402
 
 GEOMS = {
-    # tag: (R angstrom, angle deg, golden SCF energy, golden nuclear repulsion)
-    "zmat035": (0.957, 104.5, -76.0465033211, 9.19693438045),   # test/zmat.035.ccsd TEST.DAT
-    "zmat020": (1.0, 104.0, -76.0407105174, 8.80260376799),     # test/zmat.020 TEST.DAT
-    "zmat026": (0.96, 104.0, -76.0462837076, 9.16937892499),    # test/zmat.026 TEST.DAT
+    # tag: (R angstrom, angle deg, golden SCF energy, golden nuclear repulsion,
+    #       GENBAS basis name, spherical d, number of basis functions, file)
+    "zmat035": (0.957, 104.5, -76.0465033211, 9.19693438045,    # test/zmat.035.ccsd TEST.DAT
+                "DZP", False, 26, "h2o_dzp_zmat035.npz"),
+    "zmat020": (1.0, 104.0, -76.0407105174, 8.80260376799,      # test/zmat.020 TEST.DAT
+                "DZP", False, 26, "h2o_dzp_zmat020.npz"),
+    "zmat026": (0.96, 104.0, -76.0462837076, 9.16937892499,     # test/zmat.026 TEST.DAT
+                "DZP", False, 26, "h2o_dzp_zmat026.npz"),
+    "zmat046": (0.95720197, 104.52, -76.046493464757, 9.1949465922,  # out.zmat.046:339,605
+                "DZP", False, 26, "h2o_dzp_zmat046.npz"),
+    "ccpvdz": (0.9572, 104.52, None, None, "CC-PVDZ", True, 24, "h2o_ccpvdz.npz"),
 }
 
 
@@ -182,15 +198,15 @@ def pack8(g):
 
 
 def build(ref_root, tag):
-    R, A, e_scf_gold, enuc_gold = GEOMS[tag]
+    R, A, e_scf_gold, enuc_gold, bname, spherical, nbf, fname = GEOMS[tag]
     genbas = os.path.join(ref_root, "test", "KEEP", "GENBAS")
     atoms = geometry(R, A)
     shells = []
     for sym, Z, xyz in atoms:
-        for l, exps, coefs in read_genbas(genbas, f"{sym}:DZP"):
+        for l, exps, coefs in read_genbas(genbas, f"{sym}:{bname}"):
             shells.append((xyz, l, exps, coefs))
-    basis = Basis(shells)
-    assert basis.nao == 26, basis.nao
+    basis = Basis(shells, spherical=spherical)
+    assert basis.nao == nbf, basis.nao
     S, T, V, Mu = basis.one_electron([a[1] for a in atoms], [a[2] for a in atoms])
     G = basis.eri()
     enuc = nuclear_repulsion(atoms)
@@ -198,8 +214,10 @@ def build(ref_root, tag):
     E_el, eps, C = rhf(S, T + V, G, nocc)
     E_scf = E_el + enuc
     print(f"{tag}: Enuc={enuc:.11f} (golden {enuc_gold}) E_SCF={E_scf:.10f} (golden {e_scf_gold})")
-    assert abs(enuc - enuc_gold) < 1e-9
-    assert abs(E_scf - e_scf_gold) < 2e-10, E_scf - e_scf_gold
+    if enuc_gold is not None:
+        assert abs(enuc - enuc_gold) < 1e-9
+    if e_scf_gold is not None:
+        assert abs(E_scf - e_scf_gold) < 2e-10, E_scf - e_scf_gold
     irr = classify_irreps(basis, C, S)
     # reference DPD ordering: occupied by irrep, virtual by irrep, energy order within
     occ = [k for h in range(4) for k in range(nocc) if irr[k] == h]
@@ -217,7 +235,7 @@ def build(ref_root, tag):
     nucdip = sum(a[1] * a[2] for a in atoms)
     h_mo = C.T @ (T + V) @ C
     np.savez_compressed(
-        os.path.join(os.path.dirname(os.path.abspath(__file__)), f"h2o_dzp_{tag}.npz"),
+        os.path.join(os.path.dirname(os.path.abspath(__file__)), fname),
         eps=eps, irrep=irr, pop=pop, vrt=vrt, eri8=pack8(g), nmo=basis.nao,
         dipole=mu_mo, nucdip=nucdip, hcore=h_mo, e_scf=E_scf, e_nuc=enuc,
         charges=charges,
@@ -226,7 +244,9 @@ def build(ref_root, tag):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: make_h2o_dzp.py <reference root> [tag ...]")
+    ref = sys.argv[1]
     tags = sys.argv[2:] or list(GEOMS)
     for tag in tags:
         build(ref, tag)

@@ -87,6 +87,31 @@ def test_bad_arguments_return_status(lib):
     assert lib.h.aces_getlst(None, 1, 1, 9, 1) < 0
 
 
+@pytest.mark.parametrize("fn", ["aces_xgemm", "aces_xgemm_static"])
+def test_xgemm_rejects_short_leading_dimensions(lib, fn):
+    """DGEMM's argument checks (tools/xgemm.F passes them to DGEMM): lda below
+    the rows of A as stored (m for 'N', k for 'T'), ldb below the rows of B
+    (k for 'N', n for 'T') and ldc < m are refused before any device work, so
+    this runs without a GPU; the pointers are never dereferenced."""
+    f = getattr(lib.h, fn)
+    extra = (ab.PREC_FP64,) if fn == "aces_xgemm" else ()
+    m, n, k = 7, 5, 3
+    bad = [  # transa, transb, lda, ldb, ldc
+        (b"N", b"N", m - 1, k, m), (b"T", b"N", k - 1, k, m),
+        (b"N", b"N", m, k - 1, m), (b"N", b"T", m, n - 1, m), (b"N", b"N", m, k, m - 1),
+    ]
+    for ta, tb, lda, ldb, ldc in bad:
+        st = f(ta, tb, m, n, k, 1.0, None, lda, None, ldb, 0.0, None, ldc, *extra)
+        assert st == -1, (ta, tb, lda, ldb, ldc)
+    # m*n == 0: quick return before any check of the operands
+    assert f(b"N", b"N", 0, n, k, 1.0, None, 1, None, k, 0.0, None, 1, *extra) == 0
+
+
+def test_pool_stats_is_callable_without_a_gpu(lib):
+    calls, mallocs, cached = lib.pool_stats()
+    assert calls >= 0 and mallocs >= 0 and cached >= 0 and mallocs <= calls
+
+
 def test_header_is_c99_and_config_layout_matches_ctypes(tmp_path):
     """include/aces_b200.h compiles as C99 (a Fortran/C host includes it as
     is), and the aces_cc_config layout a C compiler gives (size and every

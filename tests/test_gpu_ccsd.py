@@ -135,6 +135,41 @@ def test_ccsd_h2o_dzp_026_matches_reference(lib):
     assert abs(ham.e_scf + cfg.e_ccsd - (-76.272545457483)) < 1e-10
 
 
+def test_ccsd_config1_geometry_dzp_matches_reference(lib):
+    """The benchmark geometry (0.9572 A, 104.52 deg) in the reference's DZP
+    basis (test/zmat.046): the converged CCSD energy of out.zmat.046:745,
+    which the reference reached at a residual of 1.9e-8 (hence 5e-9 Eh), and
+    the oracle's at CC_CONV 10 to 1e-11."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat046.npz"))
+    setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=10, cc_maxcyc=60, cc_exporder=5)
+    ref = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
+    assert cfg.converged == 1 and cfg.ncycle == ref["ncycle"]
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+    assert abs(cfg.e_ccsd - (-0.226017627669)) < 5e-9
+
+
+@pytest.mark.parametrize("prec", [ab.PREC_FP64, ab.PREC_BF16X3])
+def test_ccsd_config1_h2o_ccpvdz(lib, prec):
+    """Config 1: plain RHF-CCSD of H2O (0.9572 A, 104.52 deg) in cc-pVDZ, 24
+    basis functions, C2v, 5 occupied / 19 virtual, converged to a residual of
+    1e-10 (CC_CONV 10).  The FP64 engine matches the oracle to 1e-11 Eh (the
+    bar is 1e-9) with the same number of cycles and the same amplitudes; the
+    split-precision request gives the same answer, since no product of this
+    system reaches the tensor-core size thresholds (it is the FP64 path)."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_ccpvdz.npz"))
+    B, dpd = setup_lists(lib, ham)
+    assert sum(lib.vrt) == 19 and sum(lib.pop) == 5 and lib.nirrep == 4
+    cfg = lib.xvcc(cc_conv=10, cc_maxcyc=60, cc_exporder=5, precision=prec)
+    ref = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
+    assert cfg.converged == 1 and cfg.ncycle == ref["ncycle"]
+    assert abs(cfg.last_residual) < 1e-10
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+    t1, t2 = read_amplitudes(lib, dpd, ham.nocc, ham.nvir)
+    np.testing.assert_allclose(t2, ref["t2"], atol=1e-12)
+    np.testing.assert_allclose(t1, ref["t1"], atol=1e-12)
+
+
 @pytest.mark.parametrize("o,v,naux,seed", [(6, 24, 40, 5), (9, 41, 60, 11)])
 def test_ccsd_synthetic_c1_matches_oracle(lib, o, v, naux, seed):
     ham = synthetic(o, v, naux, seed)

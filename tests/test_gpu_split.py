@@ -55,6 +55,37 @@ def test_xgemm_bf16x3_error_bound(lib, m, n, k, ta, tb, beta):
     assert (err / (bound + 1e-30)).max().item() < 2e-5
 
 
+# Long contractions: the FP32 accumulation chunk shortens with K (512 K
+# elements up to K = 36864, 256 up to 73728, 128 beyond), the lengths of the
+# particle-particle contractions at o = 30, v = 270 (K = v^2 = 72900).  These
+# two shapes run the 256- and 128-element chunks (with split K: 4 output tiles).
+@pytest.mark.parametrize("k", [40000, 80000])
+@pytest.mark.parametrize("ta,tb", [("T", "N"), ("N", "T")])
+def test_xgemm_bf16x3_long_k_chunks(lib, k, ta, tb):
+    import torch
+    m = n = 256
+    g = torch.Generator(device="cpu").manual_seed(k + (ta == "T"))
+    A = torch.randn((m, k) if ta == "N" else (k, m), generator=g, dtype=torch.float64)
+    B = torch.randn((k, n) if tb == "N" else (n, k), generator=g, dtype=torch.float64)
+    A = A * torch.exp(torch.randn(A.shape, generator=g, dtype=torch.float64))
+    Cm = torch.randn((m, n), generator=g, dtype=torch.float64)
+    opA = A if ta == "N" else A.T
+    opB = B if tb == "N" else B.T
+    ref = 0.8 * opA @ opB + 1.0 * Cm
+    bound = 0.8 * opA.abs() @ opB.abs()
+    dA = A.T.contiguous().cuda()
+    dB = B.T.contiguous().cuda()
+    dC = Cm.T.contiguous().cuda()
+    lib.xgemm(ta, tb, m, n, k, 0.8, dA.data_ptr(), A.shape[0], dB.data_ptr(), B.shape[0], 1.0,
+              dC.data_ptr(), m, precision=ab.PREC_BF16X3)
+    out = dC.cpu().T
+    err = (out - ref).abs()
+    assert torch.all(err <= 4e-5 * bound + 1e-12), (err / (bound + 1e-30)).max().item()
+    # the FP32 partial sums of a chunk do not drift: the error relative to the
+    # bound stays at the size of a single split product's
+    assert (err / (bound + 1e-30)).max().item() < 2e-5
+
+
 def test_ccsd_bf16x3_energy_within_1e6(lib):
     ham = synthetic(10, 90, 120, seed=2)
     setup_lists(lib, ham)

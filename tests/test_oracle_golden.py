@@ -189,3 +189,45 @@ def test_ccsd_026_matches_reference():
     assert abs(h["e_final"] - (-0.226261749882)) < 1e-10
     assert abs(np.linalg.norm(h["t1"]) - 0.0193257962) < 1e-9
     assert abs(np.linalg.norm(h["t2"]) - 0.2200706819) < 1e-9
+
+
+def test_ccsd_046_config1_geometry_matches_reference():
+    """The benchmark geometry (R = 0.9572 A, A = 104.52 deg) in the reference's
+    DZP basis with Cartesian d: test/zmat.046 runs it as a UHF-CCSD, whose
+    closed-shell solution is the RHF one.  Pinned: nuclear repulsion and SCF
+    (out.zmat.046:339,605), MP2 pieces and T2AB norm (:604-608,638), the first
+    CC iteration (the same Jacobi step from MP2 in either spin formalism:
+    energy and largest residual element, :685-691) and the converged CCSD
+    energy (:745; the reference stops at a residual of 1.9e-8, so 5e-9 Eh).
+    Iterations 2 onwards differ by design: the UHF DIIS vector weights the
+    spin blocks differently from the RHF one (vcc/dodiis0.F)."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat046.npz"))
+    assert abs(ham.e_nuc - 9.1949465922) < 1e-9
+    assert abs(ham.e_scf - (-76.046493464757)) < 2e-10
+    B = ccsd.Blocks(ham)
+    t1, t2 = ccsd.mp2_guess(B)
+    eaa, eab, etot = ccsd.energy(B, t1, t2)
+    assert abs(eaa - (-0.025967355589)) < 1e-10 and abs(eab - (-0.165019405916)) < 1e-10
+    assert abs(etot - (-0.216954117095)) < 1e-10
+    assert abs(np.linalg.norm(t2) - 0.1983798481) < 1e-9
+    h = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
+    assert h["converged"]
+    assert abs(h["energies"][1] - (-0.221404651273)) < 1e-10
+    assert abs(abs(h["res"][0]) - 0.80627031e-02) < 2e-7 * 0.80627031e-02
+    assert abs(h["e_final"] - (-0.226017627669)) < 5e-9
+
+
+def test_ccpvdz_config1_fixture():
+    """Config 1 (H2O, 0.9572 A / 104.52 deg, cc-pVDZ with spherical d): 24
+    basis functions, 5 occupied / 19 virtual, C2v populations; the oracle's
+    CCSD converges to max|dT| < 1e-10.  No reference output exists for this
+    basis; the fixture's SCF is checked for self-consistency (occupied orbitals
+    below the virtual ones, Brillouin: the converged Fock matrix is diagonal)."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_ccpvdz.npz"))
+    assert ham.nmo == 24 and ham.nocc == 5 and ham.nvir == 19
+    pop, vrt = ham.pop_vrt()
+    assert list(pop) == [3, 1, 1, 0] and sum(vrt) == 19
+    assert ham.eps[:5].max() < ham.eps[5:].min()
+    h = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
+    assert h["converged"]
+    assert -0.22 < h["e_final"] < -0.19
