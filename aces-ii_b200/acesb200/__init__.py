@@ -36,8 +36,9 @@ SYMBOLS = [
     "aces_isymoff", "aces_dirprd", "aces_list_touch", "aces_updmoi", "aces_inipck",
     "aces_isytyp", "aces_list_dims", "aces_getlst", "aces_putlst", "aces_getlst_dev",
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
+    "aces_intprc_df",
     "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
-    "xvcc_run", "xlambda_run", "xdens_1pdm",
+    "aces_set_wait_limit", "aces_debug_inject", "xvcc_run", "xlambda_run", "xdens_1pdm",
 ]
 
 
@@ -53,6 +54,7 @@ class CCConfig(C.Structure):
         ("seconds_ladder", C.c_double), ("flops_per_iter", C.c_double),
         ("launches_per_iter", C.c_longlong), ("seconds_setup", C.c_double),
         ("triples_rank", C.c_int), ("triples_nranks", C.c_int),
+        ("damp", C.c_double), ("tguess", C.c_int),
     ]
 
 
@@ -178,6 +180,25 @@ class Lib:
         a = np.ascontiguousarray(vec, dtype=np.float64)
         self._chk("aces_putall", self.h.aces_putall(a.ctypes.data, a.size, irrepx, lst))
 
+    def intprc_df(self, B, naux=None, on_device=None):
+        """Lists 13, 10, 16, 25, 30, 233 from MO factors B[L, p, q] (DPD orbital
+        order) built on the device (aces_intprc_df).  ``B`` is a numpy array
+        (host), a torch tensor (host or CUDA) or a raw device pointer with
+        ``naux`` given."""
+        if isinstance(B, int):
+            if naux is None:
+                raise ValueError("naux is required with a raw pointer")
+            ptr, dev = B, 1 if on_device is None else int(on_device)
+        elif isinstance(B, np.ndarray):
+            B = np.ascontiguousarray(B, dtype=np.float64)
+            self._keep = B
+            ptr, dev, naux = B.ctypes.data, 0, B.shape[0]
+        else:   # torch tensor
+            if not B.is_contiguous() or str(B.dtype) != "torch.float64":
+                raise ValueError("B must be a contiguous float64 tensor")
+            ptr, dev, naux = B.data_ptr(), int(B.is_cuda), B.shape[0]
+        self._chk("aces_intprc_df", self.h.aces_intprc_df(C.c_void_p(ptr), int(naux), dev))
+
     # ---- records ------------------------------------------------------------------
     def putrec(self, label, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64)
@@ -204,6 +225,14 @@ class Lib:
                   self.h.aces_xgemm_static(transa.encode(), transb.encode(), m, n, k, alpha,
                                            A_ptr, lda, B_ptr, ldb, beta, C_ptr, ldc))
 
+    def set_wait_limit(self, seconds):
+        """Bound of the tensor-core kernels' device-side waits (aces_set_wait_limit)."""
+        self._chk("aces_set_wait_limit", self.h.aces_set_wait_limit(C.c_double(seconds)))
+
+    def debug_inject(self, mode):
+        """Test hook: 1 = the tensor-core producer issues no copies (aces_debug_inject)."""
+        self._chk("aces_debug_inject", self.h.aces_debug_inject(mode))
+
     # ---- programs -----------------------------------------------------------------
     def _run(self, fn, cfg, allow_noconv=False):
         st = getattr(self.h, fn)(C.byref(cfg))
@@ -213,11 +242,11 @@ class Lib:
 
     def xvcc(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, triples=0,
              use_graph=0, verbose=0, allow_noconv=False, timing_warmup=0, triples_rank=0,
-             triples_nranks=1):
+             triples_nranks=1, damp=1.0, tguess=0):
         cfg = CCConfig(cc_conv=cc_conv, cc_maxcyc=cc_maxcyc, cc_exporder=cc_exporder,
                        precision=precision, triples=triples, use_graph=use_graph,
                        verbose=verbose, timing_warmup=timing_warmup, triples_rank=triples_rank,
-                       triples_nranks=triples_nranks)
+                       triples_nranks=triples_nranks, damp=damp, tguess=tguess)
         return self._run("xvcc_run", cfg, allow_noconv)
 
     def xlambda(self, cc_conv=7, cc_maxcyc=50, cc_exporder=5, precision=PREC_FP64, verbose=0,

@@ -285,25 +285,19 @@ void pair_table(const SymInfo &s, int type, const std::vector<int> &irr_p,
     }
 }
 
-struct DevMap {
-  int *d_rowidx = nullptr, *d_colidx = nullptr;
-  signed char *d_rowsgn = nullptr, *d_colsgn = nullptr;
-  int *d_irr[4] = {nullptr, nullptr, nullptr, nullptr};
-  double **d_base = nullptr;
-  int *d_nrows = nullptr;
-  DpdMap m;
-  ~DevMap() {
-    dev_free(d_rowidx); dev_free(d_colidx); dev_free(d_rowsgn); dev_free(d_colsgn);
-    for (int k = 0; k < 4; ++k) dev_free(d_irr[k]);
-    dev_free(d_base); dev_free(d_nrows);
-  }
-};
-
 template <class T>
 int upload(T **d, const std::vector<T> &h) {
   ACES_CUDA(dev_alloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T)));
   if (!h.empty()) ACES_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
   return ACES_OK;
+}
+
+}  // namespace
+
+DevMap::~DevMap() {
+  dev_free(d_rowidx); dev_free(d_colidx); dev_free(d_rowsgn); dev_free(d_colsgn);
+  for (int k = 0; k < 4; ++k) dev_free(d_irr[k]);
+  dev_free(d_base); dev_free(d_nrows);
 }
 
 int make_map(DevMap &dm, int list, int typeL, int typeR, const std::vector<int> &irr_o,
@@ -355,7 +349,6 @@ int make_map(DevMap &dm, int list, int typeL, int typeR, const std::vector<int> 
   dm.m.nr = (int)ir.size(); dm.m.ns = (int)is.size();
   return ACES_OK;
 }
-}  // namespace
 
 int CCEngine::load_from_lists() {
   State &stt = state();
@@ -592,6 +585,51 @@ int CCEngine::setup_intermediates() {
   ACES_CUDA(cudaStreamSynchronize(st));
   // tmp4 is no longer needed
   if (tmp4.p) { dev_free(tmp4.p); tmp4.p = nullptr; tmp4.n = 0; }
+  return ACES_OK;
+}
+
+int CCEngine::read_guess(bool *read) {
+  *read = false;
+  const SymInfo &s = state().sym;
+  // both lists present with this system's pair types, irrep by irrep
+  for (int h = 0; h < s.nirrep; ++h) {
+    int nc = 0, nr = 0;
+    if (aces_list_dims(h + 1, 46, &nc, &nr) != ACES_OK || nc != s.irpdpd[h][13] ||
+        nr != s.irpdpd[h][12]) {
+      cudaGetLastError();
+      return ACES_OK;
+    }
+  }
+  int nc9 = 0, nr9 = 0;
+  if (aces_list_dims(1, 90, &nc9, &nr9) != ACES_OK || nc9 < 1 || nr9 != s.irpdpd[0][8])
+    return ACES_OK;
+  const long long O = o, V = v;
+  // list 46 (13,14) -> dense [a,b,i,j] -> t2[i,j,a,b]
+  DBuf tmpb;
+  ACES_TRY(alloc(tmpb, O * O * V * V));
+  {
+    DevMap dm;
+    ACES_TRY(make_map(dm, 46, 13, 14, irr_o, irr_v, false));
+    launch_gather(tmpb.p, dm.m, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  ACES_TRY(perm(t2(), o, o, v, v, 0.0, {PT(tmpb.p, 1.0, O, 1, V * O * O, O * O)}));
+  // list 90 irrep 1: one column over the (a,i) pairs of type 9
+  std::vector<double> col((size_t)nr9), h1((size_t)o * v, 0.0);
+  ACES_TRY(aces_getlst(col.data(), 1, 1, 1, 90));
+  std::vector<int> lo(o), lv(v);
+  int cnt[8] = {0};
+  for (int i = 0; i < o; ++i) lo[i] = cnt[irr_o[i]]++;
+  for (int k = 0; k < 8; ++k) cnt[k] = 0;
+  for (int a = 0; a < v; ++a) lv[a] = cnt[irr_v[a]]++;
+  for (int i = 0; i < o; ++i)
+    for (int a = 0; a < v; ++a)
+      if (irr_o[i] == irr_v[a])
+        h1[(size_t)i * v + a] = col[pair_index(s, 9, irr_v[a], lv[a], irr_o[i], lo[i])];
+  ACES_CUDA(cudaMemcpyAsync(t1(), h1.data(), h1.size() * 8, cudaMemcpyHostToDevice, st));
+  ACES_CUDA(cudaStreamSynchronize(st));
+  dev_free(tmpb.p);
+  *read = true;
   return ACES_OK;
 }
 
@@ -870,6 +908,9 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
   if (!lambda) {
     ACES_TRY(residual_run());
     launch_newt(t2n(), Z2.p, t1n(), Z1.p, eo.p, ev.p, o, v, st);
+    // DAMP_CC_RESIDUAL after NEWT2 (vcc/vcc.F:1031-1033); the energy, the
+    // error vector and the next iterate are those of the damped amplitudes
+    if (damp != 1.0) launch_blend(Xn.p, X.p, damp, len, st);
     launch_energy(d, t2n(), t1n(), I_oovv.p, fov.p, o, v, scratch.p, st);
   } else {
     // Lambda: new multipliers = (dE/dT + (dZ/dT)^T lambda) / D
@@ -906,7 +947,8 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
   e3[0] = hd[1];  // E_AA (printed alpha-alpha part)
   e3[1] = hd[0];  // E_AB
   e3[2] = 2.0 * hd[1] + hd[0] + hd[2];
-  *res = hd[3];
+  // convergence on the undamped difference (vcc/dodiis0.F:93-97)
+  *res = (!lambda && damp != 1.0) ? hd[3] / damp : hd[3];
   if (Bh.size() != 625) Bh.assign(625, 0.0);
   for (int k = 0; k < ndimr; ++k) {
     Bh[k * 25 + idimr] = hd[8 + k];
@@ -1030,6 +1072,11 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
   CCEngine &E = *engine_instance(true);
   E.prec = cfg->precision;
   E.use_graph = cfg->use_graph != 0;
+  if (!(cfg->damp >= 0.0 && cfg->damp <= 1.0)) {
+    set_error("xvcc_run: damp %g outside [0, 1] (0 means no damping)", cfg->damp);
+    return ACES_ERR_ARG;
+  }
+  E.damp = cfg->damp == 0.0 ? 1.0 : cfg->damp;
   cudaEvent_t ev0, ev1;
   ACES_CUDA(cudaEventCreate(&ev0));
   ACES_CUDA(cudaEventCreate(&ev1));
@@ -1037,7 +1084,10 @@ extern "C" int xvcc_run(aces_cc_config *cfg) {
     auto t0 = std::chrono::steady_clock::now();
     ACES_TRY(E.load_from_lists());
     ACES_TRY(E.setup_intermediates());
-    ACES_TRY(E.mp2_guess());
+    bool read = false;
+    if (cfg->tguess) ACES_TRY(E.read_guess(&read));
+    if (!read) ACES_TRY(E.mp2_guess());
+    cfg->tguess = read ? 1 : 0;
     ACES_CUDA(cudaStreamSynchronize(E.st));
     cfg->seconds_setup =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

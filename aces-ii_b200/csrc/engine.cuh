@@ -25,6 +25,8 @@ class CCEngine {
  public:
   int o = 0, v = 0, nmo = 0;
   int prec = ACES_PREC_FP64;
+  // DAMP_CC (vcc/vcc.F:71): new amplitudes T_old + damp (T_new - T_old)
+  double damp = 1.0;
   cudaStream_t st = 0;
   bool nonhf = false;
   // residual pass captured in a CUDA graph (use_graph): captured on the second
@@ -124,6 +126,9 @@ class CCEngine {
   int load_from_lists();
   int setup_intermediates();
   int mp2_guess();
+  // TGUESS restart (vcc/drdtgss.F): T1 from list 90, T2 from list 46 when both
+  // exist with this system's dimensions; *read = false leaves X untouched
+  int read_guess(bool *read);
   int residual();   // Z1, Z2 from X
   int iteration(int icycle, int exporder, double *e_out3, double *res, double *dres,
                 bool *extrap, bool lambda = false);
@@ -142,6 +147,26 @@ class CCEngine {
 };
 
 constexpr long long kHugeView = 1LL << 62;  // CView divisor meaning "no split"
+
+// Device tables mapping the dense [p,q,r,s] index space of one DPD list onto
+// its irrep blocks (pair indices, signs, orbital irreps, block pointers).
+struct DevMap {
+  int *d_rowidx = nullptr, *d_colidx = nullptr;
+  signed char *d_rowsgn = nullptr, *d_colsgn = nullptr;
+  int *d_irr[4] = {nullptr, nullptr, nullptr, nullptr};
+  double **d_base = nullptr;
+  int *d_nrows = nullptr;
+  DpdMap m;
+  DevMap() = default;
+  DevMap(const DevMap &) = delete;
+  DevMap &operator=(const DevMap &) = delete;
+  ~DevMap();
+};
+// Tables of list `list` (row pair type typeL, column pair type typeR; with
+// create the list is first touched through INIPCK) for occupied / virtual
+// orbitals of the given irreps, in DPD order.
+int make_map(DevMap &dm, int list, int typeL, int typeR, const std::vector<int> &irr_o,
+             const std::vector<int> &irr_v, bool create);
 
 int accept_update(CCEngine &E, bool extrap, int ndimr, bool lambda);
 CCEngine *engine_instance(bool create);

@@ -132,6 +132,26 @@ struct GroupedProblem {
 int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha, double beta,
                            cudaStream_t st);
 
+// Batched products over row windows of shared parent operands: entry e
+// computes C_e = alpha sum_s A_s[rowA[s] + m, :] B_s[rowB[s] + n, :]^T
+// + beta C_e for m < M, n < N, with C_e = the view C shifted by coff
+// elements.  All entries share the parents' tensor maps; one launch walks the
+// tiles of every entry (the side with fewer tiles fastest, then the entry,
+// then the other side, so that entries sharing an operand window read it from
+// DRAM once).  With f32out the output is FP32 (beta 0 or 1 only).
+constexpr int kBatchSeg = 4;
+struct alignas(16) BatchEntry {   // 48 bytes: the kernel reads the rows as two int4
+  int rowA[kBatchSeg], rowB[kBatchSeg];
+  long long coff;
+};
+static_assert(sizeof(BatchEntry) == 48, "batch entry layout");
+// d_entries: device array of nbatch entries; h_entries: the same on the host
+// (checked: every window lies inside its parent)
+int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, int nseg, int M,
+                           int N, const BatchEntry *h_entries, const BatchEntry *d_entries,
+                           int nbatch, double alpha, double beta, const CView &C, bool f32out,
+                           cudaStream_t st);
+
 // Rows [row0, row0 + rows) of a split operand (no copy).  The view's tensor
 // map ends at the parent's padded rows; rows past the view inside it belong
 // to the next slice and only reach output rows that callers discard.
@@ -140,5 +160,9 @@ SplitOperand split_view(const SplitOperand &p, int row0, int rows);
 // Error code recorded by a tcgen05 kernel whose bounded wait expired (0 = ok);
 // reading it clears it.
 int tc_status_and_clear();
+// Bound (ns) of every mbarrier wait of the tcgen05 kernels on the current
+// device, and the test-only fault injection (producer issues no copies).
+int tc_set_wait_limit(unsigned long long ns);
+int tc_set_inject(int on);
 
 }  // namespace acesb200

@@ -134,7 +134,12 @@ constexpr int kThreads = 32 * (2 + kEpiWarps);
 #endif
 constexpr int kNAcc = ACES_TC_NACC;                   // TMEM accumulators in rotation
 constexpr int kTmemCols = kNAcc * TBN;
-constexpr unsigned long long kWaitNs = 4000000000ULL;  // 4 s bound on any wait
+// Bound on every mbarrier wait (ns), per device; aces_set_wait_limit changes it.
+__device__ unsigned long long g_tc_wait_ns = 4000000000ULL;
+// Fault injection for tests of the bounded waits (aces_debug_inject): when set,
+// the TMA producer issues no copies, so the MMA and epilogue waits run out,
+// the kernel records a status and returns with nothing in flight.
+__device__ int g_tc_inject = 0;
 
 __device__ int g_tc_status;
 
@@ -172,9 +177,9 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 // bounded wait: false on timeout
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   if (mbar_try(bar, parity)) return true;
-  unsigned long long t0 = gtimer();
+  const unsigned long long t0 = gtimer(), limit = g_tc_wait_ns;
   while (!mbar_try(bar, parity)) {
-    if (gtimer() - t0 > kWaitNs) return false;
+    if (gtimer() - t0 > limit) return false;
   }
   return true;
 }
@@ -255,6 +260,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // segments with their own tensor maps.  Tiles are numbered problem by
 // problem; within a problem as above.
 constexpr int kMaxSeg = 4, kMaxProb = 3;
+static_assert(kMaxSeg == kBatchSeg, "batch entries carry one row offset per segment");
 struct Problem {
   CView C;
   int M, N, tilesM, tilesN;
@@ -263,6 +269,11 @@ struct Problem {
   int mfast;             // tile order: m tile fastest (else n tile fastest)
   int nseg, chunk;
   int kt0[kMaxSeg + 1];  // segment s owns global k tiles [kt0[s], kt0[s+1])
+  // batched problem: nbatch entries (row windows of the parents, output
+  // offsets) in device memory, or nullptr
+  const BatchEntry *batch;
+  int nbatch;
+  int f32out;            // output elements are FP32
 };
 struct Launch {
   CUtensorMap ah[kMaxProb][kMaxSeg], al[kMaxProb][kMaxSeg];
@@ -271,7 +282,7 @@ struct Launch {
   int nprob, nTiles;
 };
 struct TileRef {
-  int g, m0, n0, z, ktb, kTiles;
+  int g, m0, n0, z, ktb, kTiles, b;
 };
 __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   TileRef r;
@@ -280,7 +291,22 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   const Problem &P = L.prob[r.g];
   const int tl = t - P.tile0;
   int tm, tn;
-  if (P.mfast) {
+  r.b = 0;
+  if (P.batch) {
+    // fewer-tiles side fastest, then the entry, then the other side
+    if (P.mfast) {
+      tm = tl % P.tilesM;
+      const int q = tl / P.tilesM;
+      r.b = q % P.nbatch;
+      tn = q / P.nbatch;
+    } else {
+      tn = tl % P.tilesN;
+      const int q = tl / P.tilesN;
+      r.b = q % P.nbatch;
+      tm = q / P.nbatch;
+    }
+    r.z = 0;
+  } else if (P.mfast) {
     tm = tl % P.tilesM;
     const int q = tl / P.tilesM;
     tn = q % P.tilesN;
@@ -342,11 +368,19 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int it = 0;  // k tiles issued by this CTA
-    bool stop = false;
+    bool stop = *(volatile int *)&g_tc_inject != 0;  // injected fault: issue nothing
     for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
       const TileRef T = decode_tile(L, t);
       const Problem &P = L.prob[T.g];
       const int m0 = T.m0, n0 = T.n0, ktb = T.ktb, kTiles = T.kTiles;
+      // row windows of a batched entry (one read per tile, 8 ints)
+      int rA[kMaxSeg] = {0, 0, 0, 0}, rB[kMaxSeg] = {0, 0, 0, 0};
+      if (P.batch) {
+        const int4 *e = reinterpret_cast<const int4 *>(P.batch + T.b);
+        const int4 a = __ldg(e), b = __ldg(e + 1);
+        rA[0] = a.x; rA[1] = a.y; rA[2] = a.z; rA[3] = a.w;
+        rB[0] = b.x; rB[1] = b.y; rB[2] = b.z; rB[3] = b.w;
+      }
       for (int kt = 0; kt < kTiles; ++kt) {
         const int s = it % STAGES;
         if (it >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((it / STAGES) - 1) & 1)) {
@@ -366,10 +400,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         int sg = 0;
         while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
         const int kx = (gk - P.kt0[sg]) * TBK;
-        tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, m0, fb);
-        tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, m0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, n0, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &L.bl[T.g][sg], kx, n0, fb);
+        int ya = m0, yb = n0;
+#pragma unroll
+        for (int q = 0; q < kMaxSeg; ++q)
+          if (q == sg) {
+            ya += rA[q];
+            yb += rB[q];
+          }
+        tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb);
+        tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, yb, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &L.bl[T.g][sg], kx, yb, fb);
         ++it;
       }
     }
@@ -474,14 +515,31 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int m = m0 + row;
       if (m >= M || ncol <= 0) continue;
       const int nb = n0 + half * kCols;
-      if (part) {
+      if (P.f32out) {
+        // FP32 output (batched (T) W): plain stores for beta = 0, one RED per
+        // element for beta = 1 (single owner, so it equals load + add + store)
+        float *const cm = reinterpret_cast<float *>(C.p) +
+                          (P.batch ? __ldg(&P.batch[T.b].coff) : 0LL) +
+                          cview_dim(C.mdiv, C.sm1, C.sm0, m);
+        CViewNWalk w(C, nb);
+        if (beta == 0.0) {
+#pragma unroll
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) cm[w.off] = (float)(alpha * acc[j]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) atomicAdd(cm + w.off, (float)(alpha * acc[j]));
+        }
+      } else if (part) {
         // split-K partial, [z][n][m]: lanes write consecutive m
         double *pz = part + (size_t)z * M * N + m;
 #pragma unroll
         for (int j = 0; j < kCols; ++j)
           if (j < ncol) pz[(size_t)(nb + j) * M] = acc[j];
       } else {
-        double *const cm = C.p + cview_dim(C.mdiv, C.sm1, C.sm0, m);
+        double *const cm = C.p + (P.batch ? __ldg(&P.batch[T.b].coff) : 0LL) +
+                           cview_dim(C.mdiv, C.sm1, C.sm0, m);
         CViewNWalk w(C, nb);
         if (beta == 0.0) {
 #pragma unroll
@@ -765,6 +823,49 @@ int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, d
   return gemm_nt_bf16x3_multi(&A, &B, 1, M, N, alpha, beta, C, st);
 }
 
+int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, int nseg, int M,
+                           int N, const BatchEntry *h_entries, const BatchEntry *d_entries,
+                           int nbatch, double alpha, double beta, const CView &C, bool f32out,
+                           cudaStream_t st) {
+  if (M <= 0 || N <= 0 || nbatch <= 0) return ACES_OK;
+  if (f32out && beta != 0.0 && beta != 1.0) {
+    set_error("gemm_nt_bf16x3_batched: FP32 output takes beta 0 or 1 (%g)", beta);
+    return ACES_ERR_ARG;
+  }
+  if (f32out && C.sm0 != 1) {
+    set_error("gemm_nt_bf16x3_batched: FP32 output needs unit m stride");
+    return ACES_ERR_ARG;
+  }
+  // every live row of every window inside its parent: the TMA coordinates of
+  // live rows stay in range, rows past a window read its neighbours (or the
+  // zero fill past the parent) and only reach discarded outputs
+  for (int e = 0; e < nbatch; ++e)
+    for (int s = 0; s < nseg; ++s) {
+      const BatchEntry &q = h_entries[e];
+      if (q.rowA[s] < 0 || (long long)q.rowA[s] + M > Apar[s].rows || q.rowB[s] < 0 ||
+          (long long)q.rowB[s] + N > Bpar[s].rows || q.coff < 0) {
+        set_error("gemm_nt_bf16x3_batched: entry %d segment %d outside its operands", e, s);
+        return ACES_ERR_ARG;
+      }
+    }
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.nprob = 1;
+  ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  Problem &P = L.prob[0];
+  P.batch = d_entries;
+  P.nbatch = nbatch;
+  P.f32out = f32out ? 1 : 0;
+  const long long tiles = (long long)P.tilesM * P.tilesN * nbatch;
+  if (tiles > (1LL << 31) - 1) {
+    set_error("gemm_nt_bf16x3_batched: %lld output tiles exceed the scheduler range", tiles);
+    return ACES_ERR_ARG;
+  }
+  P.tile0 = 0;
+  L.nTiles = (int)tiles;
+  return launch_prepared(L, alpha, beta, nullptr, st);
+}
+
 SplitOperand split_view(const SplitOperand &p, int row0, int rows) {
   SplitOperand v = p;
   size_t off = (size_t)row0 * p.k_pad * 2;
@@ -774,6 +875,16 @@ SplitOperand split_view(const SplitOperand &p, int row0, int rows) {
   v.rows_pad = std::min(rows, p.rows_pad - row0);  // beyond it the tensor map zero-fills
   v.cap = 0;
   return v;
+}
+
+int tc_set_wait_limit(unsigned long long ns) {
+  ACES_CUDA(cudaMemcpyToSymbol(g_tc_wait_ns, &ns, sizeof(ns)));
+  return ACES_OK;
+}
+
+int tc_set_inject(int on) {
+  ACES_CUDA(cudaMemcpyToSymbol(g_tc_inject, &on, sizeof(on)));
+  return ACES_OK;
 }
 
 int tc_status_and_clear() {

@@ -379,6 +379,20 @@ void launch_diff(double *e, const double *xnew, const double *xold, long long n,
   k_diff<<<(unsigned)nb, 256, 0, st>>>(e, xnew, xold, n); count_launch();
 }
 
+// xn = x + damp (xn - x), two loads and a store per element
+__global__ void k_blend(double *__restrict__ xn, const double *__restrict__ x, double damp,
+                        long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    xn[i] = fma(damp, xn[i] - x[i], x[i]);
+}
+
+void launch_blend(double *xn, const double *x, double damp, long long n, cudaStream_t st) {
+  long long nb = (n + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_blend<<<(unsigned)nb, 256, 0, st>>>(xn, x, damp, n); count_launch();
+}
+
 struct HistPtrs {
   const double *p[25];
 };
@@ -713,6 +727,34 @@ __global__ void k_scatter(const double *__restrict__ dense, DpdMap m, long long 
     if (m.rowsgn[p * m.nq + q] != 1 || m.colsgn[q2 * m.ns + s] != 1) continue;
     m.base[hrs][(long long)ci * m.nrows[hrs] + ri] = dense[idx];
   }
+}
+
+// The same scatter from X[r][p][s][q] (the row-major product of the
+// integral producer, m = (r,p), n = (s,q)), read in its own order so the loads
+// coalesce; every pair type involved stores all of its pairs (FULL).
+__global__ void k_scatter_rpsq(const double *__restrict__ X, DpdMap m, long long total) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long t = idx;
+    const int q = (int)(t % m.nq); t /= m.nq;
+    const int s = (int)(t % m.ns); t /= m.ns;
+    const int p = (int)(t % m.np);
+    const int r = (int)(t / m.np);
+    const int hpq = m.irr_p[p] ^ m.irr_q[q];
+    const int hrs = m.irr_r[r] ^ m.irr_s[s];
+    if (hpq != hrs) continue;
+    const int ri = m.rowidx[p * m.nq + q], ci = m.colidx[r * m.ns + s];
+    if (ri < 0 || ci < 0) continue;
+    m.base[hrs][(long long)ci * m.nrows[hrs] + ri] = X[idx];
+  }
+}
+
+void launch_scatter_rpsq(const double *X, const DpdMap &m, cudaStream_t st) {
+  long long total = (long long)m.np * m.nq * m.nr * m.ns;
+  long long nb = (total + 255) / 256;
+  if (nb > 148 * 32) nb = 148 * 32;
+  if (nb < 1) nb = 1;
+  k_scatter_rpsq<<<(unsigned)nb, 256, 0, st>>>(X, m, total); count_launch();
 }
 
 void launch_gather(double *dense, const DpdMap &m, cudaStream_t st) {

@@ -43,6 +43,8 @@ void launch_energy(double *out2, const double *t2, const double *t1, const doubl
 int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
                      int o, int v, double *scratch, cudaStream_t st);
 void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st);
+// DAMP_CC_RESIDUAL (vcc/damp_cc_residual.F): xn = x + damp (xn - x)
+void launch_blend(double *xn, const double *x, double damp, long long n, cudaStream_t st);
 // e = xnew - xold (T1 + T2 of a pair-symmetric vector) with, in the same pass,
 // absmax_out[0] = signed absmax (as launch_absmax) and dots_out[k] = <e, hist[k]>
 // (as launch_diis_dots; hist[self] is e); scratch holds >= 592 * 27 doubles
@@ -77,6 +79,9 @@ struct DpdMap {
 };
 void launch_gather(double *dense, const DpdMap &m, cudaStream_t st);
 void launch_scatter(const double *dense, const DpdMap &m, cudaStream_t st);
+// scatter of X[r][p][s][q] (p, q the row pair, r, s the column pair) into a
+// list of FULL pair types
+void launch_scatter_rpsq(const double *X, const DpdMap &m, cudaStream_t st);
 
 // packed particle-particle ladder (engine.cu, ladder_packed): pairs[2p], pairs[2p+1]
 // = (c, d) of the symmetric pair p (np = v(v+1)/2 of them) followed by the

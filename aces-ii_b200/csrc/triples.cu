@@ -15,6 +15,7 @@
 // reading every W element once per triplet.  Partial sums are kept per
 // (triplet, block) and reduced in a fixed order: the FP64 energy sum is
 // deterministic.
+#include <algorithm>
 #include <cmath>
 #include <functional>
 #include <vector>
@@ -103,11 +104,22 @@ __device__ __forceinline__ void decode_set(int n, int &a, int &b, int &c) {
 // {a >= b >= c}, all six orderings of the set read once; the distinct
 // orderings q of repeated virtuals are counted once.  Partial sums per block,
 // reduced in a fixed order.
+// Entry e = blockIdx.y of a batch: triplet trip3[3e..3e+2], its W at
+// Wbase + e * wstride (FP64, or FP32 for the split path), partial sums at
+// part[2 * (e * gridDim.x + blockIdx.x)].
+template <typename TW>
 __global__ void __launch_bounds__(256)
-    k_triples_energy(const double *__restrict__ W, const double *__restrict__ t1,
+    k_triples_energy(const TW *__restrict__ Wbase, long long wstride,
+                     const int *__restrict__ trip3, const double *__restrict__ t1,
                      const double *__restrict__ Ioovv, const double *__restrict__ eo,
-                     const double *__restrict__ ev, int i, int j, int k, int o, int v,
-                     double scale, double *__restrict__ part) {
+                     const double *__restrict__ ev, int o, int v, double *__restrict__ part) {
+  const int e = blockIdx.y;
+  const int i = trip3[3 * e], j = trip3[3 * e + 1], k = trip3[3 * e + 2];
+  const TW *__restrict__ W = Wbase + (long long)e * wstride;
+  // the distinct permutations of (i, j, k): 6 for distinct indices, 3 when
+  // two coincide, 1 when all three do
+  const int mult = (i == j && j == k) ? 6 : ((i == j || j == k) ? 2 : 1);
+  const double scale = 1.0 / (3.0 * mult);
   const long long v2 = (long long)v * v;
   const int nsets = v * (v + 1) * (v + 2) / 6;
   const double eijk = eo[i] + eo[j] + eo[k];
@@ -126,7 +138,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
       const int p0 = ordv[s][0], p1 = ordv[s][1], p2 = ordv[s][2];
-      u[s] = W[p0 * v2 + (long long)p1 * v + p2];
+      u[s] = (double)W[p0 * v2 + (long long)p1 * v + p2];
       // V - W at (p0,p1,p2): t_i^p0 <jk|p1p2> + t_j^p1 <ik|p0p2> + t_k^p2 <ij|p0p1>
       vd[s] = ti[p0] * Ijk[p1 * v + p2] + tj[p1] * Iik[p0 * v + p2] + tk[p2] * Iij[p0 * v + p1];
     }
@@ -152,8 +164,9 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0) {
     double a4 = 0.0, a5 = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a4 += sh[0][w]; a5 += sh[1][w]; }
-    part[2 * blockIdx.x] = scale * a4;
-    part[2 * blockIdx.x + 1] = scale * a5;
+    const long long slot = (long long)e * gridDim.x + blockIdx.x;
+    part[2 * slot] = scale * a4;
+    part[2 * slot + 1] = scale * a5;
   }
 }
 
@@ -191,7 +204,7 @@ __global__ void __launch_bounds__(1024) k_sum_pairs(double *out, const double *p
 // pair-side operands: class c (W index c on the t2/H side, pairs (a,b)),
 // class a (pairs (b,c), index a) and class b (pairs (a,c), index b).  All four
 // terms of a class share one output orientation, so each class is ONE
-// tensor-core launch with four K segments (2 x K = v, 2 x K = o); every
+// tensor-core product with four K segments (2 x K = v, 2 x K = o); every
 // output view has unit stride along m, the first class stores and the other
 // two accumulate with RED.  Per class and segment (P = permutation of (ijk)):
 //   class c:  t2[k,i] x Gv[j] (P4)   t2[k,j] x GvT[i] (P5)   -H[j,k] x t2P[i] (P0)   -H[i,k] x t2Q[j] (P2)
@@ -200,18 +213,29 @@ __global__ void __launch_bounds__(1024) k_sum_pairs(double *out, const double *p
 // with Gv[z][(b,c),d] = (bd|cz), GvT[z][(c,b),d] = Gv[z][(b,c),d],
 // t2P[x][(a,b),l] = t2[x,l,a,b], t2Q[x][(b,a),l] = t2[x,l,a,b] and
 // H[y,z][c,l] = (cz|yl).
+//
+// Split precision: the triplets run in batches.  Every operand of a class is a
+// row window of one of six pre-split parent arrays, so a batch's class is ONE
+// persistent tcgen05 launch over the tiles of all its triplets (the triplets'
+// windows in a device table, W in FP32 -- below the BF16x3 products' own
+// rounding), and one energy launch covers the batch.  The tile order (small
+// side, then triplet, then large side) makes the concurrently running CTAs
+// share the large operand's rows: a window used by several triplets of the
+// batch (Gv[j] for every k of a pair (i,j), Gv[k] across pairs) is read from
+// DRAM about once per launch instead of once per triplet.  Four launches per
+// batch replace four per triplet.  The FP64 path keeps one triplet at a time.
 int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nranks) {
   const long long O = o, V = v;
   const long long V2 = V * V, V3 = V * V * V;
   cudaEvent_t t0 = nullptr, t1e = nullptr;
-  DBuf Gv, GvT, t2P, t2Q, Hn, Wb, part, outp;
+  DBuf Gv, GvT, t2P, t2Q, Hn, Wb, part, outp, dtrip, dent;
   SplitOperand sT2, sGv, sGvT, sHn, sT2P, sT2Q;
   // every exit, the error returns included, gives back the scratch and events
   struct Release {
     std::function<void()> f;
     ~Release() { f(); }
   } release_scratch{[&] {
-    for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp}) {
+    for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q, &Hn, &Wb, &part, &outp, &dtrip, &dent}) {
       if (b->p) dev_free(b->p);
       b->p = nullptr;
     }
@@ -241,7 +265,6 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   // Hn[j,k,c,l] = -(ck|jl) = -I_ooov[l,k,j,c] (the second terms enter with a minus sign)
   ACES_TRY(alloc(Hn, O * O * O * V));
   ACES_TRY(perm(Hn.p, o, o, v, o, 0.0, {PermTerm{I_ooov.p, -1.0, {s3[2], s3[1], s3[3], s3[0]}}}));
-  ACES_TRY(alloc(Wb, V3));
   // triplets i >= j >= k of this shard: index t (i, then j <= i, then k <= j)
   // with t % nranks == rank
   std::vector<int> trip;
@@ -255,10 +278,18 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
           trip.push_back(k);
         }
   const int ntrip = (int)trip.size() / 3;
-  const int nblk = 148 * 4;
-  ACES_TRY(alloc(part, (size_t)ntrip * nblk * 2));
   ACES_TRY(alloc(outp, 2));
+  ACES_TRY(alloc(dtrip, (trip.size() + 1) / 2 + 1));
+  if (!trip.empty())
+    ACES_CUDA(cudaMemcpyAsync(dtrip.p, trip.data(), trip.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, st));
+  const int *d_trip = reinterpret_cast<const int *>(dtrip.p);
   const bool use_split = prec == ACES_PREC_BF16X3 && v >= 128;
+  const CView vc{nullptr, kHugeView, 0, 1, V, V2, V};   // m = c, n = (a,b)
+  const CView va{nullptr, V, V, 1, kHugeView, 0, V2};   // m = (b,c), n = a
+  const CView vb{nullptr, V, V2, 1, kHugeView, 0, V};   // m = (a,c), n = b
+  long long nparts = 0;
+
   if (use_split) {
     ACES_TRY(split_pack(sT2, t2(), V, o * o * v, v, st));       // rows (x,y,alpha), K = d
     ACES_TRY(split_pack(sGv, Gv.p, V, o * v * v, v, st));       // rows (z,beta,gamma), K = d
@@ -267,78 +298,124 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
     ACES_TRY(split_pack(sT2P, t2P.p, O, o * v * v, o, st));     // rows (x,alpha,beta), K = l
     ACES_TRY(split_pack(sT2Q, t2Q.p, O, o * v * v, o, st));     // rows (x,beta,alpha), K = l
     // the FP64 copies are not read again
+    ACES_CUDA(cudaStreamSynchronize(st));
     for (DBuf *b : {&Gv, &GvT, &t2P, &t2Q}) {
-      ACES_CUDA(cudaStreamSynchronize(st));
       dev_free(b->p);
       b->p = nullptr;
     }
-  }
-  // operand views: R = v rows of t2[x,y] or Hn[y,z]; Q = v^2 pair rows of Gv/GvT/t2P/t2Q[z]
-  struct Opd {
-    const SplitOperand *sp;
-    const double *p;
-    long long ld;
-    long long row0;
-    int rows;
-  };
-  auto T2r = [&](int x, int y) { return Opd{&sT2, t2(), V, ((long long)x * o + y) * V, v}; };
-  auto Hr = [&](int y, int z) { return Opd{&sHn, Hn.p, O, ((long long)y * o + z) * V, v}; };
-  auto Gq = [&](int z) { return Opd{&sGv, Gv.p, V, (long long)z * V2, v * v}; };
-  auto GTq = [&](int z) { return Opd{&sGvT, GvT.p, V, (long long)z * V2, v * v}; };
-  auto Pq = [&](int x) { return Opd{&sT2P, t2P.p, O, (long long)x * V2, v * v}; };
-  auto Qq = [&](int x) { return Opd{&sT2Q, t2Q.p, O, (long long)x * V2, v * v}; };
-  // one class: C(view) = beta C + sum_s A_s B_s^T
-  auto run_class = [&](const Opd (&A)[4], const Opd (&B)[4], int M, int N, const CView &cv,
-                       double beta) -> int {
-    if (use_split) {
-      SplitOperand a[4], b[4];
+    // batch size: FP32 W slots within a quarter of the free memory, <= 4 GB
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    const double slot = (double)V3 * sizeof(float);
+    const double budget = std::min(0.25 * (double)fr, 4.0e9);
+    const int nb = (int)std::max(1.0, std::min((double)std::max(ntrip, 1), budget / slot));
+    ACES_TRY(alloc(Wb, (size_t)((V3 * nb + 1) / 2)));  // FP32 slots in a double buffer
+    // one entry per triplet and class: the windows of the four segments
+    auto T2r = [&](int x, int y) { return (x * o + y) * v; };   // rows of sT2 / sHn
+    auto Pr = [&](int z) { return z * v * v; };                  // rows of sGv/sGvT/sT2P/sT2Q
+    std::vector<BatchEntry> ent((size_t)3 * ntrip);
+    for (int t = 0; t < ntrip; ++t) {
+      const int i = trip[3 * t], j = trip[3 * t + 1], k = trip[3 * t + 2];
+      const long long coff = (long long)(t % nb) * V3;
+      BatchEntry &c = ent[(size_t)3 * t], &a = ent[(size_t)3 * t + 1],
+                 &b = ent[(size_t)3 * t + 2];
+      c = BatchEntry{{T2r(k, i), T2r(k, j), T2r(j, k), T2r(i, k)},
+                     {Pr(j), Pr(i), Pr(i), Pr(j)}, coff};
+      a = BatchEntry{{Pr(k), Pr(j), Pr(j), Pr(k)},
+                     {T2r(i, j), T2r(i, k), T2r(k, i), T2r(j, i)}, coff};
+      b = BatchEntry{{Pr(k), Pr(i), Pr(i), Pr(k)},
+                     {T2r(j, i), T2r(j, k), T2r(k, j), T2r(i, j)}, coff};
+    }
+    // entries of class q for triplets [t0, t0 + n) stored contiguously:
+    // [class][triplet] on the device
+    std::vector<BatchEntry> byclass((size_t)3 * ntrip);
+    for (int q = 0; q < 3; ++q)
+      for (int t = 0; t < ntrip; ++t) byclass[(size_t)q * ntrip + t] = ent[(size_t)3 * t + q];
+    ACES_TRY(alloc(dent, (byclass.size() * sizeof(BatchEntry) + 7) / 8 + 1));
+    if (!byclass.empty())
+      ACES_CUDA(cudaMemcpyAsync(dent.p, byclass.data(), byclass.size() * sizeof(BatchEntry),
+                                cudaMemcpyHostToDevice, st));
+    const BatchEntry *d_ent = reinterpret_cast<const BatchEntry *>(dent.p);
+    const SplitOperand Ac[4] = {sT2, sT2, sHn, sHn}, Bc[4] = {sGv, sGvT, sT2P, sT2Q};
+    const SplitOperand Aa[4] = {sGv, sGvT, sT2P, sT2Q}, Ba[4] = {sT2, sT2, sHn, sHn};
+    const int nblk = 64;
+    ACES_TRY(alloc(part, (size_t)std::max(ntrip, 1) * nblk * 2));
+    for (int t0b = 0; t0b < ntrip; t0b += nb) {
+      const int n = std::min(nb, ntrip - t0b);
+      CView cv = vc;
+      cv.p = Wb.p;
+      ACES_TRY(gemm_nt_bf16x3_batched(Ac, Bc, 4, v, v * v, &byclass[(size_t)t0b],
+                                      d_ent + t0b, n, 1.0, 0.0, cv, true, st));
+      cv = va;
+      cv.p = Wb.p;
+      ACES_TRY(gemm_nt_bf16x3_batched(Aa, Ba, 4, v * v, v, &byclass[(size_t)ntrip + t0b],
+                                      d_ent + ntrip + t0b, n, 1.0, 1.0, cv, true, st));
+      cv = vb;
+      cv.p = Wb.p;
+      ACES_TRY(gemm_nt_bf16x3_batched(Aa, Ba, 4, v * v, v, &byclass[(size_t)2 * ntrip + t0b],
+                                      d_ent + 2 * ntrip + t0b, n, 1.0, 1.0, cv, true, st));
+      k_triples_energy<float><<<dim3(nblk, n), 256, 0, st>>>(
+          reinterpret_cast<const float *>(Wb.p), V3, d_trip + 3 * t0b, t1(), I_oovv.p, eo.p,
+          ev.p, o, v, part.p + (size_t)t0b * nblk * 2);
+      count_launch();
+      ACES_CUDA(cudaGetLastError());
+    }
+    nparts = (long long)ntrip * nblk;
+  } else {
+    // FP64: one triplet at a time, W in FP64
+    ACES_TRY(alloc(Wb, V3));
+    const int nblk = 148 * 4;
+    ACES_TRY(alloc(part, (size_t)std::max(ntrip, 1) * nblk * 2));
+    auto T2p = [&](int x, int y) { return t2() + ((long long)x * o + y) * V * V; };
+    auto Hp = [&](int y, int z) { return Hn.p + ((long long)y * o + z) * V * O; };
+    auto Gp = [&](int z) { return Gv.p + (long long)z * V2 * V; };
+    auto GTp = [&](int z) { return GvT.p + (long long)z * V2 * V; };
+    auto Pp = [&](int x) { return t2P.p + (long long)x * V2 * O; };
+    auto Qp = [&](int x) { return t2Q.p + (long long)x * V2 * O; };
+    // one class: C(view) = beta C + sum_s A_s B_s^T (K = v for the t2 x (bd|ck)
+    // segments, o for the others)
+    auto run_class = [&](const double *const (&A)[4], const double *const (&B)[4], int M, int N,
+                         const CView &cv, double beta) -> int {
       for (int g = 0; g < 4; ++g) {
-        a[g] = split_view(*A[g].sp, (int)A[g].row0, A[g].rows);
-        b[g] = split_view(*B[g].sp, (int)B[g].row0, B[g].rows);
+        const int K = g < 2 ? v : o;
+        ACES_TRY(gemm_nt_f64(M, N, K, 1.0, A[g], K, B[g], K, g == 0 ? beta : 1.0, cv, st));
       }
-      return gemm_nt_bf16x3_multi(a, b, 4, M, N, 1.0, beta, cv, st);
+      return ACES_OK;
+    };
+    for (int t = 0; t < ntrip; ++t) {
+      const int i = trip[3 * t], j = trip[3 * t + 1], k = trip[3 * t + 2];
+      CView cv = vc;
+      cv.p = Wb.p;
+      {
+        const double *const A[4] = {T2p(k, i), T2p(k, j), Hp(j, k), Hp(i, k)};
+        const double *const B[4] = {Gp(j), GTp(i), Pp(i), Qp(j)};
+        ACES_TRY(run_class(A, B, v, v * v, cv, 0.0));
+      }
+      cv = va;
+      cv.p = Wb.p;
+      {
+        const double *const A[4] = {Gp(k), GTp(j), Pp(j), Qp(k)};
+        const double *const B[4] = {T2p(i, j), T2p(i, k), Hp(k, i), Hp(j, i)};
+        ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
+      }
+      cv = vb;
+      cv.p = Wb.p;
+      {
+        const double *const A[4] = {Gp(k), GTp(i), Pp(i), Qp(k)};
+        const double *const B[4] = {T2p(j, i), T2p(j, k), Hp(k, j), Hp(i, j)};
+        ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
+      }
+      k_triples_energy<double><<<dim3(nblk, 1), 256, 0, st>>>(
+          Wb.p, 0, d_trip + 3 * t, t1(), I_oovv.p, eo.p, ev.p, o, v,
+          part.p + (size_t)t * nblk * 2);
+      count_launch();
     }
-    for (int g = 0; g < 4; ++g) {
-      const int K = A[g].ld == V ? v : o;
-      ACES_TRY(gemm_nt_f64(M, N, K, 1.0, A[g].p + A[g].row0 * A[g].ld, A[g].ld,
-                           B[g].p + B[g].row0 * B[g].ld, B[g].ld, g == 0 ? beta : 1.0, cv, st));
-    }
-    return ACES_OK;
-  };
-  const CView vc{nullptr, kHugeView, 0, 1, V, V2, V};   // m = c, n = (a,b)
-  const CView va{nullptr, V, V, 1, kHugeView, 0, V2};   // m = (b,c), n = a
-  const CView vb{nullptr, V, V2, 1, kHugeView, 0, V};   // m = (a,c), n = b
-  for (int t = 0; t < ntrip; ++t) {
-    const int i = trip[3 * t], j = trip[3 * t + 1], k = trip[3 * t + 2];
-    CView cv = vc;
-    cv.p = Wb.p;
-    {
-      const Opd A[4] = {T2r(k, i), T2r(k, j), Hr(j, k), Hr(i, k)};
-      const Opd B[4] = {Gq(j), GTq(i), Pq(i), Qq(j)};
-      ACES_TRY(run_class(A, B, v, v * v, cv, 0.0));
-    }
-    cv = va;
-    cv.p = Wb.p;
-    {
-      const Opd A[4] = {Gq(k), GTq(j), Pq(j), Qq(k)};
-      const Opd B[4] = {T2r(i, j), T2r(i, k), Hr(k, i), Hr(j, i)};
-      ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
-    }
-    cv = vb;
-    cv.p = Wb.p;
-    {
-      const Opd A[4] = {Gq(k), GTq(i), Pq(i), Qq(k)};
-      const Opd B[4] = {T2r(j, i), T2r(j, k), Hr(k, j), Hr(i, j)};
-      ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
-    }
-    int mult = 1;
-    if (i == j && j == k) mult = 6;
-    else if (i == j || j == k) mult = 2;
-    k_triples_energy<<<nblk, 256, 0, st>>>(Wb.p, t1(), I_oovv.p, eo.p, ev.p, i, j, k, o, v,
-                                           1.0 / (3.0 * mult), part.p + (size_t)t * nblk * 2);
-    count_launch();
+    nparts = (long long)ntrip * nblk;
   }
-  k_sum_pairs<<<1, 1024, 0, st>>>(outp.p, part.p, (long long)ntrip * nblk);
+  k_sum_pairs<<<1, 1024, 0, st>>>(outp.p, part.p, nparts);
   count_launch();
   double h[2];
   ACES_CUDA(cudaMemcpyAsync(h, outp.p, 16, cudaMemcpyDeviceToHost, st));

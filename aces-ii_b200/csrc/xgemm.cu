@@ -88,3 +88,19 @@ extern "C" int aces_xgemm(char transa, char transb, int m, int n, int k, double 
   }
   return status;
 }
+
+extern "C" int aces_set_wait_limit(double seconds) {
+  if (!(seconds > 0.0 && seconds <= 60.0)) {
+    set_error("aces_set_wait_limit: %g s outside (0, 60]", seconds);
+    return ACES_ERR_ARG;
+  }
+  return tc_set_wait_limit((unsigned long long)(seconds * 1e9));
+}
+
+extern "C" int aces_debug_inject(int mode) {
+  if (mode != 0 && mode != 1) {
+    set_error("aces_debug_inject: mode %d (0 or 1)", mode);
+    return ACES_ERR_ARG;
+  }
+  return tc_set_inject(mode);
+}

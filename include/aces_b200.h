@@ -113,6 +113,18 @@ int aces_list_memset(int irrep, int list, int byte);
 /* Device address of (irrep, list) column 1, or NULL. */
 double *aces_list_devptr(int irrep, int list);
 
+/* The integral lists the CC programs read, produced on the device (the
+ * reference's vtran + intprc chain, intprc/clmoio.F:46-260, for
+ * density-fitted or Cholesky-decomposed MO integrals): from the factors
+ * B[L][p][q] (naux x nmo x nmo doubles, C order, symmetric in p and q,
+ * orbitals in DPD order -- occupied by irrep, then virtual by irrep -- with
+ * (pq|rs) = sum_L B[L][p][q] B[L][r][s]) it creates lists 13 <Ij|Kl>,
+ * 10 <Ij|Ka>, 16 <Ab|Ij>, 25 <Ai|Bj>, 30 <Ab|Ci> and 233 <Ab|Cd> in every irrep
+ * (INIPCK) and fills them in FP64.  `B` is a device pointer when on_device is
+ * nonzero, else host memory copied in.  Requires aces_sym_init; the orbital
+ * energies (record SCFEVALA) are the caller's, as with PUTLST. */
+int aces_intprc_df(const double *B, int naux, int on_device);
+
 /* ---- records (JOBARC) --------------------------------------------------- */
 
 /* PUTREC / GETREC (acescore/putrec.F, acescore/getrec.F): named byte
@@ -146,6 +158,20 @@ int aces_xgemm(char transa, char transb, int m, int n, int k, double alpha, cons
 int aces_xgemm_static(char transa, char transb, int m, int n, int k, double alpha,
                       const double *A, int lda, const double *B, int ldb, double beta,
                       double *Cmat, int ldc);
+
+/* Bound on every device-side wait of the tensor-core contraction kernels on
+ * the current device (default 4 s; (0, 60] accepted).  A kernel whose wait
+ * runs out records it, waits (again bounded) for the copies and products it
+ * issued, releases its tensor memory and returns; the calling entry point
+ * then returns ACES_ERR_TIMEOUT.  No counterpart in the reference (its BLAS
+ * calls cannot stall on a device). */
+int aces_set_wait_limit(double seconds);
+/* Test hook for that path (no counterpart in the reference): mode 1 makes the
+ * copy-issuing thread of the tensor-core kernels on the current device issue
+ * nothing, so every product waits out the limit above and the call reports
+ * ACES_ERR_TIMEOUT with no copy or product in flight; mode 0 restores normal
+ * operation. */
+int aces_debug_inject(int mode);
 
 /* ---- member programs ---------------------------------------------------- */
 
@@ -191,6 +217,17 @@ typedef struct aces_cc_config {
    * shard's partial sums (add them over the ranks).  0 / 0 or 0 / 1: all. */
   int triples_rank;
   int triples_nranks;
+  /* DAMP_CC (vcc/vcc.F:71, IFLAGS2 damp_cc x 0.01; vcc/damp_cc_residual.F):
+   * after the denominator division the new amplitudes become
+   * T_old + damp (T_new - T_old); convergence is judged on the undamped
+   * difference (vcc/dodiis0.F:93-97).  0 or 1: no damping. */
+  double damp;
+  /* TGUESS restart (vcc/drdtgss.F): on input 1 starts from the amplitudes in
+   * lists 90 (T1) and 46 (T2, AB) -- a previous xvcc_run's output or the
+   * caller's -- instead of the MP2 guess, when both lists exist with this
+   * system's dimensions; on output 1 if they were read, 0 if the MP2 guess
+   * was used. */
+  int tguess;
 } aces_cc_config;
 
 /* PROGRAM VCC (vcc/vcc.F:9): RHF CCSD (and (T) when cfg->triples).  Reads

@@ -267,8 +267,17 @@ def symmetrize_t2(t2):
 
 
 def run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5, t_guess=None, log=None,
-             diis=True):
+             diis=True, damp=1.0):
     """The xvcc CC loop (vcc/vcc.F:797-1437) with DIIS (IFLAGS(21)=1).
+
+    ``damp`` is DAMP_CC (IFLAGS2 damp_cc x 0.01, vcc/vcc.F:71): after NEWT2
+    the new amplitudes become T_old + damp (T_new - T_old)
+    (vcc/damp_cc_residual.F, called vcc/vcc.F:1031-1033, on the pair-
+    symmetrised T2), the energy and the DIIS error vector are those of the
+    damped amplitudes, and convergence is judged on the undamped difference,
+    max |T_new - T_old|, i.e. the damped one divided by damp
+    (vcc/dodiis0.F:93-97,165).  ``t_guess`` (t1, t2) replaces the MP2 start
+    (the TGUESS restart, vcc/drdtgss.F).
 
     Returns a dict with the per-iteration energies (as printed by CMPENG on
     the new amplitudes), the residual and DIIS-residual maxima, the converged
@@ -285,6 +294,9 @@ def run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5, t_guess=None, log=None,
         n1, n2 = update(B, t1, t2)
         n2 = symmetrize_t2(n2)
         t2s = symmetrize_t2(t2)
+        if damp != 1.0:
+            n1 = t1 + damp * (n1 - t1)
+            n2 = t2s + damp * (n2 - t2s)
         eaa, eab, etot = energy(B, n1, n2)
         hist["energies"].append(etot); hist["e_aa"].append(eaa); hist["e_ab"].append(eab)
         if diis:
@@ -295,6 +307,8 @@ def run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5, t_guess=None, log=None,
             d = diis_vector(n1, n2) - diis_vector(t1, t2s)
             res = d[np.argmax(np.abs(d))]
             dres, ext = res, None
+        if damp != 1.0:
+            res = res / damp
         hist["res"].append(res); hist["dres"].append(dres)
         if log:
             log(f"iter {icycle:3d}  E = {etot:.12f}  res = {res: .8e}  dres = {dres: .8e}")

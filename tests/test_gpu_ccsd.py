@@ -201,6 +201,45 @@ def test_ccsd_non_hartree_fock_fock_matches_oracle(lib):
     assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
 
 
+def test_ccsd_damping_matches_oracle(lib):
+    """DAMP_CC (vcc/damp_cc_residual.F): the same cycles, energies and
+    converged amplitudes as the oracle's damped loop."""
+    ham = synthetic(5, 20, 30, seed=21)
+    B, dpd = setup_lists(lib, ham)
+    cfg = lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, damp=0.7)
+    ref = ccsd.run_ccsd(ham, cc_conv=9, maxcyc=80, exporder=5, damp=0.7)
+    plain = ccsd.run_ccsd(ham, cc_conv=9, maxcyc=80, exporder=5)
+    assert cfg.converged == 1 and cfg.ncycle == ref["ncycle"] != plain["ncycle"]
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-11
+    t1, t2 = read_amplitudes(lib, dpd, ham.nocc, ham.nvir)
+    np.testing.assert_allclose(t2, ref["t2"], atol=1e-11)
+    with pytest.raises(ab.AcesError):
+        lib.xvcc(cc_conv=9, cc_maxcyc=80, damp=1.5)
+
+
+def test_tguess_restart_continues_a_run(lib):
+    """TGUESS (vcc/drdtgss.F): a run stopped after 4 cycles leaves its
+    amplitudes in lists 90/46; a second run started from them (fresh DIIS
+    history) follows the oracle's restart cycle for cycle and reaches the
+    golden energy; without the lists it falls back to the MP2 guess."""
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat035.npz"))
+    setup_lists(lib, ham)
+    first = lib.xvcc(cc_conv=7, cc_maxcyc=4, cc_exporder=5, allow_noconv=True)
+    assert first.converged == 0 and first.tguess == 0
+    again = lib.xvcc(cc_conv=7, cc_maxcyc=50, cc_exporder=5, tguess=1)
+    part = ccsd.run_ccsd(ham, cc_conv=7, maxcyc=4, exporder=5)
+    ref = ccsd.run_ccsd(ham, cc_conv=7, maxcyc=50, exporder=5, t_guess=(part["t1"], part["t2"]))
+    assert again.tguess == 1 and again.converged == 1 and again.ncycle == ref["ncycle"]
+    assert abs(again.e_ccsd - ref["e_final"]) < 1e-11
+    assert abs(again.e_ccsd - (-0.226005606663)) < 1e-7   # both converged to 1e-7
+    # restarting from converged amplitudes: converged at the first cycle
+    done = lib.xvcc(cc_conv=7, cc_maxcyc=50, cc_exporder=5, tguess=1)
+    assert done.tguess == 1 and done.ncycle == 1
+    setup_lists(lib, ham)            # aces_init: no amplitude lists any more
+    fresh = lib.xvcc(cc_conv=7, cc_maxcyc=50, cc_exporder=5, tguess=1)
+    assert fresh.tguess == 0 and fresh.ncycle == 11
+
+
 def test_ccsd_errors_are_status_codes(lib):
     lib.init(0)
     lib.sym_init([2], [5])
