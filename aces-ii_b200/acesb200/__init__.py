@@ -39,6 +39,7 @@ SYMBOLS = [
     "aces_intprc_df",
     "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
     "aces_set_wait_limit", "aces_debug_inject", "xvcc_run", "xlambda_run", "xdens_1pdm",
+    "xvee_run",
 ]
 
 
@@ -55,6 +56,16 @@ class CCConfig(C.Structure):
         ("launches_per_iter", C.c_longlong), ("seconds_setup", C.c_double),
         ("triples_rank", C.c_int), ("triples_nranks", C.c_int),
         ("damp", C.c_double), ("tguess", C.c_int),
+    ]
+
+
+class EOMConfig(C.Structure):
+    """aces_eom_config (include/aces_b200.h)."""
+    _fields_ = [
+        ("nroots", C.c_int * 8), ("eom_conv", C.c_int), ("eom_maxcyc", C.c_int),
+        ("max_subspace", C.c_int), ("precision", C.c_int), ("verbose", C.c_int),
+        ("omega", (C.c_double * 8) * 8), ("converged", C.c_int * 8), ("niter", C.c_int * 8),
+        ("nsigma", C.c_int), ("seconds", C.c_double),
     ]
 
 
@@ -98,6 +109,7 @@ class Lib:
                                         C.c_double, C.c_void_p, C.c_int]
         for fn in ("xvcc_run", "xlambda_run", "xdens_1pdm"):
             getattr(h, fn).argtypes = [C.POINTER(CCConfig)]
+        h.xvee_run.argtypes = [C.POINTER(EOMConfig)]
 
     def _chk(self, fn, status):
         if status != ACES_OK:
@@ -257,6 +269,20 @@ class Lib:
 
     def xdens(self):
         return self._run("xdens_1pdm", CCConfig())
+
+    def xvee(self, nroots, eom_conv=7, eom_maxcyc=60, max_subspace=0, precision=PREC_FP64,
+             verbose=0):
+        """Singlet EOM-EE-CCSD excitation energies (Eh) of the lowest nroots[h]
+        states of every irrep h (xvee_run); returns (config, {irrep: [omega]})."""
+        n = [int(x) for x in nroots] + [0] * (8 - len(nroots))
+        cfg = EOMConfig(eom_conv=eom_conv, eom_maxcyc=eom_maxcyc, max_subspace=max_subspace,
+                        precision=precision, verbose=verbose)
+        for h in range(8):
+            cfg.nroots[h] = n[h]
+        st = self.h.xvee_run(C.byref(cfg))
+        if st != ACES_OK:
+            raise AcesError("xvee_run", st, self.error())
+        return cfg, {h: [cfg.omega[h][r] for r in range(n[h])] for h in range(8) if n[h]}
 
 
 _lib = None

@@ -29,7 +29,8 @@ def sources():
 
 def _compile(src):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+                    if f.endswith(".cuh") or f.endswith(".h")]
     deps.append(os.path.join(ROOT, "include", "aces_b200.h"))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""

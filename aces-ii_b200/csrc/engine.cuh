@@ -114,6 +114,9 @@ class CCEngine {
   int record_residual(bool fock_active);
   int tau_op(double *out, const double *t2, const double *t1, double c);
   int lambda_rhs();
+  // EOM-EE: sigma = P (dZ/dT)^T x - D o x on the excitations of irrep h
+  // (needs record_residual at the converged amplitudes first)
+  int eom_sigma(const double *x, double *out, int h, const int *d_irr_o, const int *d_irr_v);
   int density(std::vector<double> &D);
 
   // statistics

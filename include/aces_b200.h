@@ -249,6 +249,32 @@ int xlambda_run(aces_cc_config *cfg);
  * nmo, DPD orbital order, row-major). */
 int xdens_1pdm(aces_cc_config *cfg);
 
+/* Excited states (PROGRAM VEE, vee/doeomee_david.F): singlet EOM-EE-CCSD
+ * excitation energies of a closed-shell reference, nroots[h] lowest roots of
+ * every irrep h + 1 (ESTATE_SYM), found by a Davidson iteration from the
+ * single excitations of smallest orbital-energy gap. */
+typedef struct aces_eom_config {
+  int nroots[8];       /* roots per irrep, 0..8                               */
+  int eom_conv;        /* converged when |residual| and |d omega| < 10^-eom_conv */
+  int eom_maxcyc;      /* Davidson iterations per irrep                       */
+  int max_subspace;    /* trial vectors kept before a collapse (0: 40)        */
+  int precision;       /* ACES_PREC_*                                         */
+  int verbose;
+  /* outputs */
+  double omega[8][8];  /* excitation energies (Eh), [irrep][root], ascending  */
+  int converged[8];
+  int niter[8];
+  int nsigma;          /* products with the Jacobian evaluated                */
+  double seconds;
+} aces_eom_config;
+
+/* EOM-EE-CCSD on the amplitudes left by xvcc_run: the singlet excitation
+ * energies are the eigenvalues of the CC Jacobian on the pair-symmetric
+ * amplitude space, found from its transpose (the reverse replay of the
+ * residual pass that the Lambda equations use).  Writes record EOMEXCIT
+ * (64 doubles, [irrep][root]). */
+int xvee_run(aces_eom_config *cfg);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -137,3 +137,20 @@ def test_header_is_c99_and_config_layout_matches_ctypes(tmp_path):
     assert int(out["sizeof"]) == ctypes.sizeof(ab.CCConfig)
     for f in fields:
         assert int(out[f]) == getattr(ab.CCConfig, f).offset, f
+    # the EOM config the same way
+    efields = [f for f, _ in ab.EOMConfig._fields_]
+    body = "\n".join(f'  printf("%s %zu\\n", "{f}", offsetof(aces_eom_config, {f}));'
+                     for f in efields)
+    src.write_text(
+        "#include <stddef.h>\n#include <stdio.h>\n#include \"aces_b200.h\"\n"
+        "int main(void) {\n"
+        '  printf("sizeof %zu\\n", sizeof(aces_eom_config));\n' + body + "\n  return 0;\n}\n")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True, text=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True,
+                                                       text=True, check=True).stdout.split("\n")
+               if line)
+    assert int(out["sizeof"]) == ctypes.sizeof(ab.EOMConfig)
+    for f in efields:
+        assert int(out[f]) == getattr(ab.EOMConfig, f).offset, f
