@@ -70,7 +70,7 @@ def args():
                    help="run one small case for ncu captures and exit: a contraction "
                         "shape through aces_xgemm (ladder-small, ladder-packed, thin-t1, "
                         "lowrank-t1) or "
-                        "CCSD(T) on a small system (triples-o10-v180)")
+                        "CCSD(T) on a small system (triples-o10-v180, triples-o6-v128)")
     a = p.parse_args()
     if a.use_graph is None:
         a.use_graph = 0 if a.workload == "c5" else 1
@@ -363,7 +363,15 @@ def run_ours(a, rank, world, local_rank):
         # energies are not a precision measure: the accuracy block compares
         # them on the convergent variant
         fp64 = {"seconds_per_iter": c64.seconds_per_iter,
-                "speedup_split_vs_fp64": c64.seconds_per_iter / cfg.seconds_per_iter}
+                "speedup_split_vs_fp64": c64.seconds_per_iter / cfg.seconds_per_iter,
+                "seconds_ladder": c64.seconds_ladder}
+        try:
+            fp64["cublas_reference"] = cublas_fp64_reference(o, v, dev)
+            cb = fp64["cublas_reference"]
+            fp64["ladder_vs_cublas_fp64"] = cb["ladder_seconds"] / max(c64.seconds_ladder, 1e-30)
+            fp64["split_ladder_speedup_vs_cublas_fp64"] = cb["ladder_seconds"] / max(s_lad, 1e-30)
+        except Exception as exc:  # noqa: BLE001
+            fp64["cublas_reference"] = {"error": f"{type(exc).__name__}: {exc}"}
 
     # ---- e2e_putlst: host lists -> PUTLST -> xvcc_run (K cycles) -> GETLST T2
     lib.init(local_rank)
@@ -507,6 +515,48 @@ def run_ours(a, rank, world, local_rank):
 LADDER_TRAFFIC = {"c2": 2637.7e6 + 98.1e6}
 LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped ladder "
                          "launch in the c2 cycle (one-pass launch list)")
+
+
+def cublas_fp64_reference(o, v, dev, reps=5):
+    """FP64 tensor-core throughput of the vendor library on this GPU, as the
+    yardstick for the FP64 path (the measured peaks hold no FP64 figure):
+    cuBLAS DGEMM (through torch.matmul) on an 8192^3 product and on the two
+    products of the packed particle-particle ladder at this workload's shape
+    (M = K = v(v+1)/2 and v(v-1)/2, N = o^2), CUDA-event timed after a
+    warm-up.  Only a comparator: no product of the engine uses cuBLAS."""
+    import torch
+    out = {}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    n = 8192
+    A = torch.randn(n, n, dtype=torch.float64, device=dev)
+    Bm = torch.randn(n, n, dtype=torch.float64, device=dev)
+    t = timed(lambda: A @ Bm)
+    out["dgemm_8192_tflops"] = 2.0 * n ** 3 / t / 1e12
+    del A, Bm
+    np_, nm_ = v * (v + 1) // 2, v * (v - 1) // 2
+    tl = 0.0
+    for m in (np_, nm_):
+        U = torch.randn(m, m, dtype=torch.float64, device=dev)
+        X = torch.randn(m, o * o, dtype=torch.float64, device=dev)
+        tl += timed(lambda: U @ X)
+        del U, X
+    torch.cuda.empty_cache()
+    out["ladder_seconds"] = tl
+    out["ladder_tflops"] = 2.0 * o * o * (np_ * np_ + nm_ * nm_) / tl / 1e12
+    out["note"] = ("cuBLAS FP64 through torch.matmul; the packed ladder's two products "
+                   "without the pack/unpack kernels")
+    return out
 
 
 def accuracy(lib, wname, device, rank=0, world=1, use_graph=1):
@@ -754,6 +804,8 @@ KERNEL_CASES = {
 # captures of the (T) launches; B scaled by 0.25 so the amplitudes converge)
 PROGRAM_CASES = {
     "triples-o10-v180": dict(nocc=10, nvir=180, naux=540, seed=5, bscale=0.25),
+    # the same kernels on a few GB of device memory (56 triplets, one batch)
+    "triples-o6-v128": dict(nocc=6, nvir=128, naux=300, seed=5, bscale=0.25),
     # Lambda + density on the convergent C4 system (split precision)
     "lambda-c4": dict(nocc=20, nvir=180, naux=600, seed=3, bscale=0.25, lam=True),
 }
