@@ -26,7 +26,7 @@ std::vector<DBuf *> CCEngine::registry() {
           &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
           &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
           &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec, &L, &Ln, &gE,
-          &lrhs, &bwdA, &bwdB, &bwdC, &bwdD, &Up, &Um, &taup, &taum, &Sld, &Ald, &ladpairs};
+          &lrhs, &bwdA, &bwdB, &bwdC, &bwdD, &Up, &Um, &taup, &taum, &Sld, &Ald, &ladpairs, &Ic, &I1n};
 }
 
 void CCEngine::release() {
@@ -247,6 +247,38 @@ int CCEngine::Ggroup(const GArgs *g, int n, double beta) {
     pr[i].C = q.C;
   }
   return gemm_nt_bf16x3_grouped(pr, n, 1.0, beta, st);
+}
+
+int CCEngine::Gmulti(int M, int N, const Seg *sg, int nseg, double beta, const CView &C) {
+  bool fused = prec == ACES_PREC_BF16X3 && !recording && nseg >= 2 && nseg <= 3 && M >= 16 &&
+               N >= 16;
+  for (int i = 0; i < nseg && fused; ++i)
+    fused = sg[i].K >= 128 && (double)M * N * sg[i].K >= 1.0e8;
+  if (!fused) {
+    for (int i = 0; i < nseg; ++i)
+      ACES_TRY(G(M, N, sg[i].K, 1.0, sg[i].A, sg[i].lda, sg[i].B, sg[i].ldb,
+                 i == 0 ? beta : 1.0, C, sg[i].constA, sg[i].constB));
+    return ACES_OK;
+  }
+  // coalescing orientation as in G: C^T = B A^T when the output's unit stride runs along n
+  CView Cv = C;
+  const bool swap = C.sm0 != 1 && C.sn0 == 1;
+  if (swap) Cv = CView{C.p, C.ndiv, C.sn1, C.sn0, C.mdiv, C.sm1, C.sm0};
+  const int Mv = swap ? N : M, Nv = swap ? M : N;
+  SplitOperand a[3], b[3];
+  for (int i = 0; i < nseg; ++i) {
+    gemm_calls++;
+    gemm_flops += 2.0 * M * N * (double)sg[i].K;
+    const double *pa = swap ? sg[i].B : sg[i].A, *pb = swap ? sg[i].A : sg[i].B;
+    const long long la = swap ? sg[i].ldb : sg[i].lda, lb = swap ? sg[i].lda : sg[i].ldb;
+    const bool ca = swap ? sg[i].constB : sg[i].constA, cb = swap ? sg[i].constA : sg[i].constB;
+    const SplitOperand *sa = nullptr, *sb = nullptr;
+    ACES_TRY(split_get(pa, la, Mv, sg[i].K, ca, split_tmpG[2 * i], &sa));
+    ACES_TRY(split_get(pb, lb, Nv, sg[i].K, cb, split_tmpG[2 * i + 1], &sb));
+    a[i] = *sa;
+    b[i] = *sb;
+  }
+  return gemm_nt_bf16x3_multi(a, b, nseg, Mv, Nv, 1.0, beta, Cv, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -531,6 +563,13 @@ int CCEngine::setup_intermediates() {
   ACES_TRY(perm(I1.p, o, v, o, v, 0.0, {PT(I_oovv.p, 1.0, so[0], so[2], so[1], so[3])}));
   ACES_TRY(alloc(I2, OOVV));
   ACES_TRY(perm(I2.p, o, v, o, v, 0.0, {PT(I_oovv.p, 1.0, so[0], so[3], so[1], so[2])}));
+  // Ic = I1 - I2 / 2, I1n = -I1: W(mbej) += Y2 Ic^T + XnP I1n^T (one launch)
+  ACES_TRY(alloc(Ic, OOVV));
+  ACES_TRY(perm(Ic.p, o, v, o, v, 0.0,
+                {PT(I_oovv.p, 1.0, so[0], so[2], so[1], so[3]),
+                 PT(I_oovv.p, -0.5, so[0], so[3], so[1], so[2])}));
+  ACES_TRY(alloc(I1n, OOVV));
+  ACES_TRY(perm(I1n.p, o, v, o, v, 0.0, {PT(I_oovv.p, -1.0, so[0], so[2], so[1], so[3])}));
   // IvP[b,m,e,f] = I_ovvv[m,b,e,f]; IvP2[b,m,e,f] = I_ovvv[m,b,f,e]
   ACES_TRY(alloc(IvP, OVVV));
   ACES_TRY(perm(IvP.p, v, o, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[1], sv[0], sv[2], sv[3])}));
@@ -759,12 +798,12 @@ int CCEngine::residual() {
     CView vx{XnP.p, V, OVV, 1, V, V, OV};
     ACES_TRY(G(o * v, o * v, 1, 1.0, T1, 1, T1, 1, 1.0, vx));
   }
-  ACES_TRY(perm(Y1.p, o, v, o, v, 0.0,
-                {PT(Y2.p, 1.0, OVV, OV, V, 1), PT(XnP.p, -1.0, OVV, OV, V, 1)}));
-  ACES_TRY(G(o * v, o * v, o * v, 1.0, Y1.p, OV, I1.p, OV, 1.0, cview_rowmajor(WA.p, OV), false,
-             true));
-  ACES_TRY(G(o * v, o * v, o * v, -0.5, Y2.p, OV, I2.p, OV, 1.0, cview_rowmajor(WA.p, OV), false,
-             true));
+  // WA += (Y2 - XnP) I1^T - 1/2 Y2 I2^T = Y2 Ic^T + XnP I1n^T: one two-segment launch
+  {
+    const Seg sgw[2] = {{Y2.p, OV, Ic.p, OV, o * v, false, true},
+                        {XnP.p, OV, I1n.p, OV, o * v, false, true}};
+    ACES_TRY(Gmulti(o * v, o * v, sgw, 2, 1.0, cview_rowmajor(WA.p, OV)));
+  }
   ACES_TRY(copy(WB.p, WB0.p, (size_t)OO * VV));
   ACES_TRY(G(o, o * v * v, v, -1.0, T1, V, IvP2.p, V, 1.0, cview_rowmajor(WB.p, OVV), false, true));
   CView vWn2{WB.p, kHuge, 0, OV, OV, OVV, 1};
@@ -795,8 +834,11 @@ int CCEngine::residual() {
   ACES_TRY(perm(Tp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[2], st2[1], st2[3])}));
   ACES_TRY(perm(Tpp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[3], st2[1], st2[2])}));
   CView vr1{XP.p, V, OVV, V, V, VV, 1};
-  ACES_TRY(G(o * v, o * v, o * v, 1.0, U.p, OV, WA.p, OV, 1.0, vr1));
-  ACES_TRY(G(o * v, o * v, o * v, 1.0, Tp.p, OV, WB.p, OV, 1.0, vr1));
+  {
+    const Seg sgr[2] = {{U.p, OV, WA.p, OV, o * v, false, false},
+                        {Tp.p, OV, WB.p, OV, o * v, false, false}};
+    ACES_TRY(Gmulti(o * v, o * v, sgr, 2, 1.0, vr1));
+  }
   CView vr3{XP.p, V, VV, V, V, OVV, 1};
   ACES_TRY(G(o * v, o * v, o * v, 1.0, Tpp.p, OV, WB.p, OV, 1.0, vr3));
   // Z2 += XP + XP^T(ia<->jb) (SUMSYM / SUMRNG)

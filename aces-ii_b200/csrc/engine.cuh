@@ -49,6 +49,7 @@ class CCEngine {
   // precomputed resorted integrals
   DBuf L_oovv, LF, LovP, LooP, LmeP, I1, I2, IvP, IvP2, IX, IX2, WA0, WB0, IoP3, IvT, IvT2,
       IooT, LT1;
+  DBuf Ic, I1n;  // I1 - I2/2 and -I1 (the W(mbej) ring intermediates' integrals)
 
   // amplitudes: X = [t1 | t2] contiguous
   DBuf X, Xn, Z1, Z2;
@@ -90,6 +91,18 @@ class CCEngine {
     bool constA, constB;
   };
   int Ggroup(const GArgs *g, int n, double beta);
+  // C = beta C + sum_s A_s B_s^T over up to 4 segments with the same M, N and
+  // output (each its own K): one multi-segment tensor-core launch when every
+  // segment takes the split path, else one G call per segment
+  struct Seg {
+    const double *A;
+    long long lda;
+    const double *B;
+    long long ldb;
+    int K;
+    bool constA, constB;
+  };
+  int Gmulti(int M, int N, const Seg *sg, int nseg, double beta, const CView &C);
 
   // Lambda (adjoint) state: lambda = [l1 | l2] like X, dE/dT, tape
   DBuf L, Ln, gE, lrhs;

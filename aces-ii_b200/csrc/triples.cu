@@ -85,6 +85,56 @@ __device__ __forceinline__ void accum_sets(const bool (&use)[6], const double (&
   if constexpr (Q < 5) accum_sets<Q + 1>(use, u, vd, g4, g5);
 }
 
+// For a set of three distinct virtuals every ordering q is used, and the
+// energy terms above form a fixed bilinear form in the six W values:
+//   g4 = sum_{q,p} (4 u_s0 + u_s1 + u_s2)(u_s0 - u_s3) = u^T M u,
+//   g5 = sum_{q,p} (4 u_s0 + u_s1 + u_s2)(vd_s0 - vd_s3) = u^T M vd,
+// with integer M[a][b] = sum_{q,p} r_qp[a] c_qp[b], r = 4 e_s0 + e_s1 + e_s2,
+// c = e_s0 - e_s3 (s_m = kT.v[q][p][m]).  Built at compile time.
+struct FormTable {
+  int m[6][6];
+};
+constexpr FormTable make_form_table() {
+  FormTable f{};
+  for (int q = 0; q < 6; ++q)
+    for (int p = 0; p < 6; ++p) {
+      const int s0 = kT.v[q][p][0], s1 = kT.v[q][p][1], s2 = kT.v[q][p][2],
+                s3 = kT.v[q][p][3];
+      const int r[3] = {s0, s1, s2}, rw[3] = {4, 1, 1};
+      for (int k = 0; k < 3; ++k) {
+        f.m[r[k]][s0] += rw[k];
+        f.m[r[k]][s3] -= rw[k];
+      }
+    }
+  return f;
+}
+constexpr FormTable kM = make_form_table();
+template <int A, int B>
+struct MM {
+  static constexpr int value = kM.m[A][B];
+};
+// y[B] = sum_A M[A][B] u[A] (zero coefficients fold away)
+template <int B, int A = 0>
+__device__ __forceinline__ double form_col(const double (&u)[6]) {
+  if constexpr (A == 6) {
+    return 0.0;
+  } else {
+    constexpr int c = MM<A, B>::value;
+    if constexpr (c == 0) return form_col<B, A + 1>(u);
+    else return (double)c * u[A] + form_col<B, A + 1>(u);
+  }
+}
+template <int B = 0>
+__device__ __forceinline__ void form_apply(const double (&u)[6], const double (&vd)[6], double &g4,
+                                           double &g5) {
+  if constexpr (B < 6) {
+    const double y = form_col<B>(u);
+    g4 += y * u[B];
+    g5 += y * vd[B];
+    form_apply<B + 1>(u, vd, g4, g5);
+  }
+}
+
 // a >= b >= c from the flat index n of the set in the order
 // (a, then b <= a, then c <= b): n = a(a+1)(a+2)/6 + b(b+1)/2 + c
 __device__ __forceinline__ void decode_set(int n, int &a, int &b, int &c) {
@@ -100,70 +150,134 @@ __device__ __forceinline__ void decode_set(int n, int &a, int &b, int &c) {
   c = r - y * (y + 1) / 2;
 }
 
-// One triplet's contribution to E[4]T and E[5]ST: one thread per virtual set
-// {a >= b >= c}, all six orderings of the set read once; the distinct
-// orderings q of repeated virtuals are counted once.  Partial sums per block,
-// reduced in a fixed order.
-// Entry e = blockIdx.y of a batch: triplet trip3[3e..3e+2], its W at
-// Wbase + e * wstride (FP64, or FP32 for the split path), partial sums at
-// part[2 * (e * gridDim.x + blockIdx.x)].
+// One batch entry's contribution to E[4]T and E[5]ST, every set {a >= b >= c}
+// of virtuals evaluated once with all six of its orderings, the distinct
+// orderings q of repeated virtuals counted once (a = b keeps q = 0, 1, 4;
+// b = c keeps q = 0, 2, 3; a = b = c keeps q = 0).  The loads are staged
+// through shared memory.  Block
+// (blockIdx.x, blockIdx.y = e) takes one tile triple A >= B >= C of 8-wide
+// virtual tiles (decoded like a set) of triplet e and loads, with sector-
+// complete row reads, the six permuted 8x8x8 cubes of W (tiles (A,B,C),
+// (A,C,B), ..., one per ordering), the 8x8 tiles of the <jk|..>, <ik|..>,
+// <ij|..> slabs for every ordered pair of the three tiles, and the t1 rows and
+// orbital energies of the three tiles.  Each of its 128 threads then
+// evaluates four sets {a >= b >= c} of the cube from shared memory: sets of
+// three distinct virtuals through the constant bilinear form, sets with a
+// repeated virtual through the general per-ordering sum.
+constexpr int kTile = 8;
+// kOrd[s][r] in device code: the first position is s / 2, the other two
+// follow in increasing order for even s and swapped for odd s
+__host__ __device__ __forceinline__ constexpr int ordpos(int s, int r) {
+  const int f = s >> 1, lo = f == 0 ? 1 : 0, hi = f == 2 ? 1 : 2;
+  return r == 0 ? f : (r == 1 ? ((s & 1) ? hi : lo) : ((s & 1) ? lo : hi));
+}
+static_assert(ordpos(0, 2) == kOrd[0][2] && ordpos(3, 1) == kOrd[3][1] &&
+                  ordpos(4, 2) == kOrd[4][2] && ordpos(5, 0) == kOrd[5][0] &&
+                  ordpos(1, 1) == kOrd[1][1] && ordpos(2, 1) == kOrd[2][1],
+              "ordpos restates kOrd");
 template <typename TW>
-__global__ void __launch_bounds__(256)
-    k_triples_energy(const TW *__restrict__ Wbase, long long wstride,
-                     const int *__restrict__ trip3, const double *__restrict__ t1,
-                     const double *__restrict__ Ioovv, const double *__restrict__ eo,
-                     const double *__restrict__ ev, int o, int v, double *__restrict__ part) {
+__global__ void __launch_bounds__(128)
+    k_triples_energy_tiled(const TW *__restrict__ Wbase, long long wstride,
+                           const int *__restrict__ trip3, const double *__restrict__ t1,
+                           const double *__restrict__ Ioovv, const double *__restrict__ eo,
+                           const double *__restrict__ ev, int o, int v,
+                           double *__restrict__ part) {
+  __shared__ TW cube[6][kTile][kTile + 1][kTile + 1];
+  __shared__ double It[3][6][kTile][kTile + 1];
+  __shared__ double ts[3][3][kTile];   // [t_i, t_j, t_k][tile position][local]
+  __shared__ double es[3][kTile];      // ev of the three tiles
+  __shared__ double sh[2][4];
   const int e = blockIdx.y;
   const int i = trip3[3 * e], j = trip3[3 * e + 1], k = trip3[3 * e + 2];
   const TW *__restrict__ W = Wbase + (long long)e * wstride;
-  // the distinct permutations of (i, j, k): 6 for distinct indices, 3 when
-  // two coincide, 1 when all three do
   const int mult = (i == j && j == k) ? 6 : ((i == j || j == k) ? 2 : 1);
   const double scale = 1.0 / (3.0 * mult);
   const long long v2 = (long long)v * v;
-  const int nsets = v * (v + 1) * (v + 2) / 6;
+  int T[3];
+  decode_set((int)blockIdx.x, T[0], T[1], T[2]);
+  const int b0[3] = {T[0] * kTile, T[1] * kTile, T[2] * kTile};
+  const int tid = threadIdx.x;
+  // six cubes: cube s spans tiles (T[kOrd[s][0]], T[kOrd[s][1]], T[kOrd[s][2]])
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const int c0 = b0[ordpos(s, 0)], c1 = b0[ordpos(s, 1)], c2 = b0[ordpos(s, 2)];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = tid + 128 * q;
+      const int x = idx >> 6, y = (idx >> 3) & 7, z = idx & 7;
+      const int gx = c0 + x, gy = c1 + y, gz = c2 + z;
+      cube[s][x][y][z] = (gx < v && gy < v && gz < v) ? W[gx * v2 + (long long)gy * v + gz]
+                                                      : (TW)0;
+    }
+  }
+  // integral tiles: slab 0 = <jk|..>, 1 = <ik|..>, 2 = <ij|..>; ordered pair
+  // (x, y) of tile positions -> index x * 2 + (y > x ? y - 1 : y)
+  const double *slab[3] = {Ioovv + ((long long)j * o + k) * v2, Ioovv + ((long long)i * o + k) * v2,
+                           Ioovv + ((long long)i * o + j) * v2};
+  for (int idx = tid; idx < 3 * 6 * 64; idx += 128) {
+    const int sl = idx / 384, pr = (idx / 64) % 6, r = (idx >> 3) & 7, c = idx & 7;
+    const int x = pr >> 1, yy = pr & 1, y = yy < x ? yy : yy + 1;
+    const int gr = b0[x] + r, gc = b0[y] + c;
+    It[sl][pr][r][c] = (gr < v && gc < v) ? slab[sl][(long long)gr * v + gc] : 0.0;
+  }
+  if (tid < 72) {
+    const int w = tid / 24, pos = (tid / 8) % 3, l = tid & 7;
+    const int occ = w == 0 ? i : (w == 1 ? j : k), g = b0[pos] + l;
+    ts[w][pos][l] = g < v ? t1[(long long)occ * v + g] : 0.0;
+  } else if (tid < 96) {
+    const int pos = (tid - 72) / 8, l = tid & 7, g = b0[pos] + l;
+    es[pos][l] = g < v ? ev[g] : 0.0;
+  }
+  __syncthreads();
   const double eijk = eo[i] + eo[j] + eo[k];
-  // the three <jk|..>, <ik|..>, <ij|..> slabs of <ij|ab> and the t1 rows
-  const double *Ijk = Ioovv + ((long long)j * o + k) * v2;
-  const double *Iik = Ioovv + ((long long)i * o + k) * v2;
-  const double *Iij = Ioovv + ((long long)i * o + j) * v2;
-  const double *ti = t1 + (long long)i * v, *tj = t1 + (long long)j * v, *tk = t1 + (long long)k * v;
   double s4 = 0.0, s5 = 0.0;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nsets; n += gridDim.x * blockDim.x) {
-    int a, b, c;
-    decode_set(n, a, b, c);
-    // orderings (a,b,c) (a,c,b) (b,a,c) (b,c,a) (c,a,b) (c,b,a), as kOrd
-    const int ordv[6][3] = {{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a}, {c, a, b}, {c, b, a}};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int n = tid + 128 * q;
+    const int l[3] = {n >> 6, (n >> 3) & 7, n & 7};
+    const int a = b0[0] + l[0], b = b0[1] + l[1], c = b0[2] + l[2];
+    if (a >= v || b >= v || c >= v || a < b || b < c) continue;
     double u[6], vd[6];
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
-      const int p0 = ordv[s][0], p1 = ordv[s][1], p2 = ordv[s][2];
-      u[s] = (double)W[p0 * v2 + (long long)p1 * v + p2];
+      const int P0 = ordpos(s, 0), P1 = ordpos(s, 1), P2 = ordpos(s, 2);
+      u[s] = (double)cube[s][l[P0]][l[P1]][l[P2]];
+      const int p12 = P1 * 2 + (P2 > P1 ? P2 - 1 : P2), p02 = P0 * 2 + (P2 > P0 ? P2 - 1 : P2),
+                p01 = P0 * 2 + (P1 > P0 ? P1 - 1 : P1);
       // V - W at (p0,p1,p2): t_i^p0 <jk|p1p2> + t_j^p1 <ik|p0p2> + t_k^p2 <ij|p0p1>
-      vd[s] = ti[p0] * Ijk[p1 * v + p2] + tj[p1] * Iik[p0 * v + p2] + tk[p2] * Iij[p0 * v + p1];
+      vd[s] = ts[0][P0][l[P0]] * It[0][p12][l[P1]][l[P2]] +
+              ts[1][P1][l[P1]] * It[1][p02][l[P0]][l[P2]] +
+              ts[2][P2][l[P2]] * It[2][p01][l[P0]][l[P1]];
     }
-    // ordering q duplicates an earlier one when the set repeats a virtual:
-    // a = b keeps q = 0, 1, 4; b = c keeps q = 0, 2, 3; a = b = c keeps q = 0
-    const bool ab = a == b, bc = b == c;
-    const bool use[6] = {true, !bc, !ab, !ab, !bc, !(ab || bc)};
-    const double D = eijk - ev[a] - ev[b] - ev[c];
+    const double D = eijk - es[0][l[0]] - es[1][l[1]] - es[2][l[2]];
     double g4 = 0.0, g5 = 0.0;
-    accum_sets<0>(use, u, vd, g4, g5);
-    s4 += g4 / D;
-    s5 += g5 / D;
+    if (a > b && b > c) {
+      form_apply(u, vd, g4, g5);
+    } else {
+      const bool ab = a == b, bc = b == c;
+      const bool use[6] = {true, !bc, !ab, !ab, !bc, !(ab || bc)};
+      accum_sets<0>(use, u, vd, g4, g5);
+    }
+    const double inv = 1.0 / D;
+    s4 += g4 * inv;
+    s5 += g5 * inv;
   }
-  // block reduction (fixed order)
-  __shared__ double sh[2][8];
   for (int off = 16; off; off >>= 1) {
     s4 += __shfl_down_sync(0xffffffffu, s4, off);
     s5 += __shfl_down_sync(0xffffffffu, s5, off);
   }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { sh[0][wid] = s4; sh[1][wid] = s5; }
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) {
+    sh[0][wid] = s4;
+    sh[1][wid] = s5;
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     double a4 = 0.0, a5 = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a4 += sh[0][w]; a5 += sh[1][w]; }
+    for (int w = 0; w < 4; ++w) {
+      a4 += sh[0][w];
+      a5 += sh[1][w];
+    }
     const long long slot = (long long)e * gridDim.x + blockIdx.x;
     part[2 * slot] = scale * a4;
     part[2 * slot + 1] = scale * a5;
@@ -341,7 +455,8 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
     const BatchEntry *d_ent = reinterpret_cast<const BatchEntry *>(dent.p);
     const SplitOperand Ac[4] = {sT2, sT2, sHn, sHn}, Bc[4] = {sGv, sGvT, sT2P, sT2Q};
     const SplitOperand Aa[4] = {sGv, sGvT, sT2P, sT2Q}, Ba[4] = {sT2, sT2, sHn, sHn};
-    const int nblk = 64;
+    const int nt = (v + kTile - 1) / kTile;
+    const int nblk = nt * (nt + 1) * (nt + 2) / 6;   // tile triples A >= B >= C
     ACES_TRY(alloc(part, (size_t)std::max(ntrip, 1) * nblk * 2));
     for (int t0b = 0; t0b < ntrip; t0b += nb) {
       const int n = std::min(nb, ntrip - t0b);
@@ -357,7 +472,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
       cv.p = Wb.p;
       ACES_TRY(gemm_nt_bf16x3_batched(Aa, Ba, 4, v * v, v, &byclass[(size_t)2 * ntrip + t0b],
                                       d_ent + 2 * ntrip + t0b, n, 1.0, 1.0, cv, true, st));
-      k_triples_energy<float><<<dim3(nblk, n), 256, 0, st>>>(
+      k_triples_energy_tiled<float><<<dim3(nblk, n), 128, 0, st>>>(
           reinterpret_cast<const float *>(Wb.p), V3, d_trip + 3 * t0b, t1(), I_oovv.p, eo.p,
           ev.p, o, v, part.p + (size_t)t0b * nblk * 2);
       count_launch();
@@ -367,7 +482,8 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   } else {
     // FP64: one triplet at a time, W in FP64
     ACES_TRY(alloc(Wb, V3));
-    const int nblk = 148 * 4;
+    const int nt = (v + kTile - 1) / kTile;
+    const int nblk = nt * (nt + 1) * (nt + 2) / 6;
     ACES_TRY(alloc(part, (size_t)std::max(ntrip, 1) * nblk * 2));
     auto T2p = [&](int x, int y) { return t2() + ((long long)x * o + y) * V * V; };
     auto Hp = [&](int y, int z) { return Hn.p + ((long long)y * o + z) * V * O; };
@@ -408,7 +524,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
         const double *const B[4] = {T2p(j, i), T2p(j, k), Hp(k, j), Hp(i, j)};
         ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
       }
-      k_triples_energy<double><<<dim3(nblk, 1), 256, 0, st>>>(
+      k_triples_energy_tiled<double><<<dim3(nblk, 1), 128, 0, st>>>(
           Wb.p, 0, d_trip + 3 * t, t1(), I_oovv.p, eo.p, ev.p, o, v,
           part.p + (size_t)t * nblk * 2);
       count_launch();
