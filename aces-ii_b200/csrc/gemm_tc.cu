@@ -622,16 +622,17 @@ EncodeTiledFn encode_fn() {
 // operand views for every triplet: 16 maps per launch without the cache.
 struct MapKey {
   const void *base;
-  int rows_pad, k_pad, box_rows;
+  int rows_pad, k_pad, k, box_rows;
   bool operator==(const MapKey &o) const {
-    return base == o.base && rows_pad == o.rows_pad && k_pad == o.k_pad &&
+    return base == o.base && rows_pad == o.rows_pad && k_pad == o.k_pad && k == o.k &&
            box_rows == o.box_rows;
   }
 };
 struct MapKeyHash {
   size_t operator()(const MapKey &k) const {
     size_t h = std::hash<const void *>()(k.base);
-    h ^= ((size_t)k.rows_pad * 0x9E3779B97F4A7C15ULL) + ((size_t)k.k_pad << 20) + k.box_rows;
+    h ^= ((size_t)k.rows_pad * 0x9E3779B97F4A7C15ULL) + ((size_t)k.k_pad << 20) +
+         ((size_t)k.k << 40) + k.box_rows;
     return h;
   }
 };
@@ -644,8 +645,13 @@ MapCache &map_cache() {
   return *c;
 }
 
-int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) {
-  const MapKey key{base, rows_pad, k_pad, box_rows};
+// The map's K extent is the operand's true K (rows stay k_pad elements apart):
+// the tail of the last k tile of a segment is the TMA's zero fill, read from
+// neither L2 nor DRAM (for a K = nocc segment, 20 of the 64 columns of a k
+// tile are data).  The padding in memory is zero as well, so the products
+// are the same either way.
+int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int k, int box_rows) {
+  const MapKey key{base, rows_pad, k_pad, k, box_rows};
   MapCache &mc = map_cache();
   {
     std::lock_guard<std::mutex> lk(mc.mu);
@@ -660,7 +666,7 @@ int make_map(CUtensorMap *m, void *base, int rows_pad, int k_pad, int box_rows) 
     set_error("cuTensorMapEncodeTiled unavailable");
     return ACES_ERR_CUDA;
   }
-  cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows_pad};
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows_pad};
   cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
   cuuint32_t box[2] = {(cuuint32_t)TBK, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
@@ -701,10 +707,11 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
                 a.k_pad, b.k_pad, a.rows, b.rows);
       return ACES_ERR_ARG;
     }
-    ACES_TRY(make_map(&L.ah[g][s], a.hi, a.rows_pad, a.k_pad, TBM));
-    ACES_TRY(make_map(&L.al[g][s], a.lo, a.rows_pad, a.k_pad, TBM));
-    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, TBN));
-    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, TBN));
+    const int kk = std::min(a.k, b.k) > 0 ? std::min(a.k, b.k) : a.k_pad;
+    ACES_TRY(make_map(&L.ah[g][s], a.hi, a.rows_pad, a.k_pad, kk, TBM));
+    ACES_TRY(make_map(&L.al[g][s], a.lo, a.rows_pad, a.k_pad, kk, TBM));
+    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, kk, TBN));
+    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, kk, TBN));
     P.kt0[s + 1] = P.kt0[s] + a.k_pad / TBK;
   }
   for (int s = nseg + 1; s <= kMaxSeg; ++s) P.kt0[s] = P.kt0[nseg];

@@ -70,7 +70,8 @@ def args():
                    help="run one small case for ncu captures and exit: a contraction "
                         "shape through aces_xgemm (ladder-small, ladder-packed, thin-t1, "
                         "lowrank-t1) or "
-                        "CCSD(T) on a small system (triples-o10-v180, triples-o6-v128)")
+                        "CCSD(T) on a small system (triples-o10-v180, triples-o6-v128) or "
+                        "split CCSD cycles (ccsd-o40-v100)")
     a = p.parse_args()
     if a.use_graph is None:
         a.use_graph = 0 if a.workload == "c5" else 1
@@ -312,6 +313,17 @@ def run_batch(a, rank=0, world=1, local_rank=0):
     print(json.dumps(line), flush=True)
 
 
+def getlst_pinned(lib, host, lst, irrep=1):
+    """GETLST of every column of (irrep, lst) into the pinned host tensor
+    `host` (the caller-owned destination buffer of acescore/getlst.F)."""
+    import ctypes
+    nr, nc = lib.list_dims(irrep, lst)
+    assert host.numel() >= nr * nc
+    lib._chk("aces_getlst", lib.h.aces_getlst(ctypes.c_void_p(host.data_ptr()), 1, nc, irrep,
+                                              lst))
+    return host[:nr * nc]
+
+
 def put_lists(lib, eps, lists):
     lib.putrec("SCFEVALA", eps)
     nbytes = eps.nbytes
@@ -399,6 +411,7 @@ def run_ours(a, rank, world, local_rank):
     Bpin = torch.empty(Bf.shape, dtype=torch.float64, pin_memory=True)
     Bpin.copy_(torch.from_numpy(Bf))
     del Bf
+    t2_host = torch.empty(o * o * v * v, dtype=torch.float64, pin_memory=True)
     lib.init(local_rank)
     torch.cuda.synchronize()
     barrier(world)
@@ -411,7 +424,7 @@ def run_ours(a, rank, world, local_rank):
                   use_graph=a.use_graph)
     tx = time.perf_counter()
     nr, nc = lib.list_dims(1, 46)
-    t2 = lib.getlst(1, nc, 1, 46)
+    t2 = getlst_pinned(lib, t2_host, 46)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     e2e_parts = {"intprc_df_s": tp - t0, "xvcc_s": tx - tp, "xvcc_setup_s": ce.seconds_setup,
@@ -419,8 +432,8 @@ def run_ours(a, rank, world, local_rank):
     barrier(world)
     e2e = max_over_ranks((t1 - t0) / K, world)
     h2d = Bpin.numel() * 8 + eps_h.nbytes
-    d2h = t2.nbytes + 8
-    del Bpin
+    d2h = t2.numel() * 8 + 8
+    del Bpin, t2_host
     lib.fin()
 
     pk, pk_src = peaks()
@@ -808,6 +821,9 @@ PROGRAM_CASES = {
     "triples-o6-v128": dict(nocc=6, nvir=128, naux=300, seed=5, bscale=0.25),
     # Lambda + density on the convergent C4 system (split precision)
     "lambda-c4": dict(nocc=20, nvir=180, naux=600, seed=3, bscale=0.25, lam=True),
+    # split CCSD cycles of a system whose o^2 v^2 arrays (128 MB) exceed L2 while
+    # the whole run holds a few GB: DRAM counters of the bandwidth-bound kernels
+    "ccsd-o40-v100": dict(nocc=40, nvir=100, naux=300, seed=7, bscale=0.25, cycles=4),
 }
 
 
@@ -819,13 +835,20 @@ def run_program_case(a):
     from acesb200.workloads import synthetic_df
     wl = dict(PROGRAM_CASES[a.kernel_case])
     lam = wl.pop("lam", False)
+    cycles = wl.pop("cycles", None)
     eps, B, _ = synthetic_df(**wl)
     e, lists, o, v = _lists_from_df(eps, B, wl["nocc"], wl["nvir"], torch.device("cuda", 0))
     lib = ab.load()
     lib.init(0)
     lib.sym_init([o], [v])
     put_lists(lib, e, lists)
-    if lam:
+    if cycles:
+        c = lib.xvcc(cc_conv=30, cc_maxcyc=cycles, cc_exporder=5, precision=ab.PREC_BF16X3,
+                     allow_noconv=True)
+        print(json.dumps({"kernel_case": a.kernel_case, "cycles": c.ncycle,
+                          "seconds_per_iter": c.seconds_per_iter,
+                          "launches_per_iter": c.launches_per_iter}), flush=True)
+    elif lam:
         c = lib.xvcc(cc_conv=9, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3)
         cl = lib.xlambda(cc_conv=9, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3,
                          timing_warmup=1)
