@@ -324,11 +324,10 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   return r;
 }
 
-// 200 registers per thread: 320 threads x 200 = 64000 of the SM's 65536, one
-// CTA per SM, and the epilogue's 64 FP64 column sums stay in registers (a
-// launch bound of 320 threads let the compiler stop at 168 and spill)
-static_assert(kThreads * 200 <= 65536, "register budget of one CTA per SM");
-__global__ void __maxnreg__(200)
+// One CTA of 10 warps per SM: registers are allocated per SM sub-partition
+// (16384 each) and three of the warps share one, so a thread gets at most
+// 168 (the epilogue spills a few of its 64 FP64 column sums, L1-resident)
+__global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
                   double *__restrict__ part) {
   const int nTiles = L.nTiles;
