@@ -5,6 +5,7 @@
 //
 // Index conventions (C order): t1[i,a]; t2[i,j,a,b] = t_{iJ}^{aB} (the
 // reference's list 46, Ab x Ij, in C1); integrals <pq|rs> as I_xxxx[p,q,r,s].
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -859,7 +860,114 @@ int CCEngine::residual() {
 // half the flops.  U+/U- are built once from the dense <ab|cd> (or the list).
 // The map is linear in tau and needs no symmetry of it, so the Lambda
 // backward pass calls it with (Z2 adjoint, tau adjoint) for in and out.
+int CCEngine::ladder_packed_blocks(const double *in, double *out) {
+  const int nir = state().sym.nirrep;
+  LadderBlocks &Lb = ladb;
+  if (!Up.p) {
+    // pair lists by pair irrep: symmetric c <= d and antisymmetric c < d (d
+    // slowest), occupied pairs ij by irrep; local indices of every pair
+    std::vector<int> pp, mm, pidx((size_t)v * v, -1), midx((size_t)v * v, -1), ijs, ijl(o * o);
+    Lb.nirrep = nir;
+    Lb.o = o;
+    Lb.v = v;
+    Lb.offP[0] = Lb.offM[0] = Lb.offIJ[0] = 0;
+    for (int g = 0; g < nir; ++g) {
+      int np_g = 0, nm_g = 0, nij = 0;
+      for (int d = 0; d < v; ++d)
+        for (int c = 0; c <= d; ++c) {
+          if ((irr_v[c] ^ irr_v[d]) != g) continue;
+          pp.push_back(c);
+          pp.push_back(d);
+          pidx[(size_t)c * v + d] = np_g++;
+          if (c < d) {
+            mm.push_back(c);
+            mm.push_back(d);
+            midx[(size_t)c * v + d] = nm_g++;
+          }
+        }
+      for (int ij = 0; ij < o * o; ++ij)
+        if ((irr_o[ij / o] ^ irr_o[ij % o]) == g) {
+          ijs.push_back(ij);
+          ijl[ij] = nij++;
+        }
+      Lb.nP[g] = np_g;
+      Lb.nM[g] = nm_g;
+      Lb.nIJ[g] = nij;
+      Lb.offP[g + 1] = Lb.offP[g] + np_g;
+      Lb.offM[g + 1] = Lb.offM[g] + nm_g;
+      Lb.offIJ[g + 1] = Lb.offIJ[g] + nij;
+    }
+    for (int g = nir; g < 8; ++g) Lb.nP[g] = Lb.nM[g] = Lb.nIJ[g] = 0;
+    Lb.offUp[0] = Lb.offUm[0] = 0;
+    for (int g = 0; g < nir; ++g) {
+      Lb.offUp[g + 1] = Lb.offUp[g] + (long long)Lb.nP[g] * Lb.nP[g];
+      Lb.offUm[g + 1] = Lb.offUm[g] + (long long)Lb.nM[g] * Lb.nM[g];
+    }
+    std::vector<int> tab;
+    auto put = [&](const std::vector<int> &x) {
+      const size_t at = tab.size();
+      tab.insert(tab.end(), x.begin(), x.end());
+      return at;
+    };
+    std::vector<int> io(irr_o.begin(), irr_o.end()), iv(irr_v.begin(), irr_v.end());
+    const size_t a_pp = put(pp), a_mm = put(mm), a_pi = put(pidx), a_mi = put(midx),
+                 a_ijs = put(ijs), a_ijl = put(ijl), a_io = put(io), a_iv = put(iv);
+    ACES_TRY(alloc(ladpairs, (tab.size() + 1) / 2 + 1));
+    ACES_CUDA(cudaMemcpyAsync(ladpairs.p, tab.data(), tab.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, st));
+    const int *base = reinterpret_cast<const int *>(ladpairs.p);
+    Lb.pp = base + a_pp;
+    Lb.mm = base + a_mm;
+    Lb.pidx = base + a_pi;
+    Lb.midx = base + a_mi;
+    Lb.ijs = base + a_ijs;
+    Lb.ijl = base + a_ijl;
+    Lb.irr_o = base + a_io;
+    Lb.irr_v = base + a_iv;
+    ACES_TRY(alloc(Up, (size_t)std::max(1LL, Lb.offUp[nir])));
+    ACES_TRY(alloc(Um, (size_t)std::max(1LL, Lb.offUm[nir])));
+    launch_ladder_pack_v_blk(Up.p, Um.p, I_vvvv.p, Lb, st);
+    ACES_CUDA(cudaStreamSynchronize(st));
+  }
+  // per-call blocks of the vector's symmetry
+  Lb.hs = ladder_sym;
+  Lb.offTp[0] = Lb.offTm[0] = 0;
+  for (int g = 0; g < nir; ++g) {
+    const long long rows = Lb.nIJ[g ^ Lb.hs];
+    Lb.offTp[g + 1] = Lb.offTp[g] + rows * Lb.nP[g];
+    Lb.offTm[g + 1] = Lb.offTm[g] + rows * Lb.nM[g];
+  }
+  ACES_TRY(alloc(taup, (size_t)std::max(1LL, Lb.offTp[nir])));
+  ACES_TRY(alloc(taum, (size_t)std::max(1LL, Lb.offTm[nir])));
+  ACES_TRY(alloc(Sld, (size_t)std::max(1LL, Lb.offTp[nir])));
+  ACES_TRY(alloc(Ald, (size_t)std::max(1LL, Lb.offTm[nir])));
+  launch_ladder_pack_tau_blk(taup.p, taum.p, in, Lb, st);
+  // block products S_g = U+_g tau+_g^T, A_g = U-_g tau-_g^T, three per grouped launch
+  std::vector<GArgs> probs;
+  for (int g = 0; g < nir; ++g) {
+    const int rows = Lb.nIJ[g ^ Lb.hs];
+    if (rows == 0) continue;
+    const int np_g = Lb.nP[g], nm_g = Lb.nM[g];
+    if (np_g > 0)
+      probs.push_back({np_g, rows, np_g, Up.p + Lb.offUp[g], np_g, taup.p + Lb.offTp[g], np_g,
+                       cview_colmajor(Sld.p + Lb.offTp[g], np_g), true, false});
+    if (nm_g > 0)
+      probs.push_back({nm_g, rows, nm_g, Um.p + Lb.offUm[g], nm_g, taum.p + Lb.offTm[g], nm_g,
+                       cview_colmajor(Ald.p + Lb.offTm[g], nm_g), true, false});
+  }
+  // the largest products first, so each grouped launch pairs similar sizes
+  std::sort(probs.begin(), probs.end(), [](const GArgs &x, const GArgs &y) {
+    return (double)x.M * x.N * x.K > (double)y.M * y.N * y.K;
+  });
+  for (size_t q = 0; q < probs.size(); q += 3)
+    ACES_TRY(Ggroup(probs.data() + q, (int)std::min<size_t>(3, probs.size() - q), 0.0));
+  launch_ladder_unpack_blk(out, Sld.p, Ald.p, Lb, st);
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
 int CCEngine::ladder_packed(const double *in, double *out) {
+  if (state().sym.nirrep > 1) return ladder_packed_blocks(in, out);
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2, oo = o * o;
   if (!Up.p) {
     // pair tables: p(c,d) = d(d+1)/2 + c (c <= d), m(c,d) = d(d-1)/2 + c (c < d)

@@ -65,6 +65,12 @@ class CCEngine {
   DBuf Up, Um, taup, taum, Sld, Ald, ladpairs;
   // out[ij,ab] += <ab|cd> in[ij,cd] at half the dense flops
   int ladder_packed(const double *in, double *out);
+  // the same on irrep blocks (more than one irrep): pair irrep g of (a,b) and
+  // (c,d) with occupied pairs of irrep g ^ ladder_sym (0 for the amplitudes
+  // and Lambda, the state's irrep for EOM products)
+  int ladder_packed_blocks(const double *in, double *out);
+  int ladder_sym = 0;
+  LadderBlocks ladb{};  // block tables (device pointers into ladpairs)
   DBuf scratch, dev_small;  // reductions / DIIS scalars
   // DIIS history
   std::vector<DBuf> hx, he;

@@ -118,7 +118,12 @@ int CCEngine::eom_sigma(const double *x, double *out, int h, const int *d_irr_o,
   if (!z1b || !z2b) return ACES_ERR_NOMEM;
   launch_axpy(z1b, x, 1.0, ov, st);
   launch_axpy(z2b, x + ov, 1.0, len - ov, st);
-  ACES_TRY(backward());
+  // the ladder couples occupied pairs of irrep g ^ h with virtual pairs of
+  // irrep g for a vector of irrep h
+  ladder_sym = h;
+  const int bs = backward();
+  ladder_sym = 0;
+  ACES_TRY(bs);
   const double *g = adj(X.p);
   // pair symmetriser on the doubles: out2 = (g2 + g2^T) / 2, g2^T[i,j,a,b] = g2[j,i,b,a]
   const long long s2[4] = {O * V * V, V * V, V, 1};

@@ -898,4 +898,118 @@ void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, i
   count_launch();
 }
 
+// ---- irrep-blocked packed ladder ----------------------------------------------
+// block g of a flat index over blocks with sizes given by a prefix array
+__device__ __forceinline__ int find_block(const long long *pref, int nb, long long e) {
+  int g = 0;
+  while (g + 1 < nb && e >= pref[g + 1]) ++g;
+  return g;
+}
+
+__global__ void k_ladder_pack_v_blk(double *__restrict__ Up, double *__restrict__ Um,
+                                    const double *__restrict__ V, LadderBlocks L) {
+  const size_t v = L.v, vv = v * v;
+  const long long nup = L.offUp[L.nirrep], total = nup + L.offUm[L.nirrep];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < nup) {
+      const int g = find_block(L.offUp, L.nirrep, e);
+      const long long r = e - L.offUp[g];
+      const int n = L.nP[g], pl = (int)(r / n), ql = (int)(r - (long long)pl * n);
+      const int a = L.pp[2 * (L.offP[g] + pl)], b = L.pp[2 * (L.offP[g] + pl) + 1];
+      const int c = L.pp[2 * (L.offP[g] + ql)], d = L.pp[2 * (L.offP[g] + ql) + 1];
+      const double *row = V + ((size_t)a * v + b) * vv;
+      Up[e] = c == d ? row[(size_t)c * v + c] : 0.5 * (row[(size_t)c * v + d] + row[(size_t)d * v + c]);
+    } else {
+      const long long em = e - nup;
+      const int g = find_block(L.offUm, L.nirrep, em);
+      const long long r = em - L.offUm[g];
+      const int n = L.nM[g], pl = (int)(r / n), ql = (int)(r - (long long)pl * n);
+      const int a = L.mm[2 * (L.offM[g] + pl)], b = L.mm[2 * (L.offM[g] + pl) + 1];
+      const int c = L.mm[2 * (L.offM[g] + ql)], d = L.mm[2 * (L.offM[g] + ql) + 1];
+      const double *row = V + ((size_t)a * v + b) * vv;
+      Um[em] = 0.5 * (row[(size_t)c * v + d] - row[(size_t)d * v + c]);
+    }
+  }
+}
+
+void launch_ladder_pack_v_blk(double *Up, double *Um, const double *V, const LadderBlocks &L,
+                              cudaStream_t st) {
+  const long long total = L.offUp[L.nirrep] + L.offUm[L.nirrep];
+  if (total == 0) return;
+  const long long nb = std::min<long long>((total + 255) / 256, 148 * 32);
+  k_ladder_pack_v_blk<<<(unsigned)nb, 256, 0, st>>>(Up, Um, V, L);
+  count_launch();
+}
+
+__global__ void k_ladder_pack_tau_blk(double *__restrict__ tp, double *__restrict__ tm,
+                                      const double *__restrict__ tau, LadderBlocks L) {
+  const size_t v = L.v, vv = v * v;
+  const long long ntp = L.offTp[L.nirrep], total = ntp + L.offTm[L.nirrep];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const bool plus = e < ntp;
+    const long long ee = plus ? e : e - ntp;
+    const int g = find_block(plus ? L.offTp : L.offTm, L.nirrep, ee);
+    const long long r = ee - (plus ? L.offTp[g] : L.offTm[g]);
+    const int n = plus ? L.nP[g] : L.nM[g];
+    const int rl = (int)(r / n), ql = (int)(r - (long long)rl * n);
+    const int ij = L.ijs[L.offIJ[g ^ L.hs] + rl];
+    const int *pl = plus ? L.pp + 2 * (L.offP[g] + ql) : L.mm + 2 * (L.offM[g] + ql);
+    const int c = pl[0], d = pl[1];
+    const double *t = tau + (size_t)ij * vv;
+    if (plus)
+      tp[e] = c == d ? t[(size_t)c * v + c] : t[(size_t)c * v + d] + t[(size_t)d * v + c];
+    else
+      tm[ee] = t[(size_t)c * v + d] - t[(size_t)d * v + c];
+  }
+}
+
+void launch_ladder_pack_tau_blk(double *tp, double *tm, const double *tau, const LadderBlocks &L,
+                                cudaStream_t st) {
+  const long long total = L.offTp[L.nirrep] + L.offTm[L.nirrep];
+  if (total == 0) return;
+  const long long nb = std::min<long long>((total + 255) / 256, 148 * 32);
+  k_ladder_pack_tau_blk<<<(unsigned)nb, 256, 0, st>>>(tp, tm, tau, L);
+  count_launch();
+}
+
+// Z2[ij][a][b] += S + A / S - A / S over the elements whose pair irreps
+// satisfy irrep(ab) ^ irrep(ij) == hs; S, A: block g = irrep(ab), column
+// ij's local index within the occupied pairs of irrep g ^ hs
+__global__ void k_ladder_unpack_blk(double *__restrict__ Z2, const double *__restrict__ S,
+                                    const double *__restrict__ A, LadderBlocks L) {
+  const long long v = L.v, vv = v * v, total = (long long)L.o * L.o * vv;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ij = (int)(e / vv);
+    const int ab = (int)(e - (long long)ij * vv);
+    const int a = ab / (int)v, b = ab - a * (int)v;
+    const int i = ij / L.o, j = ij - i * L.o;
+    const int g = L.irr_v[a] ^ L.irr_v[b];
+    if ((g ^ L.irr_o[i] ^ L.irr_o[j]) != L.hs) continue;
+    const long long rl = L.ijl[ij];
+    const double *s = S + L.offTp[g] + rl * L.nP[g];
+    const double *an = A + L.offTm[g] + rl * L.nM[g];
+    double x;
+    if (a == b) {
+      x = s[L.pidx[ab]];
+    } else if (a < b) {
+      x = s[L.pidx[ab]] + an[L.midx[ab]];
+    } else {
+      const int ba = b * (int)v + a;
+      x = s[L.pidx[ba]] - an[L.midx[ba]];
+    }
+    Z2[e] += x;
+  }
+}
+
+void launch_ladder_unpack_blk(double *Z2, const double *S, const double *A,
+                              const LadderBlocks &L, cudaStream_t st) {
+  const long long total = (long long)L.o * L.o * L.v * L.v;
+  const long long nb = std::min<long long>((total + 255) / 256, 148 * 32);
+  k_ladder_unpack_blk<<<(unsigned)std::max(1LL, nb), 256, 0, st>>>(Z2, S, A, L);
+  count_launch();
+}
+
 }  // namespace acesb200

@@ -93,4 +93,24 @@ void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int
 void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
                           cudaStream_t st);
 
+// The same ladder on irrep blocks.  Virtual pairs are ordered by pair irrep g
+// (symmetric c <= d and antisymmetric c < d lists, block offsets offP/offM),
+// occupied pairs ij by their irrep (list ijs, offsets offIJ, local index ijl);
+// U+- are block-diagonal (block g: nP[g]^2 / nM[g]^2 doubles at offUp/offUm)
+// and a vector of symmetry hs couples the virtual pairs of irrep g with the
+// occupied pairs of irrep g ^ hs (tau blocks nIJ[g ^ hs] x nP[g] at offTp /
+// offTm, products S/A with the same sizes, column-major).
+struct LadderBlocks {
+  int nirrep, hs, o, v;
+  int nP[8], nM[8], nIJ[8], offP[9], offM[9], offIJ[9];
+  long long offUp[9], offUm[9], offTp[9], offTm[9];
+  const int *pp, *mm, *pidx, *midx, *ijs, *ijl, *irr_o, *irr_v;
+};
+void launch_ladder_pack_v_blk(double *Up, double *Um, const double *V, const LadderBlocks &L,
+                              cudaStream_t st);
+void launch_ladder_pack_tau_blk(double *tp, double *tm, const double *tau, const LadderBlocks &L,
+                                cudaStream_t st);
+void launch_ladder_unpack_blk(double *Z2, const double *S, const double *A,
+                              const LadderBlocks &L, cudaStream_t st);
+
 }  // namespace acesb200

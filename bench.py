@@ -514,6 +514,11 @@ def run_ours(a, rank, world, local_rank):
             line["lambda"] = lambda_block(lib, "c4conv", local_rank)
         except Exception as exc:  # noqa: BLE001
             line["lambda"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if prec == ab.PREC_BF16X3 and not a.no_lambda and a.workload == W_NAME:
+        try:
+            line["eom"] = eom_block(lib, "c2conv", local_rank)
+        except Exception as exc:  # noqa: BLE001
+            line["eom"] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(a.workload, budget_s=90.0)
@@ -690,6 +695,36 @@ def lambda_block(lib, wname, device, seed=4, delta=1e-4):
     out["lambda_speedup_bf16x3_vs_fp64"] = (out["fp64"]["lambda_seconds_per_iter"] /
                                             out["bf16x3"]["lambda_seconds_per_iter"])
     lib.fin()
+    return out
+
+
+def eom_block(lib, wname, device, nroots=2):
+    """Singlet EOM-EE-CCSD (xvee_run) on the convergent c2 system: the lowest
+    `nroots` excitation energies in split precision and in FP64, each after
+    its own CCSD (CC_CONV 9), with the Davidson's Jacobian-product count and
+    time per product (one reverse replay of the residual pass each)."""
+    import torch
+    import acesb200 as ab
+    from acesb200.workloads import WORKLOADS, synthetic_df
+    wl = WORKLOADS[wname]
+    eps, B, _ = synthetic_df(**wl)
+    o, v = wl["nocc"], wl["nvir"]
+    out = {"workload": f"{wname}: nocc={o}, nvir={v}, naux={wl['naux']}, seed={wl['seed']}, "
+                       f"B scaled by {wl['bscale']}", "nroots": nroots}
+    for prec, name in ((ab.PREC_BF16X3, "bf16x3"), (ab.PREC_FP64, "fp64")):
+        lib.init(device)
+        lib.sym_init([o], [v])
+        lib.putrec("SCFEVALA", eps)
+        lib.intprc_df(torch.from_numpy(B).to(torch.device("cuda", device)))
+        lib.xvcc(cc_conv=9, cc_maxcyc=80, cc_exporder=5, precision=prec)
+        cfg, w = lib.xvee([nroots], eom_conv=6, eom_maxcyc=60, precision=prec)
+        out[name] = {"omega": w[0], "iterations": cfg.niter[0], "products": cfg.nsigma,
+                     "seconds": cfg.seconds, "seconds_per_product": cfg.seconds / max(cfg.nsigma, 1)}
+    lib.fin()
+    out["max_abs_domega"] = max(abs(x - y) for x, y in zip(out["bf16x3"]["omega"],
+                                                           out["fp64"]["omega"]))
+    out["speedup_per_product"] = (out["fp64"]["seconds_per_product"] /
+                                  out["bf16x3"]["seconds_per_product"])
     return out
 
 
