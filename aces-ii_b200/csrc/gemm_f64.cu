@@ -2,8 +2,9 @@
 // (mma.sync.m8n8k4.f64): the plain-FP64 comparator of the engine and the
 // arithmetic of the reference's XGEMM -> DGEMM (tools/xgemm.F:10-49).
 //
-// Tile 128 x 128 x 16, 256 threads (8 warps as 2 x 4, each warp 64 x 32),
-// cp.async double buffering, padded shared-memory rows (20 doubles) so the
+// Tile 128 x 128 x 16, 256 threads (8 warps as 2 x 4, each warp 64 x 32), a
+// 4-stage cp.async pipeline (three k tiles in flight while one is computed,
+// one barrier per k tile), padded shared-memory rows (20 doubles) so the
 // fragment loads of a half-warp hit 32 distinct banks.
 #include <algorithm>
 
@@ -15,8 +16,10 @@ namespace acesb200 {
 namespace {
 constexpr int BM = 128, BN = 128, BK = 16, LDS = BK + 4;
 constexpr int kThreads = 256;
+constexpr int kStages = 4;
 constexpr int kStageDoubles = (BM + BN) * LDS;
-constexpr int kSmemBytes = 2 * kStageDoubles * 8;
+constexpr int kSmemBytes = kStages * kStageDoubles * 8;
+static_assert(kSmemBytes <= 227 * 1024, "pipeline depth");
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -34,6 +37,10 @@ __device__ __forceinline__ void cp_async(double *dst, const double *src, bool va
 
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -70,8 +77,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                   const double *__restrict__ B, long long ldb, double beta, CView C, int kchunk,
                   double *__restrict__ part) {
   extern __shared__ double smem[];
-  double *sA[2] = {smem, smem + kStageDoubles};
-  double *sB[2] = {smem + BM * LDS, smem + kStageDoubles + BM * LDS};
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
@@ -86,18 +91,27 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int kb = blockIdx.z * kchunk;
   const int ke = min(K, kb + kchunk);
   const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
-  if (nk > 0) load_stage<VEC>(sA[0], sB[0], A, lda, B, ldb, M, N, ke, m0, n0, kb);
-  cp_commit();
+  auto stA = [&](int s) { return smem + s * kStageDoubles; };
+  auto stB = [&](int s) { return smem + s * kStageDoubles + BM * LDS; };
+  // prologue: k tiles 0 .. kStages-2 in flight (one commit group each, empty
+  // groups past the end keep the count uniform)
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nk) load_stage<VEC>(stA(s), stB(s), A, lda, B, ldb, M, N, ke, m0, n0, kb + s * BK);
+    cp_commit();
+  }
   for (int kt = 0; kt < nk; ++kt) {
-    cp_wait0();
+    // group kt complete: at most kStages-2 younger groups still pending
+    cp_wait<kStages - 2>();
     __syncthreads();
-    if (kt + 1 < nk) {
-      load_stage<VEC>(sA[(kt + 1) & 1], sB[(kt + 1) & 1], A, lda, B, ldb, M, N, ke, m0, n0,
-                      kb + (kt + 1) * BK);
-      cp_commit();
-    }
-    const double *a_s = sA[kt & 1] + (wm * 64) * LDS;
-    const double *b_s = sB[kt & 1] + (wn * 32) * LDS;
+    // refill the slot computed in the previous iteration (every thread is past it)
+    const int nxt = kt + kStages - 1;
+    if (nxt < nk)
+      load_stage<VEC>(stA(nxt % kStages), stB(nxt % kStages), A, lda, B, ldb, M, N, ke, m0, n0,
+                      kb + nxt * BK);
+    cp_commit();
+    const double *a_s = stA(kt % kStages) + (wm * 64) * LDS;
+    const double *b_s = stB(kt % kStages) + (wn * 32) * LDS;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       double af[8], bf[4];
@@ -110,8 +124,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    __syncthreads();
   }
+  cp_wait0();
   if (part) {
     // split-K partial: dense [z][M][N]
     double *pz = part + (size_t)blockIdx.z * M * N;

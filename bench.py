@@ -261,6 +261,7 @@ def run_batch(a, rank=0, world=1, local_rank=0):
     rows = []
     tot = {"bf16x3": 0.0, "fp64": 0.0}
     flops_ladder = 0.0
+    flops_exec = 0.0
     for k, sysk in enumerate(systems):
         if k not in mine:
             continue
@@ -268,9 +269,18 @@ def run_batch(a, rank=0, world=1, local_rank=0):
         o, v = sysk["nocc"], sysk["nvir"]
         lib.init(local_rank)
         put_lists_dpd(lib, eps, B, irr, o, v, dev)
-        # particle-particle ladder flops summed over the irrep blocks
+        # particle-particle ladder flops summed over the irrep blocks (the
+        # reference's per-irrep LADAB1 products), and what the engine executes:
+        # the packed symmetric / antisymmetric pair blocks of every pair irrep
         flops_ladder += sum(2.0 * lib.irpdpd(h + 1, 13) ** 2 * lib.irpdpd(h + 1, 14)
                             for h in range(lib.nirrep))
+        io, iv = np.asarray(irr[:o]), np.asarray(irr[o:])
+        for g in range(lib.nirrep):
+            nij = int(np.sum((io[:, None] ^ io[None, :]) == g))
+            pg = (iv[:, None] ^ iv[None, :]) == g
+            npl = int(np.sum(np.triu(pg)))          # c <= d
+            nmi = int(np.sum(np.triu(pg, 1)))       # c < d
+            flops_exec += 2.0 * nij * (npl * npl + nmi * nmi)
         row = {"k": k, "nocc": o, "nvir": v}
         for prec, name in ((ab.PREC_BF16X3, "bf16x3"), (ab.PREC_FP64, "fp64")):
             c = lib.xvcc(cc_conv=7, cc_maxcyc=80, cc_exporder=5, precision=prec,
@@ -291,6 +301,7 @@ def run_batch(a, rank=0, world=1, local_rank=0):
         e_fp64 = gather_values({r["k"]: r["fp64"]["e"] for r in rows}, n, mine)
         dE = [abs(x - y) for x, y in zip(e_split, e_fp64)]
         flops_ladder = sum(gather_values({0: flops_ladder}, 1, [0]))
+        flops_exec = sum(gather_values({0: flops_exec}, 1, [0]))
         conv = allreduce_max(0.0 if conv else 1.0) == 0.0
         tot = {k_: allreduce_max(v_) for k_, v_ in tot.items()}
         if rank != 0:
@@ -309,6 +320,7 @@ def run_batch(a, rank=0, world=1, local_rank=0):
             "fp64_seconds": tot["fp64"], "speedup_split_vs_fp64": tot["fp64"] / tot["bf16x3"],
             "max_abs_dE": max(dE), "all_converged": conv,
             "ladder_flops_block_summed": flops_ladder,
+            "ladder_flops_executed_packed_blocks": flops_exec,
             "systems": rows if world == 1 else f"{len(rows)} of {len(systems)} on rank 0"}
     print(json.dumps(line), flush=True)
 
