@@ -23,7 +23,7 @@ CCEngine::~CCEngine() { release(); }
 std::vector<DBuf *> CCEngine::registry() {
   return {&eo, &ev, &foo, &fvv, &fov, &offo, &offv, &fovT, &I_oooo, &I_ooov, &I_oovv,
           &I_ovov, &I_ovvv, &I_vvvv, &L_oovv, &LF, &LovP, &LooP, &LmeP, &I1, &I2, &IvP,
-          &IvP2, &IX, &IX2, &WA0, &WB0, &IoP3, &IvT, &IvT2, &IooT, &LT1, &X, &Xn, &Z1,
+          &IvP2, &IX, &IX2, &WA0, &WB0, &IoP3, &IvT, &IooT, &LT1, &X, &Xn, &Z1,
           &Z2, &tau, &taut, &tautP, &tauT, &U, &Tp, &Tpp, &uT, &wP, &t2P, &Y1, &Y2, &XnP,
           &WA, &WB, &ZT, &XP, &Xmn, &Wmnij, &WmnT, &t1T, &Fae, &Fmi, &Fme, &Fp, &Fpp,
           &FmiT, &FppT, &FmeT, &tmp4, &scratch, &dev_small, &Bmat, &dvec, &L, &Ln, &gE,
@@ -59,6 +59,10 @@ void CCEngine::release() {
   }
   split_tmpA = SplitOperand();
   split_tmpB = SplitOperand();
+  for (auto &m : memo)
+    if (m.op.hi) dev_free(m.op.hi);
+  memo.clear();
+  memo_on = false;
   if (residual_exec) cudaGraphExecDestroy(residual_exec);
   residual_exec = nullptr;
   if (ev_lad0) cudaEventDestroy(ev_lad0);
@@ -98,7 +102,96 @@ int CCEngine::copy(double *dst, const double *src, size_t n) {
     if (is_active(src)) mark_active(dst);
     tape.push_back(op);
   }
+  memo_written(dst, (long long)n);
   if (n) ACES_CUDA(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, st));
+  return ACES_OK;
+}
+
+CCEngine::MemoEntry &CCEngine::memo_slot(const double *src, long long ld, int rows, int K) {
+  for (auto &m : memo)
+    if (m.src == src && m.ld == ld && m.rows == rows && m.K == K) return m;
+  memo.emplace_back();
+  MemoEntry &m = memo.back();
+  m.src = src;
+  m.ld = ld;
+  m.rows = rows;
+  m.K = K;
+  m.valid = m.fp64 = false;
+  return m;
+}
+
+// every entry whose FP64 source range overlaps [p, p + n) doubles
+void CCEngine::memo_written(const void *p, long long n) {
+  if (memo.empty()) return;
+  const char *lo = (const char *)p, *hi = lo + n * 8;
+  for (auto &m : memo) {
+    if (!m.valid) continue;
+    const char *a = (const char *)m.src;
+    const char *b = a + ((long long)(m.rows - 1) * m.ld + m.K) * 8;
+    if (a < hi && lo < b) m.valid = false;
+  }
+}
+
+// the elements of an M x N view: its extent from the largest offset of each
+// dimension ((i / div) * s1 + (i % div) * s0 over i < M or N; strides >= 0)
+void CCEngine::memo_written(const CView &C, int M, int N) {
+  if (memo.empty() || M <= 0 || N <= 0) return;
+  auto span = [](long long div, long long s1, long long s0, int n) {
+    if (s1 < 0 || s0 < 0) return -1LL;
+    if (div > 0x7fffffff) return (long long)(n - 1) * s0;
+    return (long long)((n - 1) / div) * s1 + std::min<long long>(n - 1, div - 1) * s0;
+  };
+  const long long sm = span(C.mdiv, C.sm1, C.sm0, M), sn = span(C.ndiv, C.sn1, C.sn0, N);
+  if (sm < 0 || sn < 0) {
+    for (auto &m : memo) m.valid = false;
+    return;
+  }
+  memo_written(C.p, sm + sn + 1);
+}
+
+bool CCEngine::fp64_missing(const double *p) const {
+  for (const auto &m : memo)
+    if (m.valid && !m.fp64 && m.src == p) return true;
+  return false;
+}
+
+bool CCEngine::splits(int M, int N, long long K) const {
+  return prec == ACES_PREC_BF16X3 && M >= 16 && N >= 16 && K >= 128 &&
+         (double)M * N * (double)K >= 1.0e8;
+}
+
+int CCEngine::perm_split(double *out, int rows, int K, bool consumer_splits, bool keep_fp64,
+                         int n0, int n1, int n2, int n3, std::initializer_list<PermTerm> terms) {
+  if (!memo_on || recording || !consumer_splits)
+    return perm(out, n0, n1, n2, n3, 0.0, terms);
+  PermSpec s;
+  s.n[0] = n0; s.n[1] = n1; s.n[2] = n2; s.n[3] = n3;
+  s.nterms = 0;
+  s.beta = 0.0;
+  for (const PermTerm &t : terms) s.t[s.nterms++] = t;
+  const long long total = (long long)n0 * n1 * n2 * n3;
+  if (total != (long long)rows * K) {
+    set_error("perm_split: %lld outputs are not %d rows of %d", total, rows, K);
+    return ACES_ERR_ARG;
+  }
+  memo_written(out, total);
+  MemoEntry &m = memo_slot(out, K, rows, K);
+  const int kp = (K + kSplitKPad - 1) / kSplitKPad * kSplitKPad;
+  const size_t need = (size_t)rows * kp * 2 * 2;
+  if (!m.op.hi || m.op.cap < need) {
+    if (m.op.hi) dev_free(m.op.hi);
+    m.op = SplitOperand();
+    ACES_CUDA(dev_alloc(&m.op.hi, need));
+    m.op.cap = need;
+    ACES_CUDA(cudaMemsetAsync(m.op.hi, 0, need, st));  // the K padding stays zero
+  }
+  m.op.rows = m.op.rows_pad = rows;
+  m.op.k = K;
+  m.op.k_pad = kp;
+  m.op.lo = (char *)m.op.hi + (size_t)rows * kp * 2;
+  ACES_TRY(permute_split(keep_fp64 ? out : nullptr, m.op.hi, m.op.lo, K, kp, s, st));
+  m.valid = true;
+  m.fp64 = keep_fp64;
   return ACES_OK;
 }
 
@@ -113,6 +206,7 @@ int CCEngine::tau_op(double *out, const double *t2v, const double *t1v, double c
     mark_active(out);
     tape.push_back(op);
   }
+  memo_written(out, (long long)o * o * v * v);
   launch_tau(out, t2v, t1v, c, o, v, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -138,6 +232,7 @@ int CCEngine::perm(double *out, int n0, int n1, int n2, int n3, double beta,
     if (any) mark_active(out);
     tape.push_back(op);
   }
+  memo_written(out, (long long)n0 * n1 * n2 * n3);
   return permute(out, s, st);
 }
 
@@ -167,15 +262,19 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
     if (op.a_act || op.b_act) mark_active(C.p);
     tape.push_back(op);
   }
-  // matrix-vector products are bandwidth bound: FP64 GEMV
-  if (N == 1) return gemv_f64(M, K, alpha, A, lda, B, beta, C, false, st);
-  if (M == 1) return gemv_f64(N, K, alpha, B, ldb, A, beta, C, true, st);
+  memo_written(C, M, N);
   // the tensor-core split path: every contraction with K >= 128 and both
   // output dimensions >= 16 (a thin dimension such as nocc is padded to the
   // 128-row tile: the BF16 tensor cores still beat FP64 FMA several-fold);
   // K = nocc products (low-rank updates) stay on the FP64 kernels
-  bool split = prec == ACES_PREC_BF16X3 && M >= 16 && N >= 16 && K >= 128 &&
-               (double)M * N * K >= 1.0e8;
+  const bool split = splits(M, N, K);
+  if (!split && (fp64_missing(A) || fp64_missing(B))) {
+    set_error("contraction %d x %d x %d reads an operand held only as split planes", M, N, K);
+    return ACES_ERR_ARG;
+  }
+  // matrix-vector products are bandwidth bound: FP64 GEMV
+  if (N == 1) return gemv_f64(M, K, alpha, A, lda, B, beta, C, false, st);
+  if (M == 1) return gemv_f64(N, K, alpha, B, ldb, A, beta, C, true, st);
   if (!split) return gemm_nt_f64(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
   // the tensor-core epilogue gives each thread one output row m (consecutive
   // lanes: consecutive m); an output whose unit stride runs along n is
@@ -196,6 +295,15 @@ int CCEngine::G(int M, int N, int K, double alpha, const double *A, long long ld
 
 int CCEngine::split_get(const double *src, long long ld, int rows, int K, bool cst,
                         SplitOperand &tmp, const SplitOperand **out) {
+  if (memo_on && !cst) {
+    MemoEntry &m = memo_slot(src, ld, rows, K);
+    if (!m.valid) {
+      ACES_TRY(split_pack(m.op, src, ld, rows, K, st));
+      m.valid = m.fp64 = true;
+    }
+    *out = &m.op;
+    return ACES_OK;
+  }
   if (cst) {
     for (auto &e : split_cache)
       if (e.src == src && e.op.rows == rows && e.op.k == K) {
@@ -216,9 +324,7 @@ int CCEngine::split_get(const double *src, long long ld, int rows, int K, bool c
 
 int CCEngine::Ggroup(const GArgs *g, int n, double beta) {
   bool grouped = prec == ACES_PREC_BF16X3 && !recording && n >= 2 && n <= 3;
-  for (int i = 0; i < n && grouped; ++i)
-    grouped = g[i].M >= 16 && g[i].N >= 16 && g[i].K >= 128 &&
-              (double)g[i].M * g[i].N * g[i].K >= 1.0e8;
+  for (int i = 0; i < n && grouped; ++i) grouped = splits(g[i].M, g[i].N, g[i].K);
   if (!grouped) {
     for (int i = 0; i < n; ++i)
       ACES_TRY(G(g[i].M, g[i].N, g[i].K, 1.0, g[i].A, g[i].lda, g[i].B, g[i].ldb, beta, g[i].C,
@@ -227,6 +333,7 @@ int CCEngine::Ggroup(const GArgs *g, int n, double beta) {
   }
   const SplitOperand *sa[3], *sb[3];
   GroupedProblem pr[3];
+  for (int i = 0; i < n; ++i) memo_written(g[i].C, g[i].M, g[i].N);
   for (int i = 0; i < n; ++i) {
     GArgs q = g[i];
     gemm_calls++;
@@ -251,16 +358,15 @@ int CCEngine::Ggroup(const GArgs *g, int n, double beta) {
 }
 
 int CCEngine::Gmulti(int M, int N, const Seg *sg, int nseg, double beta, const CView &C) {
-  bool fused = prec == ACES_PREC_BF16X3 && !recording && nseg >= 2 && nseg <= 3 && M >= 16 &&
-               N >= 16;
-  for (int i = 0; i < nseg && fused; ++i)
-    fused = sg[i].K >= 128 && (double)M * N * sg[i].K >= 1.0e8;
+  bool fused = prec == ACES_PREC_BF16X3 && !recording && nseg >= 2 && nseg <= 3;
+  for (int i = 0; i < nseg && fused; ++i) fused = splits(M, N, sg[i].K);
   if (!fused) {
     for (int i = 0; i < nseg; ++i)
       ACES_TRY(G(M, N, sg[i].K, 1.0, sg[i].A, sg[i].lda, sg[i].B, sg[i].ldb,
                  i == 0 ? beta : 1.0, C, sg[i].constA, sg[i].constB));
     return ACES_OK;
   }
+  memo_written(C, M, N);
   // coalescing orientation as in G: C^T = B A^T when the output's unit stride runs along n
   CView Cv = C;
   const bool swap = C.sm0 != 1 && C.sn0 == 1;
@@ -589,11 +695,9 @@ int CCEngine::setup_intermediates() {
   // IoP3[i,j,b,m] = I_ooov[i,j,m,b]
   ACES_TRY(alloc(IoP3, OOOV));
   ACES_TRY(perm(IoP3.p, o, o, v, o, 0.0, {PT(I_ooov.p, 1.0, s3[0], s3[1], s3[3], s3[2])}));
-  // IvT[j,a,b,e] = I_ovvv[j,e,b,a]; IvT2[a,m,e,f] = I_ovvv[m,a,e,f]
+  // IvT[j,a,b,e] = I_ovvv[j,e,b,a]
   ACES_TRY(alloc(IvT, OVVV));
   ACES_TRY(perm(IvT.p, o, v, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[0], sv[3], sv[2], sv[1])}));
-  ACES_TRY(alloc(IvT2, OVVV));
-  ACES_TRY(perm(IvT2.p, v, o, v, v, 0.0, {PT(I_ovvv.p, 1.0, sv[1], sv[0], sv[2], sv[3])}));
   // IooT[i,m,n,e] = I_ooov[m,n,i,e]
   ACES_TRY(alloc(IooT, OOOV));
   ACES_TRY(perm(IooT.p, o, o, o, v, 0.0, {PT(I_ooov.p, 1.0, s3[2], s3[0], s3[1], s3[3])}));
@@ -685,6 +789,20 @@ int CCEngine::mp2_guess() {
 // the residual of one CCSD iteration: Z1, Z2 from X = [t1 | t2]
 // ---------------------------------------------------------------------------
 int CCEngine::residual() {
+  // split planes of the pass's non-constant operands are shared between its
+  // contractions (and written by the resorts that produce them) only inside
+  // this pass; every entry starts invalid
+  for (auto &m : memo) m.valid = false;
+  struct MemoScope {
+    CCEngine &E;
+    explicit MemoScope(CCEngine &e) : E(e) {
+      E.memo_on = !E.recording && E.prec == ACES_PREC_BF16X3;
+    }
+    ~MemoScope() {
+      E.memo_on = false;
+      for (auto &m : E.memo) m.valid = false;
+    }
+  } memo_scope(*this);
   const long long O = o, V = v;
   const long long OV = O * V, VV = V * V, OO = O * O, OVV = O * V * V, OOV = O * O * V;
   double *T1 = t1(), *T2 = t2();
@@ -699,7 +817,8 @@ int CCEngine::residual() {
   ACES_TRY(G(v, v, o, -0.5, t1T.p, O, fovT.p, O, 1.0, cview_rowmajor(Fae.p, V)));
   ACES_TRY(G(v * v, 1, o * v, 1.0, LF.p, OV, T1, OV, 1.0, cview_rowmajor(Fae.p, 1), true));
   // tautP[a,m,n,f] = taut[m,n,a,f]
-  ACES_TRY(perm(tautP.p, v, o, o, v, 0.0, {PT(taut.p, 1.0, st2[2], st2[0], st2[1], st2[3])}));
+  ACES_TRY(perm_split(tautP.p, v, o * o * v, splits(v, v, OOV), false, v, o, o, v,
+                      {PT(taut.p, 1.0, st2[2], st2[0], st2[1], st2[3])}));
   ACES_TRY(G(v, v, o * o * v, -1.0, tautP.p, OOV, LovP.p, OOV, 1.0, cview_rowmajor(Fae.p, V),
              false, true));
   // ---- F(mi): QUAD2 + T1INW2 (vcc/quad2.f, vcc/t1inw2.f) ----
@@ -725,20 +844,21 @@ int CCEngine::residual() {
   ACES_TRY(G(o, v, v, 1.0, T1, V, Fae.p, V, 1.0, cview_rowmajor(Z1.p, V)));
   ACES_TRY(G(o, v, o, -1.0, FmiT.p, O, t1T.p, O, 1.0, cview_rowmajor(Z1.p, V)));
   // U[i,a,m,e] = 2 t2[i,m,a,e] - t2[m,i,a,e]
-  ACES_TRY(perm(U.p, o, v, o, v, 0.0,
-                {PT(T2, 2.0, st2[0], st2[2], st2[1], st2[3]),
-                 PT(T2, -1.0, st2[1], st2[2], st2[0], st2[3])}));
+  ACES_TRY(perm_split(U.p, o * v, o * v, splits(o * v, o * v, OV), true, o, v, o, v,
+                      {PT(T2, 2.0, st2[0], st2[2], st2[1], st2[3]),
+                       PT(T2, -1.0, st2[1], st2[2], st2[0], st2[3])}));
   ACES_TRY(G(o * v, 1, o * v, 1.0, U.p, OV, Fme.p, OV, 1.0, cview_rowmajor(Z1.p, 1)));
   ACES_TRY(G(o * v, 1, o * v, 1.0, LT1.p, OV, T1, OV, 1.0, cview_rowmajor(Z1.p, 1), true));
-  // T2T1AB1: wP[i,m,e,f] = 2 t2[i,m,f,e] - t2[i,m,e,f];  Z1[i,a] += sum IvT2[a,(mef)] wP[i,(mef)]
-  ACES_TRY(perm(wP.p, o, o, v, v, 0.0,
-                {PT(T2, 2.0, st2[0], st2[1], st2[3], st2[2]),
-                 PT(T2, -1.0, st2[0], st2[1], st2[2], st2[3])}));
-  ACES_TRY(G(v, o, o * v * v, 1.0, IvT2.p, OVV, wP.p, OVV, 1.0, cview_colmajor(Z1.p, V), true));
+  // T2T1AB1: wP[i,m,e,f] = 2 t2[i,m,f,e] - t2[i,m,e,f];  Z1[i,a] += sum IvP[a,(mef)] wP[i,(mef)]
+  // (IvP[a,m,e,f] = <ma|ef>)
+  ACES_TRY(perm_split(wP.p, o, o * v * v, splits(v, o, OVV), false, o, o, v, v,
+                      {PT(T2, 2.0, st2[0], st2[1], st2[3], st2[2]),
+                       PT(T2, -1.0, st2[0], st2[1], st2[2], st2[3])}));
+  ACES_TRY(G(v, o, o * v * v, 1.0, IvP.p, OVV, wP.p, OVV, 1.0, cview_colmajor(Z1.p, V), true));
   // T2T1AB2: uT[a,m,n,e] = 2 t2[m,n,a,e] - t2[n,m,a,e];  Z1[i,a] -= sum uT[a,(mne)] IooT[i,(mne)]
-  ACES_TRY(perm(uT.p, v, o, o, v, 0.0,
-                {PT(T2, 2.0, st2[2], st2[0], st2[1], st2[3]),
-                 PT(T2, -1.0, st2[2], st2[1], st2[0], st2[3])}));
+  ACES_TRY(perm_split(uT.p, v, o * o * v, splits(v, o, OOV), false, v, o, o, v,
+                      {PT(T2, 2.0, st2[2], st2[0], st2[1], st2[3]),
+                       PT(T2, -1.0, st2[2], st2[1], st2[0], st2[3])}));
   ACES_TRY(G(v, o, o * o * v, -1.0, uT.p, OOV, IooT.p, OOV, 1.0, cview_colmajor(Z1.p, V), false,
              true));
 
@@ -755,7 +875,8 @@ int CCEngine::residual() {
   // INITIN: Z2 <- <ij|ab>
   ACES_TRY(copy(Z2.p, I_oovv.p, (size_t)OO * VV));
   // tauT[a,b,m,n] = tau[m,n,a,b]
-  ACES_TRY(perm(tauT.p, v, v, o, o, 0.0, {PT(tau.p, 1.0, st2[2], st2[3], st2[0], st2[1])}));
+  ACES_TRY(perm_split(tauT.p, v * v, o * o, splits(v * v, o * o, OO), false, v, v, o, o,
+                      {PT(tau.p, 1.0, st2[2], st2[3], st2[0], st2[1])}));
   ACES_TRY(G(v * v, o * o, o * o, 1.0, tauT.p, OO, WmnT.p, OO, 1.0, cview_colmajor(Z2.p, VV)));
   // ---- particle-particle ladder (DRLAD ITYPE=6, vcc/ladab1.F:61) ----
   if (!ev_lad0) {
@@ -791,7 +912,8 @@ int CCEngine::residual() {
   CView vWn{WA.p, kHuge, 0, OV, OV, OVV, 1};
   ACES_TRY(G(v, o * o * v, o, -1.0, t1T.p, O, IX.p, O, 1.0, vWn, false, true));
   // Y2[j,b,n,f] = t2[n,j,f,b];  XnP[j,b,n,f] = 1/2 t2[j,n,f,b] + t1[j,f] t1[n,b]; Y1 = Y2 - XnP
-  ACES_TRY(perm(Y2.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[1], st2[3], st2[0], st2[2])}));
+  ACES_TRY(perm_split(Y2.p, o * v, o * v, splits(o * v, o * v, OV), false, o, v, o, v,
+                      {PT(T2, 1.0, st2[1], st2[3], st2[0], st2[2])}));
   ACES_TRY(perm(XnP.p, o, v, o, v, 0.0, {PT(T2, 0.5, st2[0], st2[3], st2[1], st2[2])}));
   // + t1[j,f] t1[n,b]: rank-1 per (j,b,n,f) -> GEMM over a unit K: A[(j),f]... use outer product
   {
@@ -820,10 +942,12 @@ int CCEngine::residual() {
   CView vfm{XP.p, VV, OVV, 1, kHuge, 0, VV};
   ACES_TRY(G(o * v * v, o, o, -1.0, t2P.p, O, FppT.p, O, 1.0, vfm));
   // ZT[i,j,b,m] = <mb|ij> + sum_ef <mb|ef> tau(ij,ef) + sum_e <mb|ej> t(ie) + sum_e <mb|ie> t(je)
-  // (T1INT2A, T1INW1, T12INT2), then XP -= sum_m t(ma) ZT[(ijb), m]
+  // (T1INT2A, T1INW1, T12INT2), then XP -= sum_m t(ma) ZT[(ijb), m].  The
+  // tau product runs over the rows (b, m) of IvP[b,m,e,f] = <mb|ef>, the
+  // order of ZT's (b, m): unit stride along the product's rows.
   ACES_TRY(copy(ZT.p, IoP3.p, (size_t)OOV * O));
-  CView vz1{ZT.p, V, 1, O, kHuge, 0, V * O};
-  ACES_TRY(G(o * v, o * o, v * v, 1.0, I_ovvv.p, VV, tau.p, VV, 1.0, vz1, true));
+  ACES_TRY(G(o * v, o * o, v * v, 1.0, IvP.p, VV, tau.p, VV, 1.0, cview_colmajor(ZT.p, OV),
+             true));
   ACES_TRY(G(o * v * o, o, v, 1.0, WA0.p, V, T1, V, 1.0, cview_colmajor(ZT.p, OOV), true));
   CView vz3{ZT.p, V * O, OOV, 1, kHuge, 0, V * O};
   ACES_TRY(G(o * v * o, o, v, -1.0, WB0.p, V, T1, V, 1.0, vz3, true));
@@ -832,8 +956,10 @@ int CCEngine::residual() {
   // T1INT2B (vcc/t1int2b.f)
   ACES_TRY(G(o, o * v * v, v, 1.0, T1, V, IvT.p, V, 1.0, cview_rowmajor(XP.p, OVV), false, true));
   // ring (DRRNG/RNGDRV, vcc/rngdrv.f): Tp[i,a,m,e] = t2[i,m,a,e]; Tpp[j,a,m,e] = t2[j,m,e,a]
-  ACES_TRY(perm(Tp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[2], st2[1], st2[3])}));
-  ACES_TRY(perm(Tpp.p, o, v, o, v, 0.0, {PT(T2, 1.0, st2[0], st2[3], st2[1], st2[2])}));
+  ACES_TRY(perm_split(Tp.p, o * v, o * v, splits(o * v, o * v, OV), false, o, v, o, v,
+                      {PT(T2, 1.0, st2[0], st2[2], st2[1], st2[3])}));
+  ACES_TRY(perm_split(Tpp.p, o * v, o * v, splits(o * v, o * v, OV), false, o, v, o, v,
+                      {PT(T2, 1.0, st2[0], st2[3], st2[1], st2[2])}));
   CView vr1{XP.p, V, OVV, V, V, VV, 1};
   {
     const Seg sgr[2] = {{U.p, OV, WA.p, OV, o * v, false, false},
@@ -941,6 +1067,8 @@ int CCEngine::ladder_packed_blocks(const double *in, double *out) {
   ACES_TRY(alloc(taum, (size_t)std::max(1LL, Lb.offTm[nir])));
   ACES_TRY(alloc(Sld, (size_t)std::max(1LL, Lb.offTp[nir])));
   ACES_TRY(alloc(Ald, (size_t)std::max(1LL, Lb.offTm[nir])));
+  memo_written(taup.p, std::max(1LL, Lb.offTp[nir]));
+  memo_written(taum.p, std::max(1LL, Lb.offTm[nir]));
   launch_ladder_pack_tau_blk(taup.p, taum.p, in, Lb, st);
   // block products S_g = U+_g tau+_g^T, A_g = U-_g tau-_g^T, three per grouped launch
   std::vector<GArgs> probs;
@@ -961,6 +1089,7 @@ int CCEngine::ladder_packed_blocks(const double *in, double *out) {
   });
   for (size_t q = 0; q < probs.size(); q += 3)
     ACES_TRY(Ggroup(probs.data() + q, (int)std::min<size_t>(3, probs.size() - q), 0.0));
+  memo_written(out, (long long)o * o * v * v);
   launch_ladder_unpack_blk(out, Sld.p, Ald.p, Lb, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -995,11 +1124,14 @@ int CCEngine::ladder_packed(const double *in, double *out) {
   ACES_TRY(alloc(taum, (size_t)oo * std::max(nm, 1)));
   ACES_TRY(alloc(Sld, (size_t)oo * np));
   ACES_TRY(alloc(Ald, (size_t)oo * std::max(nm, 1)));
+  memo_written(taup.p, (long long)oo * np);
+  memo_written(taum.p, (long long)oo * std::max(nm, 1));
   launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st);
   // both products in one grouped launch (their tiles fill each other's last wave)
   const GArgs g[2] = {{np, oo, np, Up.p, np, taup.p, np, cview_colmajor(Sld.p, np), true, false},
                       {nm, oo, nm, Um.p, nm, taum.p, nm, cview_colmajor(Ald.p, nm), true, false}};
   ACES_TRY(Ggroup(g, nm > 0 ? 2 : 1, 0.0));
+  memo_written(out, (long long)o * o * v * v);
   launch_ladder_unpack(out, Sld.p, Ald.p, v, oo, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -1116,8 +1248,7 @@ int CCEngine::iteration(int icycle, int exporder, double *e3, double *res, doubl
   std::vector<const double *> pe(ndimr);
   for (int k = 0; k < ndimr; ++k) pe[k] = he[k].p;
   ACES_TRY(alloc(dvec, len));
-  launch_lincomb(dvec.p, nullptr, d + 40, pe.data(), ndimr, len, st);
-  launch_absmax(d + 4, dvec.p, o, v, scratch.p, st);
+  launch_lincomb_absmax(dvec.p, d + 40, pe.data(), ndimr, o, v, scratch.p, d + 4, st);
   int hstat = 0;
   ACES_CUDA(cudaMemcpyAsync(&hstat, status, 4, cudaMemcpyDeviceToHost, st));
   ACES_CUDA(cudaMemcpyAsync(dres, d + 4, 8, cudaMemcpyDeviceToHost, st));

@@ -47,7 +47,7 @@ class CCEngine {
   // integrals (dense, physicists' notation)
   DBuf I_oooo, I_ooov, I_oovv, I_ovov, I_ovvv, I_vvvv;
   // precomputed resorted integrals
-  DBuf L_oovv, LF, LovP, LooP, LmeP, I1, I2, IvP, IvP2, IX, IX2, WA0, WB0, IoP3, IvT, IvT2,
+  DBuf L_oovv, LF, LovP, LooP, LmeP, I1, I2, IvP, IvP2, IX, IX2, WA0, WB0, IoP3, IvT,
       IooT, LT1;
   DBuf Ic, I1n;  // I1 - I2/2 and -I1 (the W(mbej) ring intermediates' integrals)
 
@@ -85,6 +85,34 @@ class CCEngine {
   // split operand of src (rows x K, leading dimension ld): cached when cst
   int split_get(const double *src, long long ld, int rows, int K, bool cst, SplitOperand &tmp,
                 const SplitOperand **out);
+  // Split planes of non-constant operands within one residual pass (memo_on):
+  // the resorted amplitudes that permute_split writes straight into planes,
+  // and every operand split once and read again by a later contraction of the
+  // pass.  An entry stays valid until its source range is written again (the
+  // engine's writers report every write through memo_written); fp64 = false
+  // marks planes whose FP64 source was never written.  Entries keep their
+  // planes (and addresses) across passes, so a captured residual graph
+  // replays the same buffers.
+  struct MemoEntry {
+    const double *src;
+    long long ld;
+    int rows, K;
+    bool valid, fp64;
+    SplitOperand op;
+  };
+  std::deque<MemoEntry> memo;
+  bool memo_on = false;
+  MemoEntry &memo_slot(const double *src, long long ld, int rows, int K);
+  void memo_written(const void *p, long long n);
+  void memo_written(const CView &C, int M, int N);
+  bool fp64_missing(const double *p) const;
+  // the dispatch rule of G: does an M x N x K contraction take the split path
+  bool splits(int M, int N, long long K) const;
+  // perm (beta = 0) whose output is one contraction operand of rows x K
+  // (K-contiguous): with memo_on and a consumer that splits, the planes are
+  // written by the resort itself, plus the FP64 output only when keep_fp64
+  int perm_split(double *out, int rows, int K, bool consumer_splits, bool keep_fp64, int n0,
+                 int n1, int n2, int n3, std::initializer_list<PermTerm> terms);
   // several contractions C_g = A_g B_g^T + beta C_g in one grouped tensor-core
   // launch when all take the split path (else one G call each)
   struct GArgs {

@@ -11,6 +11,9 @@
 //   &C[m,n] = p + (m / mdiv)*sm1 + (m % mdiv)*sm0 + (n / ndiv)*sn1 + (n % ndiv)*sn0
 #pragma once
 #include <cuda_runtime.h>
+#ifdef __CUDACC__
+#include <cuda_bf16.h>
+#endif
 
 namespace acesb200 {
 
@@ -106,6 +109,16 @@ struct SplitOperand {
 
 // K padding of split operands (the tcgen05 kernel's k tile)
 constexpr int kSplitKPad = 64;
+
+#ifdef __CUDACC__
+// the two BF16 planes of one FP64 value: hi = bf16(x) (round to nearest even
+// through FP32), lo = bf16(x - hi); every producer of split operands uses it,
+// so a fused resort and split_pack give bit-identical planes
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &h, __nv_bfloat16 &l) {
+  h = __float2bfloat16_rn((float)x);
+  l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+}
+#endif
 
 // Fill a split operand from an FP64 K-contiguous matrix (src[r*ld + k]).
 int split_pack(SplitOperand &op, const double *src, long long ld, int rows, int k, cudaStream_t st);

@@ -176,16 +176,37 @@ __global__ void __launch_bounds__(kThreads, 1)
 }  // namespace
 
 // C = alpha * sum_z part[z] + beta * C
-// part[z][m][n] (mfast false) or part[z][n][m] (mfast true)
+// part[z][m][n] (mfast false) or part[z][n][m] (mfast true); the slices are
+// summed in order z = 0, 1, ... with four of them loaded at a time.  Wide =
+// false: M * N below 2^31, the index split with FastDiv (fd: M if mfast, else N).
+template <bool Wide>
 __global__ void k_splitk_reduce(CView C, const double *__restrict__ part, int M, int N, int Z,
-                                double alpha, double beta, bool mfast) {
-  long long total = (long long)M * N;
+                                double alpha, double beta, bool mfast, FastDiv fd) {
+  const long long total = (long long)M * N;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    int m = mfast ? (int)(idx % M) : (int)(idx / N);
-    int n = mfast ? (int)(idx / M) : (int)(idx % N);
+    int m, n;
+    if (Wide) {
+      m = mfast ? (int)(idx % M) : (int)(idx / N);
+      n = mfast ? (int)(idx / M) : (int)(idx % N);
+    } else {
+      const unsigned q = fd.div((unsigned)idx), r = (unsigned)idx - q * fd.d;
+      m = mfast ? (int)r : (int)q;
+      n = mfast ? (int)q : (int)r;
+    }
+    const double *pz = part + idx;
     double s = 0.0;
-    for (int z = 0; z < Z; ++z) s += part[(size_t)z * total + idx];
+    int z = 0;
+    for (; z + 4 <= Z; z += 4) {
+      const double a0 = __ldg(pz), a1 = __ldg(pz + total), a2 = __ldg(pz + 2 * total),
+                   a3 = __ldg(pz + 3 * total);
+      s += a0;
+      s += a1;
+      s += a2;
+      s += a3;
+      pz += 4 * total;
+    }
+    for (; z < Z; ++z, pz += total) s += __ldg(pz);
     double *cp = C.p + cview_off(C, m, n);
     double r = alpha * s;
     if (beta != 0.0) r += beta * *cp;
@@ -489,7 +510,11 @@ int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, doubl
   }
   long long nb = (total + 255) / 256;
   if (nb > 148 * 16) nb = 148 * 16;
-  k_splitk_reduce<<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, mfast);
+  const FastDiv fd((unsigned)std::max(1, mfast ? M : N));
+  if (total < (1LL << 31))
+    k_splitk_reduce<false><<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, mfast, fd);
+  else
+    k_splitk_reduce<true><<<(unsigned)nb, 256, 0, st>>>(C, part, M, N, Z, alpha, beta, mfast, fd);
   count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;

@@ -53,11 +53,11 @@ __global__ void k_split_pack(__nv_bfloat162 *__restrict__ hi, __nv_bfloat162 *__
     }
     const double *row = src + r * ld;
     const double x0 = c < k ? row[c] : 0.0, x1 = c + 1 < k ? row[c + 1] : 0.0;
-    const __nv_bfloat16 h0 = __float2bfloat16_rn((float)x0), h1 = __float2bfloat16_rn((float)x1);
-    const float r0 = (float)(x0 - (double)__bfloat162float(h0));
-    const float r1 = (float)(x1 - (double)__bfloat162float(h1));
+    __nv_bfloat16 h0, l0, h1, l1;
+    split_bf16(x0, h0, l0);
+    split_bf16(x1, h1, l1);
     hi[idx] = __halves2bfloat162(h0, h1);
-    lo[idx] = __halves2bfloat162(__float2bfloat16_rn(r0), __float2bfloat16_rn(r1));
+    lo[idx] = __halves2bfloat162(l0, l1);
   }
 }
 

@@ -4,6 +4,7 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "gemm.cuh"
 #include "kernels.cuh"
 
 namespace acesb200 {
@@ -21,9 +22,35 @@ struct PermArgs {
   FastDiv fd1, fd2, fd3;  // divisors n[1], n[2], n[3]
 };
 
-// Wide = false: element count below 2^31, indices split with FastDiv.
-template <bool Wide>
-__global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long total) {
+// two BF16 values as one 32-bit word, the first at the lower address
+__device__ __forceinline__ unsigned pack_bf16x2(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16);
+}
+
+// Optional BF16 split planes of a resort's output, read as a rows x K
+// K-contiguous contraction operand: output element idx (below 2^31) is
+// operand element (r, c) = (idx / K, idx % K), stored at r * k_pad + c of
+// both planes (the K padding is zero from the planes' allocation).
+struct SplitOut {
+  __nv_bfloat16 *hi = nullptr, *lo = nullptr;
+  int k_pad = 0;
+  FastDiv fk;  // divisor K
+};
+
+__device__ __forceinline__ void put_split(const SplitOut &so, long long idx, double x) {
+  const unsigned r = so.fk.div((unsigned)idx);
+  const long long p = (long long)r * so.k_pad + ((unsigned)idx - r * so.fk.d);
+  __nv_bfloat16 h, l;
+  split_bf16(x, h, l);
+  so.hi[p] = h;
+  so.lo[p] = l;
+}
+
+// Wide = false: element count below 2^31, indices split with FastDiv.  S:
+// the output also goes to split planes (out may then be null: no FP64 copy).
+template <bool Wide, bool S>
+__global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long total,
+                                SplitOut so) {
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     int i0, i1, i2, i3;
@@ -44,15 +71,19 @@ __global__ void k_permute_naive(double *__restrict__ out, PermArgs a, long long 
     for (int t = 0; t < a.nterms; ++t)
       acc += a.alpha[t] * __ldg(a.src[t] + i0 * a.s[t][0] + i1 * a.s[t][1] + i2 * a.s[t][2] +
                                 i3 * a.s[t][3]);
-    out[idx] = acc;
+    if (!S || out) out[idx] = acc;
+    if (S) put_split(so, idx, acc);
   }
 }
 
 // The gather of k_permute_naive for outputs whose innermost extent is a
 // multiple of 4 (every source has unit stride along it): a thread owns 4
 // consecutive outputs of one row, splits its index once and issues 4
-// independent loads per term and two 16-byte stores.
-__global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long quads) {
+// independent loads per term and two 16-byte stores (with S and K % 4 == 0,
+// one 8-byte store per split plane).
+template <bool S>
+__global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long quads,
+                                SplitOut so) {
   for (long long qd = blockIdx.x * (long long)blockDim.x + threadIdx.x; qd < quads;
        qd += (long long)gridDim.x * blockDim.x) {
     const long long idx = qd * 4;
@@ -78,15 +109,34 @@ __global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long 
 #pragma unroll
       for (int u = 0; u < 4; ++u) acc[u] += a.alpha[t] * x[u];
     }
-    *reinterpret_cast<double2 *>(out + idx) = make_double2(acc[0], acc[1]);
-    *reinterpret_cast<double2 *>(out + idx + 2) = make_double2(acc[2], acc[3]);
+    if (!S || out) {
+      *reinterpret_cast<double2 *>(out + idx) = make_double2(acc[0], acc[1]);
+      *reinterpret_cast<double2 *>(out + idx + 2) = make_double2(acc[2], acc[3]);
+    }
+    if (S) {
+      if ((so.fk.d & 3u) == 0) {  // the 4 outputs are one aligned run of an operand row
+        const unsigned rr = so.fk.div((unsigned)idx);
+        const long long p = (long long)rr * so.k_pad + ((unsigned)idx - rr * so.fk.d);
+        __nv_bfloat16 h[4], l[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) split_bf16(acc[u], h[u], l[u]);
+        *reinterpret_cast<uint2 *>(so.hi + p) =
+            make_uint2(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]));
+        *reinterpret_cast<uint2 *>(so.lo + p) =
+            make_uint2(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]));
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) put_split(so, idx + u, acc[u]);
+      }
+    }
   }
 }
 
 // 32x32 shared-memory tiles over (i3, i_d) where every term reads i_d with
 // unit stride: reads coalesced along i_d, writes coalesced along i3.
-template <int D>
-__global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out, PermArgs a) {
+template <int D, bool S>
+__global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out, PermArgs a,
+                                                       SplitOut so) {
   __shared__ double tile[32][33];
   const int nd = a.n[D];
   const int t3 = (a.n[3] + 31) / 32, td = (nd + 31) / 32;
@@ -127,29 +177,16 @@ __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out,
       int idx_[4];
       idx_[3] = i3; idx_[D] = id; idx_[o0] = io0; idx_[o1] = io1;
       long long o = (((long long)idx_[0] * a.n[1] + idx_[1]) * a.n[2] + idx_[2]) * a.n[3] + idx_[3];
-      out[o] = (a.beta == 0.0 ? 0.0 : a.beta * out[o]) + acc[k];
+      const double val = (a.beta == 0.0 ? 0.0 : a.beta * out[o]) + acc[k];
+      if (!S || out) out[o] = val;
+      if (S) put_split(so, o, val);
     }
   }
 }
 
-int permute(double *out, const PermSpec &spec, cudaStream_t st) {
-  PermArgs a;
-  long long total = 1;
-  for (int k = 0; k < 4; ++k) {
-    a.n[k] = spec.n[k];
-    total *= spec.n[k];
-  }
-  if (total == 0) return ACES_OK;
-  a.nterms = spec.nterms;
-  a.beta = spec.beta;
-  a.fd1 = FastDiv((unsigned)a.n[1]);
-  a.fd2 = FastDiv((unsigned)a.n[2]);
-  a.fd3 = FastDiv((unsigned)a.n[3]);
-  for (int t = 0; t < 4; ++t) {
-    a.src[t] = t < spec.nterms ? spec.t[t].src : nullptr;
-    a.alpha[t] = t < spec.nterms ? spec.t[t].alpha : 0.0;
-    for (int k = 0; k < 4; ++k) a.s[t][k] = t < spec.nterms ? spec.t[t].s[k] : 0;
-  }
+template <bool S>
+static void permute_launch(double *out, PermArgs &a, const PermSpec &spec, long long total,
+                           const SplitOut &so, cudaStream_t st) {
   // tiled path when the innermost output index is strided in every source and
   // some other index has unit stride in all of them
   int D = -1;
@@ -169,125 +206,218 @@ int permute(double *out, const PermSpec &spec, cudaStream_t st) {
     for (int k = 0; k < 3; ++k)
       if (k != D) nb *= a.n[k];
     dim3 blk(32, 8);
-    if (D == 0) k_permute_tiled<0><<<(unsigned)nb, blk, 0, st>>>(out, a);
-    if (D == 1) k_permute_tiled<1><<<(unsigned)nb, blk, 0, st>>>(out, a);
-    if (D == 2) k_permute_tiled<2><<<(unsigned)nb, blk, 0, st>>>(out, a);
+    if (D == 0) k_permute_tiled<0, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+    if (D == 1) k_permute_tiled<1, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+    if (D == 2) k_permute_tiled<2, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
     count_launch();
   } else {
     long long nb = (total + 255) / 256;
     if (nb > 148 * 64) nb = 148 * 64;
     const bool rows4 = all_unit3 && a.n[3] % 4 == 0 && total < (1LL << 31) &&
-                       ((uintptr_t)out & 15) == 0;
+                       (!out || ((uintptr_t)out & 15) == 0);
     if (rows4) {
       long long nq = (total / 4 + 255) / 256;
       if (nq > 148 * 64) nq = 148 * 64;
-      k_permute_rows4<<<(unsigned)nq, 256, 0, st>>>(out, a, total / 4);
-    } else if (total < (1LL << 31))
-      k_permute_naive<false><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
-    else
-      k_permute_naive<true><<<(unsigned)nb, 256, 0, st>>>(out, a, total);
+      k_permute_rows4<S><<<(unsigned)nq, 256, 0, st>>>(out, a, total / 4, so);
+    } else if (S || total < (1LL << 31)) {
+      k_permute_naive<false, S><<<(unsigned)nb, 256, 0, st>>>(out, a, total, so);
+    } else {
+      k_permute_naive<true, false><<<(unsigned)nb, 256, 0, st>>>(out, a, total, so);
+    }
     count_launch();
   }
+}
+
+static void perm_args(PermArgs &a, const PermSpec &spec, long long &total) {
+  total = 1;
+  for (int k = 0; k < 4; ++k) {
+    a.n[k] = spec.n[k];
+    total *= spec.n[k];
+  }
+  a.nterms = spec.nterms;
+  a.beta = spec.beta;
+  a.fd1 = FastDiv((unsigned)a.n[1]);
+  a.fd2 = FastDiv((unsigned)a.n[2]);
+  a.fd3 = FastDiv((unsigned)a.n[3]);
+  for (int t = 0; t < 4; ++t) {
+    a.src[t] = t < spec.nterms ? spec.t[t].src : nullptr;
+    a.alpha[t] = t < spec.nterms ? spec.t[t].alpha : 0.0;
+    for (int k = 0; k < 4; ++k) a.s[t][k] = t < spec.nterms ? spec.t[t].s[k] : 0;
+  }
+}
+
+int permute(double *out, const PermSpec &spec, cudaStream_t st) {
+  PermArgs a;
+  long long total;
+  perm_args(a, spec, total);
+  if (total == 0) return ACES_OK;
+  permute_launch<false>(out, a, spec, total, SplitOut(), st);
+  ACES_CUDA(cudaGetLastError());
+  return ACES_OK;
+}
+
+int permute_split(double *out, void *hi, void *lo, int K, int k_pad, const PermSpec &spec,
+                  cudaStream_t st) {
+  PermArgs a;
+  long long total;
+  perm_args(a, spec, total);
+  if (total == 0) return ACES_OK;
+  if (K < 1 || k_pad < K || total % K != 0 || total >= (1LL << 31) || spec.beta != 0.0 ||
+      (!out && !hi)) {
+    set_error("permute_split: %lld outputs as rows of K = %d (k_pad %d) not supported", total, K,
+              k_pad);
+    return ACES_ERR_ARG;
+  }
+  SplitOut so;
+  so.hi = (__nv_bfloat16 *)hi;
+  so.lo = (__nv_bfloat16 *)lo;
+  so.k_pad = k_pad;
+  so.fk = FastDiv((unsigned)K);
+  permute_launch<true>(out, a, spec, total, so, st);
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
 }
 
 // ---------------------------------------------------------------------------
-// Elementwise
+// Pair blocks of [o,o,v,v] arrays
 // ---------------------------------------------------------------------------
-// [i,j,a,b] index of an o*o*v*v element: pair p = i*o + j (below 2^31 / v^2)
-// and ab = a*v + b split with FastDiv
-struct Ijab {
-  int i, j, a, b;
+// Work units (p, c): p a pair of occupied indices, c a chunk of kPbChunk
+// consecutive (a,b) of its v*v pair block; thread t of the unit's block owns
+// (a,b) = c*kPbChunk + t + kPbThreads*u for u < kPbPer, so a warp's loads are
+// coalesced and each thread keeps kPbPer (twice that for two blocks) loads in
+// flight without any per-element 64-bit index split.  The symmetric walks run
+// p over the o(o+1)/2 pairs i <= j (p = j(j+1)/2 + i) and read the [i,j] and
+// [j,i] blocks of a unit together: an element and its exchange partner
+// x[j,i,a,b] (= x[i,j,b,a] for a pair-symmetric vector) meet in registers and
+// every element is loaded once.
+constexpr int kPbThreads = 256, kPbPer = 4, kPbChunk = kPbThreads * kPbPer;
+
+struct PairBlocks {
+  int o, v;
+  long long vv;        // elements per pair block
+  int nchunk;          // chunks per pair block
+  long long nunits;    // pairs x chunks
+  FastDiv fv;          // divisor v, for a = ab / v
 };
-__device__ __forceinline__ Ijab split_ijab(long long idx, const FastDiv &fvv, const FastDiv &fv,
-                                           const FastDiv &fo) {
-  Ijab r;
-  unsigned p, ab;
-  if (idx < (1LL << 31)) {
-    p = fvv.div((unsigned)idx);
-    ab = (unsigned)idx - p * fvv.d;
-  } else {  // 64-bit division only past 2^31 elements; the pair index still fits
-    const long long q = idx / fvv.d;
-    p = (unsigned)q;
-    ab = (unsigned)(idx - q * fvv.d);
-  }
-  r.a = (int)fv.div(ab);
-  r.b = (int)(ab - (unsigned)r.a * fv.d);
-  r.i = (int)fo.div(p);
-  r.j = (int)(p - (unsigned)r.i * fo.d);
-  return r;
+
+PairBlocks pair_blocks(int o, int v, bool symmetric) {
+  PairBlocks P;
+  P.o = o;
+  P.v = v;
+  P.vv = (long long)v * v;
+  P.nchunk = (int)((P.vv + kPbChunk - 1) / kPbChunk);
+  const long long npair = symmetric ? (long long)o * (o + 1) / 2 : (long long)o * o;
+  P.nunits = npair * P.nchunk;
+  P.fv = FastDiv((unsigned)std::max(v, 1));
+  return P;
 }
 
-__global__ void k_tau(double *__restrict__ tau, const double *__restrict__ t2,
-                      const double *__restrict__ t1, double c, int o, int v, long long total,
-                      FastDiv fvv, FastDiv fv, FastDiv fo) {
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const Ijab x = split_ijab(idx, fvv, fv, fo);
-    tau[idx] = t2[idx] + c * t1[x.i * v + x.a] * t1[x.j * v + x.b];
+// (i, j) with i <= j of the symmetric pair index p = j(j+1)/2 + i
+__device__ __forceinline__ void pb_pair(long long p, int &i, int &j) {
+  int jj = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+  while ((long long)(jj + 1) * (jj + 2) / 2 <= p) ++jj;
+  while ((long long)jj * (jj + 1) / 2 > p) --jj;
+  j = jj;
+  i = (int)(p - (long long)jj * (jj + 1) / 2);
+}
+
+// 256-thread blocks, a multiple of the SM count, at most one block per unit
+inline unsigned pb_grid(long long nunits, int per_sm) {
+  return (unsigned)std::max(1LL, std::min(nunits, 148LL * per_sm));
+}
+
+// tau[i,j,a,b] = t2[i,j,a,b] + c t1[i,a] t1[j,b]; units over all o^2 pairs
+__global__ void __launch_bounds__(kPbThreads)
+    k_tau(double *__restrict__ tau, const double *__restrict__ t2,
+          const double *__restrict__ t1, double c, PairBlocks P) {
+  for (long long u = blockIdx.x; u < P.nunits; u += gridDim.x) {
+    const long long p = u / P.nchunk;
+    const int ab0 = (int)(u - p * P.nchunk) * kPbChunk + threadIdx.x;
+    const int i = (int)(p / P.o), j = (int)(p - (long long)i * P.o);
+    const long long base = p * P.vv;
+    double x[kPbPer];
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      x[k] = ab < P.vv ? t2[base + ab] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      if (ab < P.vv) {
+        const int a = (int)P.fv.div((unsigned)ab), b = ab - a * P.v;
+        tau[base + ab] = x[k] + c * __ldg(t1 + i * P.v + a) * __ldg(t1 + j * P.v + b);
+      }
+    }
   }
 }
 
 void launch_tau(double *tau, const double *t2, const double *t1, double c, int o, int v,
                 cudaStream_t st) {
-  long long total = (long long)o * o * v * v;
-  long long nb = (total + 255) / 256;
-  if (nb > 148 * 32) nb = 148 * 32;
-  k_tau<<<(unsigned)nb, 256, 0, st>>>(tau, t2, t1, c, o, v, total, FastDiv((unsigned)(v * v)),
-                                      FastDiv((unsigned)v), FastDiv((unsigned)o));
+  const PairBlocks P = pair_blocks(o, v, false);
+  if (P.nunits == 0) return;
+  k_tau<<<pb_grid(P.nunits, 8), kPbThreads, 0, st>>>(tau, t2, t1, c, P);
   count_launch();
 }
 
 // NEWT2 for a closed-shell pair-symmetric T2: t2n[i,j,a,b] = t2n[j,i,b,a] =
-// (z2[i,j,a,b] + z2[j,i,b,a]) / 2 / (e_i + e_j - e_a - e_b).  One block per
-// (pair i <= j, 32 x 32 tile of (a, b)); the [j,i] block is read and written
-// through a shared-memory transpose so every global access is coalesced.
+// (z2[i,j,a,b] + z2[j,i,b,a]) / 2 / (e_i + e_j - e_a - e_b).  A unit is one
+// pair i <= j and one 32 x 32 (a, b) tile: the [i,j] tile (rows a) and the
+// [j,i] tile (rows b) are loaded together into shared memory (8 loads in
+// flight per thread), then both output tiles are written with coalesced
+// stores (the [j,i] one through the transposed shared-memory read).
 __global__ void __launch_bounds__(256)
     k_newt(double *__restrict__ t2n, const double *__restrict__ z2, double *__restrict__ t1n,
            const double *__restrict__ z1, const double *__restrict__ eo,
-           const double *__restrict__ ev, int o, int v) {
-  __shared__ double tz[32][33];
-  __shared__ double tw[32][33];
+           const double *__restrict__ ev, int o, int v, int tiles, long long nunits) {
+  __shared__ double tz[2][32][33];   // [ij tile: a rows][ji tile: b rows]
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  if (blockIdx.y == 0) {
-    // T1: z1 / (e_i - e_a), spread over the blocks of the first grid row
-    for (int e = blockIdx.x * 256 + threadIdx.x; e < o * v; e += gridDim.x * 256)
-      t1n[e] = z1[e] / (eo[e / v] - ev[e % v]);
-  }
-  const int tiles = (v + 31) / 32;
-  const int a0 = (blockIdx.x / tiles) * 32, b0 = (blockIdx.x % tiles) * 32;
-  const size_t vv = (size_t)v * v;
-  for (int pr = blockIdx.y; pr < o * o; pr += gridDim.y) {
-    const int i = pr / o, j = pr % o;
-    if (i > j) continue;  // block-uniform: the [j,i] pair is written by block [i,j]
-    const double *zij = z2 + ((size_t)i * o + j) * vv;
-    const double *zji = z2 + ((size_t)j * o + i) * vv;
-    double *wij = t2n + ((size_t)i * o + j) * vv;
-    double *wji = t2n + ((size_t)j * o + i) * vv;
-    __syncthreads();  // tz/tw of the previous pair are consumed
+  // T1: z1 / (e_i - e_a)
+  for (int e = blockIdx.x * 256 + threadIdx.x; e < o * v; e += gridDim.x * 256)
+    t1n[e] = z1[e] / (eo[e / v] - ev[e % v]);
+  const long long vv = (long long)v * v;
+  const int tt = tiles * tiles;
+  for (long long u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const long long p = u / tt;
+    const int tile = (int)(u - p * tt);
+    const int a0 = (tile / tiles) * 32, b0 = (tile % tiles) * 32;
+    int i, j;
+    pb_pair(p, i, j);
+    const double *zij = z2 + ((long long)i * o + j) * vv;
+    const double *zji = z2 + ((long long)j * o + i) * vv;
+    double *wij = t2n + ((long long)i * o + j) * vv;
+    double *wji = t2n + ((long long)j * o + i) * vv;
+    double xa[4], xb[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
-      tz[bl][tx] = (a < v && b < v) ? zji[(size_t)b * v + a] : 0.0;
+      const int r = ty + 8 * k;
+      const int a = a0 + r, b = b0 + tx;     // [i,j] tile element (a, b)
+      xa[k] = (a < v && b < v) ? zij[(long long)a * v + b] : 0.0;
+      const int bb = b0 + r, aa = a0 + tx;   // [j,i] tile element (b, a)
+      xb[k] = (aa < v && bb < v) ? zji[(long long)bb * v + aa] : 0.0;
+    }
+    __syncthreads();  // the previous unit's tile reads are done
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      tz[0][ty + 8 * k][tx] = xa[k];
+      tz[1][ty + 8 * k][tx] = xb[k];
     }
     __syncthreads();
     const double eij = eo[i] + eo[j];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int al = ty + 8 * k, a = a0 + al, b = b0 + tx;
-      if (a < v && b < v) {
-        const double x = 0.5 * (zij[(size_t)a * v + b] + tz[tx][al]) / (eij - ev[a] - ev[b]);
-        wij[(size_t)a * v + b] = x;
-        tw[al][tx] = x;
-      }
+      if (a < v && b < v)
+        wij[(long long)a * v + b] =
+            0.5 * (tz[0][al][tx] + tz[1][tx][al]) / (eij - ev[a] - ev[b]);
     }
-    if (i == j) continue;
-    __syncthreads();
+    if (i == j) continue;  // block-uniform
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
-      if (a < v && b < v) wji[(size_t)b * v + a] = tw[tx][bl];
+      if (a < v && b < v)
+        wji[(long long)b * v + a] =
+            0.5 * (tz[0][tx][bl] + tz[1][bl][tx]) / (eij - ev[a] - ev[b]);
     }
   }
 }
@@ -295,8 +425,9 @@ __global__ void __launch_bounds__(256)
 void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, const double *eo,
                  const double *ev, int o, int v, cudaStream_t st) {
   const int tiles = (v + 31) / 32;
-  dim3 grid((unsigned)(tiles * tiles), (unsigned)std::min(o * o, 65535));
-  k_newt<<<grid, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v);
+  const long long nunits = (long long)o * (o + 1) / 2 * tiles * tiles;
+  const unsigned grid = (unsigned)std::max(1LL, std::min(nunits, 148LL * 8));
+  k_newt<<<grid, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, tiles, nunits);
   count_launch();
 }
 
@@ -325,25 +456,62 @@ __device__ void block_reduce(double (&vals)[N], double *out) {
   }
 }
 
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
+  return x;
+}
+
 // E = sum tau[ijab] (2 V[ijab] - V[ijba]) + 2 sum f_ia t_ia, accumulated as
 // s0 = sum tau V, s1 = sum tau (V[ijab] - V[ijba]) / 2, s2 = 2 sum f t1.  For
-// real orbitals <ij|ba> = <ji|ab>, so the exchange integral is read from the
-// [j,i] pair block at the same (a, b): every load is coalesced.
-__global__ void k_energy(double *__restrict__ part, const double *__restrict__ t2,
-                         const double *__restrict__ t1, const double *__restrict__ V,
-                         const double *__restrict__ fov, int o, int v, long long total,
-                         FastDiv fvv, FastDiv fv, FastDiv fo) {
+// real orbitals <ij|ba> = <ji|ab>: the exchange integral of an [i,j] element
+// is the [j,i] element at the same (a, b), read in the same pair-block unit.
+__global__ void __launch_bounds__(kPbThreads)
+    k_energy(double *__restrict__ part, const double *__restrict__ t2,
+             const double *__restrict__ t1, const double *__restrict__ V,
+             const double *__restrict__ fov, PairBlocks P) {
   double s[3] = {0.0, 0.0, 0.0};
-  const long long vv = (long long)v * v;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const Ijab x = split_ijab(idx, fvv, fv, fo);
-    double tau = t2[idx] + t1[x.i * v + x.a] * t1[x.j * v + x.b];
-    double vij = V[idx];
-    double vji = V[idx + ((long long)(x.j - x.i) * o + (x.i - x.j)) * vv];
-    s[0] += tau * vij;
-    s[1] += 0.5 * tau * (vij - vji);
-    if (idx < (long long)o * v) s[2] += 2.0 * fov[idx] * t1[idx];
+  const int n1 = P.o * P.v;
+  for (int e = blockIdx.x * kPbThreads + threadIdx.x; e < n1; e += gridDim.x * kPbThreads)
+    s[2] += 2.0 * fov[e] * t1[e];
+  for (long long u = blockIdx.x; u < P.nunits; u += gridDim.x) {
+    const long long p = u / P.nchunk;
+    const int ab0 = (int)(u - p * P.nchunk) * kPbChunk + threadIdx.x;
+    int i, j;
+    pb_pair(p, i, j);
+    const long long o1 = ((long long)i * P.o + j) * P.vv, o2 = ((long long)j * P.o + i) * P.vv;
+    if (i == j) {
+#pragma unroll
+      for (int k = 0; k < kPbPer; ++k) {
+        const int ab = ab0 + k * kPbThreads;
+        if (ab < P.vv) {
+          const int a = (int)P.fv.div((unsigned)ab), b = ab - a * P.v;
+          const double tau = t2[o1 + ab] + __ldg(t1 + i * P.v + a) * __ldg(t1 + i * P.v + b);
+          s[0] += tau * V[o1 + ab];
+        }
+      }
+      continue;
+    }
+    double x1[kPbPer], x2[kPbPer], v1[kPbPer], v2[kPbPer];
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      const bool in = ab < P.vv;
+      x1[k] = in ? t2[o1 + ab] : 0.0;
+      x2[k] = in ? t2[o2 + ab] : 0.0;
+      v1[k] = in ? V[o1 + ab] : 0.0;
+      v2[k] = in ? V[o2 + ab] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      if (ab < P.vv) {
+        const int a = (int)P.fv.div((unsigned)ab), b = ab - a * P.v;
+        const double tau1 = x1[k] + __ldg(t1 + i * P.v + a) * __ldg(t1 + j * P.v + b);
+        const double tau2 = x2[k] + __ldg(t1 + j * P.v + a) * __ldg(t1 + i * P.v + b);
+        s[0] += tau1 * v1[k] + tau2 * v2[k];
+        s[1] += 0.5 * tau1 * (v1[k] - v2[k]) + 0.5 * tau2 * (v2[k] - v1[k]);
+      }
+    }
   }
   block_reduce<3>(s, part + 3 * blockIdx.x);
 }
@@ -359,24 +527,10 @@ __global__ void k_final_sum(double *out, const double *part, int nblk, int nv) {
 
 void launch_energy(double *out3, const double *t2, const double *t1, const double *voovv,
                    const double *fov, int o, int v, double *scratch, cudaStream_t st) {
-  long long total = (long long)o * o * v * v;
-  k_energy<<<kRedBlocks, 256, 0, st>>>(scratch, t2, t1, voovv, fov, o, v, total,
-                                       FastDiv((unsigned)(v * v)), FastDiv((unsigned)v),
-                                       FastDiv((unsigned)o));
+  const PairBlocks P = pair_blocks(o, v, true);
+  k_energy<<<kRedBlocks, kPbThreads, 0, st>>>(scratch, t2, t1, voovv, fov, P);
   count_launch();
   k_final_sum<<<3, 32, 0, st>>>(out3, scratch, kRedBlocks, 3); count_launch();
-}
-
-__global__ void k_diff(double *e, const double *a, const double *b, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    e[i] = a[i] - b[i];
-}
-
-void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st) {
-  long long nb = (n + 255) / 256;
-  if (nb > 148 * 32) nb = 148 * 32;
-  k_diff<<<(unsigned)nb, 256, 0, st>>>(e, xnew, xold, n); count_launch();
 }
 
 // xn = x + damp (xn - x), two loads and a store per element
@@ -397,107 +551,11 @@ struct HistPtrs {
   const double *p[25];
 };
 
-// dots of e with hist[k] over T1, T2(AB) and packed T2(AA) (i<j, a<b).  The
-// AA block of a pair-symmetric vector x (x[i,j,a,b] = x[j,i,b,a], which every
-// amplitude, difference and extrapolated vector is, bit for bit) obeys
-//   sum_{i<j,a<b} (x_ijab - x_ijba)(y_ijab - y_ijba) = sum_{i<j} sum_ab x_ijab (y_ijab - y_jiab),
-// so the exchange partner is read from the [j,i] pair block at the same (a,b)
-// and every load is coalesced.
-__global__ void k_diis_dots(double *__restrict__ part, const double *__restrict__ e, HistPtrs h,
-                            int nh, int o, int v, FastDiv fvv, FastDiv fv, FastDiv fo) {
-  double s[25];
-  for (int k = 0; k < 25; ++k) s[k] = 0.0;
-  const long long n1 = (long long)o * v;
-  const long long n2 = (long long)o * o * v * v;
-  const long long vv = (long long)v * v;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const double x = e[idx];
-    long long tix = -1;
-    if (idx >= n1) {
-      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
-      if (q.i < q.j) tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;  // [j,i,a,b]
-    }
-    for (int k = 0; k < nh; ++k) {
-      const double y = h.p[k][idx];
-      double acc = x * y;
-      if (tix >= 0) acc += x * (y - h.p[k][tix]);
-      s[k] += acc;
-    }
-  }
-  // reduce 25 values
-  __shared__ double sh[25][8];
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int k = 0; k < nh; ++k) {
-    double x = s[k];
-    for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
-    if (lane == 0) sh[k][wid] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < nh) {
-    double x = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
-    part[(long long)blockIdx.x * 25 + threadIdx.x] = x;
-  }
-}
-
-int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
-                     int o, int v, double *scratch, cudaStream_t st) {
-  if (nh < 1 || nh > 25) return ACES_ERR_ARG;
-  HistPtrs h;
-  for (int k = 0; k < 25; ++k) h.p[k] = k < nh ? hist[k] : nullptr;
-  k_diis_dots<<<kRedBlocks, 256, 0, st>>>(scratch, e_new, h, nh, o, v, FastDiv((unsigned)(v * v)),
-                                          FastDiv((unsigned)v), FastDiv((unsigned)o));
-  count_launch();
-  k_final_sum<<<nh, 32, 0, st>>>(dots_out, scratch, kRedBlocks, 25); count_launch();
-  ACES_CUDA(cudaGetLastError());
-  return ACES_OK;
-}
-
 // signed absmax; ties resolved towards the lower index (ISAMAX)
 __device__ inline void amax_merge(double &bv, long long &bi, double v, long long i) {
   if (fabs(v) > fabs(bv) || (fabs(v) == fabs(bv) && i < bi)) {
     bv = v;
     bi = i;
-  }
-}
-
-// largest |element| of T1, T2(AB) and packed T2(AA); the AA element
-// (i<j, a<b) x_ijab - x_ijba is formed as x_ijab - x_jiab (pair symmetry, see
-// k_diis_dots) so the partner load is coalesced
-__global__ void k_absmax(double *__restrict__ pv, long long *__restrict__ pi,
-                         const double *__restrict__ x, int o, int v, FastDiv fvv, FastDiv fv,
-                         FastDiv fo) {
-  const long long n1 = (long long)o * v;
-  const long long n2 = (long long)o * o * v * v;
-  const long long vv = (long long)v * v;
-  double bv = 0.0;
-  long long bi = 0x7fffffffffffffffLL;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
-       idx += (long long)gridDim.x * blockDim.x) {
-    amax_merge(bv, bi, x[idx], idx);
-    if (idx >= n1) {
-      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
-      if (q.i < q.j && q.a < q.b) {
-        const long long tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;
-        amax_merge(bv, bi, x[idx] - x[tix], n1 + n2 + idx);
-      }
-    }
-  }
-  for (int off = 16; off; off >>= 1) {
-    double ov = __shfl_down_sync(0xffffffff, bv, off);
-    long long oi = __shfl_down_sync(0xffffffff, bi, off);
-    amax_merge(bv, bi, ov, oi);
-  }
-  __shared__ double sv[8];
-  __shared__ long long si[8];
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { sv[wid] = bv; si[wid] = bi; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax_merge(bv, bi, sv[w], si[w]);
-    pv[blockIdx.x] = bv;
-    pi[blockIdx.x] = bi;
   }
 }
 
@@ -515,64 +573,11 @@ __global__ void k_absmax_final(double *out, const double *pv, const long long *p
   if (threadIdx.x == 0) out[0] = bv;
 }
 
-void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st) {
-  double *pv = scratch;
-  long long *pi = (long long *)(scratch + kRedBlocks);
-  k_absmax<<<kRedBlocks, 256, 0, st>>>(pv, pi, x, o, v, FastDiv((unsigned)(v * v)),
-                                       FastDiv((unsigned)v), FastDiv((unsigned)o));
-  count_launch();
-  k_absmax_final<<<1, 32, 0, st>>>(out, pv, pi, kRedBlocks); count_launch();
-}
-
-// One pass over the new DIIS error vector e = xnew - xold: writes e, its
-// signed absmax over T1, T2(AB) and packed T2(AA) (as k_absmax) and its dots
-// with the n history error vectors (as k_diis_dots; history slot `self` is e
-// itself, taken from registers).  The [j,i,a,b] partner of a T2 element is
-// recomputed from xnew and xold, never read back from e.
-__global__ void k_diff_stats(double *__restrict__ e, const double *__restrict__ xnew,
-                             const double *__restrict__ xold, HistPtrs h, int nh, int self,
-                             int o, int v, FastDiv fvv, FastDiv fv, FastDiv fo,
-                             double *__restrict__ part, double *__restrict__ pv,
-                             long long *__restrict__ pi) {
-  double s[25];
-  for (int k = 0; k < 25; ++k) s[k] = 0.0;
-  const long long n1 = (long long)o * v;
-  const long long n2 = (long long)o * o * v * v;
-  const long long vv = (long long)v * v;
-  double bv = 0.0;
-  long long bi = 0x7fffffffffffffffLL;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n1 + n2;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const double x = xnew[idx] - xold[idx];
-    e[idx] = x;
-    amax_merge(bv, bi, x, idx);
-    long long tix = -1;
-    double xp = 0.0;
-    if (idx >= n1) {
-      const Ijab q = split_ijab(idx - n1, fvv, fv, fo);
-      if (q.i < q.j) {
-        tix = idx + ((long long)(q.j - q.i) * o + (q.i - q.j)) * vv;  // [j,i,a,b]
-        xp = xnew[tix] - xold[tix];
-        if (q.a < q.b) amax_merge(bv, bi, x - xp, n1 + n2 + idx);
-      }
-    }
-    for (int k = 0; k < nh; ++k) {
-      const double y = k == self ? x : h.p[k][idx];
-      double acc = x * y;
-      if (tix >= 0) acc += x * (y - (k == self ? xp : h.p[k][tix]));
-      s[k] += acc;
-    }
-  }
-  // dots: same block reduction as k_diis_dots
-  __shared__ double sh[25][8];
+// block-level absmax into pv[blockIdx.x], pi[blockIdx.x]
+__device__ void block_absmax(double bv, long long bi, double *pv, long long *pi) {
   __shared__ double sv[8];
   __shared__ long long si[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int k = 0; k < nh; ++k) {
-    double x = s[k];
-    for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffff, x, off);
-    if (lane == 0) sh[k][wid] = x;
-  }
   for (int off = 16; off; off >>= 1) {
     const double ov = __shfl_down_sync(0xffffffff, bv, off);
     const long long oi = __shfl_down_sync(0xffffffff, bi, off);
@@ -583,16 +588,126 @@ __global__ void k_diff_stats(double *__restrict__ e, const double *__restrict__ 
     si[wid] = bi;
   }
   __syncthreads();
-  if (threadIdx.x < nh) {
-    double x = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
-    part[(long long)blockIdx.x * 25 + threadIdx.x] = x;
-  }
   if (threadIdx.x == 0) {
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax_merge(bv, bi, sv[w], si[w]);
     pv[blockIdx.x] = bv;
     pi[blockIdx.x] = bi;
   }
+}
+
+// The absmax candidates of a pair-symmetric vector x = [T1 | T2]: every
+// element (its index), and for i < j, a < b the packed same-spin amplitude
+// x[i,j,a,b] - x[i,j,b,a] = x[i,j,a,b] - x[j,i,a,b] (index n1 + n2 + the
+// [i,j,a,b] element's index); x1 / x2 are the [i,j] / [j,i] elements of a unit.
+__device__ __forceinline__ void pb_absmax(double &bv, long long &bi, const double (&x1)[kPbPer],
+                                          const double (&x2)[kPbPer], bool off, long long g1,
+                                          long long g2, long long aa, int ab0,
+                                          const PairBlocks &P) {
+#pragma unroll
+  for (int k = 0; k < kPbPer; ++k) {
+    const int ab = ab0 + k * kPbThreads;
+    if (ab < P.vv) {
+      amax_merge(bv, bi, x1[k], g1 + ab);
+      if (off) {
+        amax_merge(bv, bi, x2[k], g2 + ab);
+        const int a = (int)P.fv.div((unsigned)ab), b = ab - a * P.v;
+        if (a < b) amax_merge(bv, bi, x1[k] - x2[k], aa + g1 + ab);
+      }
+    }
+  }
+}
+
+// One pass over the new DIIS error vector e = xnew - xold: writes e, its
+// signed absmax over T1, T2(AB) and packed T2(AA), and its dots with the nh
+// history error vectors, where the dot of two pair-symmetric vectors over
+// T1, T2(AB) and packed T2(AA) (i<j, a<b) is
+//   sum x y + sum_{i<j} sum_ab x_ijab (y_ijab - y_jiab)
+// (history slot `self` is e itself, taken from registers).  Per unit and
+// history slot a warp sums its lanes' products and lane 0 adds the sum to the
+// warp's shared slot: a fixed order, so the dots are deterministic.
+__global__ void __launch_bounds__(kPbThreads)
+    k_diff_stats(double *__restrict__ e, const double *__restrict__ xnew,
+                 const double *__restrict__ xold, HistPtrs h, int nh, int self, PairBlocks P,
+                 double *__restrict__ part, double *__restrict__ pv, long long *__restrict__ pi) {
+  __shared__ double sh[25][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 25; ++k) sh[k][wid] = 0.0;
+  const long long n1 = (long long)P.o * P.v, n2 = (long long)P.o * P.o * P.vv;
+  double bv = 0.0;
+  long long bi = 0x7fffffffffffffffLL;
+  // T1
+  for (int k = 0; k < nh; ++k) {
+    double acc = 0.0;
+    for (long long idx = blockIdx.x * kPbThreads + threadIdx.x; idx < n1;
+         idx += (long long)gridDim.x * kPbThreads) {
+      const double x = xnew[idx] - xold[idx];
+      if (k == 0) {
+        e[idx] = x;
+        amax_merge(bv, bi, x, idx);
+      }
+      acc += x * (k == self ? x : h.p[k][idx]);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) sh[k][wid] += acc;
+  }
+  // T2, by pair-block units
+  for (long long u = blockIdx.x; u < P.nunits; u += gridDim.x) {
+    const long long p = u / P.nchunk;
+    const int ab0 = (int)(u - p * P.nchunk) * kPbChunk + threadIdx.x;
+    int i, j;
+    pb_pair(p, i, j);
+    const bool off = i != j;
+    const long long g1 = n1 + ((long long)i * P.o + j) * P.vv;
+    const long long g2 = n1 + ((long long)j * P.o + i) * P.vv;
+    double x1[kPbPer], x2[kPbPer];
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      const bool in = ab < P.vv;
+      x1[k] = in ? xnew[g1 + ab] - xold[g1 + ab] : 0.0;
+      x2[k] = in && off ? xnew[g2 + ab] - xold[g2 + ab] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kPbPer; ++k) {
+      const int ab = ab0 + k * kPbThreads;
+      if (ab < P.vv) {
+        e[g1 + ab] = x1[k];
+        if (off) e[g2 + ab] = x2[k];
+      }
+    }
+    pb_absmax(bv, bi, x1, x2, off, g1, g2, n2, ab0, P);
+    for (int k = 0; k < nh; ++k) {
+      double acc = 0.0;
+      if (k == self) {
+#pragma unroll
+        for (int q = 0; q < kPbPer; ++q)
+          acc += x1[q] * x1[q] + (off ? x1[q] * (x1[q] - x2[q]) + x2[q] * x2[q] : 0.0);
+      } else {
+        const double *y = h.p[k];
+        double y1[kPbPer], y2[kPbPer];
+#pragma unroll
+        for (int q = 0; q < kPbPer; ++q) {
+          const int ab = ab0 + q * kPbThreads;
+          const bool in = ab < P.vv;
+          y1[q] = in ? y[g1 + ab] : 0.0;
+          y2[q] = in && off ? y[g2 + ab] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kPbPer; ++q)
+          acc += x1[q] * y1[q] + (off ? x1[q] * (y1[q] - y2[q]) + x2[q] * y2[q] : 0.0);
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) sh[k][wid] += acc;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nh) {
+    double x = 0.0;
+    for (int w = 0; w < kPbThreads / 32; ++w) x += sh[threadIdx.x][w];
+    part[(long long)blockIdx.x * 25 + threadIdx.x] = x;
+  }
+  block_absmax(bv, bi, pv, pi);
 }
 
 int launch_diff_stats(double *e, const double *xnew, const double *xold,
@@ -604,9 +719,8 @@ int launch_diff_stats(double *e, const double *xnew, const double *xold,
   double *part = scratch;                   // [kRedBlocks][25]
   double *pv = scratch + kRedBlocks * 25;   // [kRedBlocks]
   long long *pi = (long long *)(scratch + kRedBlocks * 26);
-  k_diff_stats<<<kRedBlocks, 256, 0, st>>>(e, xnew, xold, h, nh, self, o, v,
-                                           FastDiv((unsigned)(v * v)), FastDiv((unsigned)v),
-                                           FastDiv((unsigned)o), part, pv, pi);
+  const PairBlocks P = pair_blocks(o, v, true);
+  k_diff_stats<<<kRedBlocks, kPbThreads, 0, st>>>(e, xnew, xold, h, nh, self, P, part, pv, pi);
   count_launch();
   k_absmax_final<<<1, 32, 0, st>>>(absmax_out, pv, pi, kRedBlocks);
   count_launch();
@@ -614,6 +728,74 @@ int launch_diff_stats(double *e, const double *xnew, const double *xold,
   count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
+}
+
+// out = sum_k c[k] p_k over a pair-symmetric [T1 | T2] (the DIIS residual of
+// the stored error vectors) with its signed absmax (as k_diff_stats) in the
+// same pass; the sums run over k in order, element by element.
+__global__ void __launch_bounds__(kPbThreads)
+    k_lincomb_absmax(double *__restrict__ out, const double *__restrict__ c, HistPtrs hp, int n,
+                     PairBlocks P, double *__restrict__ pv, long long *__restrict__ pi) {
+  __shared__ double cs[25];
+  if (threadIdx.x < n) cs[threadIdx.x] = c[threadIdx.x];
+  __syncthreads();
+  const long long n1 = (long long)P.o * P.v, n2 = (long long)P.o * P.o * P.vv;
+  double bv = 0.0;
+  long long bi = 0x7fffffffffffffffLL;
+  for (long long idx = blockIdx.x * kPbThreads + threadIdx.x; idx < n1;
+       idx += (long long)gridDim.x * kPbThreads) {
+    double acc = 0.0;
+    for (int k = 0; k < n; ++k) acc += cs[k] * hp.p[k][idx];
+    out[idx] = acc;
+    amax_merge(bv, bi, acc, idx);
+  }
+  for (long long u = blockIdx.x; u < P.nunits; u += gridDim.x) {
+    const long long p = u / P.nchunk;
+    const int ab0 = (int)(u - p * P.nchunk) * kPbChunk + threadIdx.x;
+    int i, j;
+    pb_pair(p, i, j);
+    const bool off = i != j;
+    const long long g1 = n1 + ((long long)i * P.o + j) * P.vv;
+    const long long g2 = n1 + ((long long)j * P.o + i) * P.vv;
+    double x1[kPbPer], x2[kPbPer];
+#pragma unroll
+    for (int q = 0; q < kPbPer; ++q) x1[q] = x2[q] = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const double *y = hp.p[k];
+      const double ck = cs[k];
+#pragma unroll
+      for (int q = 0; q < kPbPer; ++q) {
+        const int ab = ab0 + q * kPbThreads;
+        if (ab < P.vv) {
+          x1[q] += ck * y[g1 + ab];
+          if (off) x2[q] += ck * y[g2 + ab];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kPbPer; ++q) {
+      const int ab = ab0 + q * kPbThreads;
+      if (ab < P.vv) {
+        out[g1 + ab] = x1[q];
+        if (off) out[g2 + ab] = x2[q];
+      }
+    }
+    pb_absmax(bv, bi, x1, x2, off, g1, g2, n2, ab0, P);
+  }
+  block_absmax(bv, bi, pv, pi);
+}
+
+void launch_lincomb_absmax(double *out, const double *c, const double *const *p, int n, int o,
+                           int v, double *scratch, double *absmax_out, cudaStream_t st) {
+  HistPtrs a;
+  for (int k = 0; k < 25; ++k) a.p[k] = k < n ? p[k] : nullptr;
+  double *pv = scratch;
+  long long *pi = (long long *)(scratch + kRedBlocks);
+  const PairBlocks P = pair_blocks(o, v, true);
+  k_lincomb_absmax<<<kRedBlocks, kPbThreads, 0, st>>>(out, c, a, n, P, pv, pi);
+  count_launch();
+  k_absmax_final<<<1, 32, 0, st>>>(absmax_out, pv, pi, kRedBlocks);
+  count_launch();
 }
 
 // Bordered DIIS system [[0,-1..],[-1,B]] (lam,c) = (-1,0,..) by LU with

@@ -22,6 +22,12 @@ struct PermSpec {
   double beta;
 };
 int permute(double *out, const PermSpec &spec, cudaStream_t st);
+// The same resort (beta = 0, fewer than 2^31 outputs) with the result also
+// written as the two BF16 planes (hi, lo; see split_pack) of a contraction
+// operand of rows x K, K-contiguous and zero-padded to k_pad: output element
+// idx is operand element (idx / K, idx % K).  out may be null (planes only).
+int permute_split(double *out, void *hi, void *lo, int K, int k_pad, const PermSpec &spec,
+                  cudaStream_t st);
 
 // ---- elementwise -----------------------------------------------------------
 // tau = t2 + c * t1[i,a] t1[j,b] over [o,o,v,v] (libr/ftau.f)
@@ -37,22 +43,21 @@ void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, c
 void launch_energy(double *out2, const double *t2, const double *t1, const double *voovv,
                    const double *fov, int o, int v, double *scratch, cudaStream_t st);
 
-// DIIS: error e = x_new - x_old over [t1 | t2]; writes e, the signed absmax of
-// e over T1, T2(AB) and packed T2(AA) into absmax_out, and dots of e with the
-// n stored error vectors (including e itself when stored) into dots_out.
-int launch_diis_dots(double *dots_out, const double *e_new, const double *const *hist, int nh,
-                     int o, int v, double *scratch, cudaStream_t st);
-void launch_diff(double *e, const double *xnew, const double *xold, long long n, cudaStream_t st);
 // DAMP_CC_RESIDUAL (vcc/damp_cc_residual.F): xn = x + damp (xn - x)
 void launch_blend(double *xn, const double *x, double damp, long long n, cudaStream_t st);
 // e = xnew - xold (T1 + T2 of a pair-symmetric vector) with, in the same pass,
-// absmax_out[0] = signed absmax (as launch_absmax) and dots_out[k] = <e, hist[k]>
-// (as launch_diis_dots; hist[self] is e); scratch holds >= 592 * 27 doubles
+// absmax_out[0] = its signed absmax over T1, T2(AB) and packed T2(AA) and
+// dots_out[k] = <e, hist[k]> over the same three parts (hist[self] is e);
+// scratch holds >= 592 * 27 doubles
 int launch_diff_stats(double *e, const double *xnew, const double *xold,
                       const double *const *hist, int nh, int self, int o, int v,
                       double *scratch, double *absmax_out, double *dots_out, cudaStream_t st);
-// signed absmax over [t1 | t2 | packed AA(t2)]
-void launch_absmax(double *out, const double *x, int o, int v, double *scratch, cudaStream_t st);
+// out = sum_k c[k] p[k] over a pair-symmetric [t1 | t2] (c in device memory,
+// n <= 25) and absmax_out[0] = its signed absmax over [t1 | t2 | packed AA(t2)]
+// (the DIIS residual and its largest element, vcc/dodiis0.F:131-160);
+// scratch holds >= 2 * 592 doubles
+void launch_lincomb_absmax(double *out, const double *c, const double *const *p, int n, int o,
+                           int v, double *scratch, double *absmax_out, cudaStream_t st);
 // solve the bordered DIIS system for n <= 25 on the device (libr/dodiis.F);
 // B is 25x25 row-major, coef_out[0..n-1]; status_out[0] = 0 ok / 1 singular
 void launch_diis_solve(double *coef_out, int *status_out, const double *B, int n, cudaStream_t st);
