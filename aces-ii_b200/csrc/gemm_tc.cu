@@ -8,12 +8,16 @@
 // dropped), which gives ~16 significant bits per product and FP32 sums that
 // are promoted to FP64 every CHUNK = 512 K elements (fewer for very long K).
 //
-// Persistent kernel, one CTA per SM, output tile 128 x 128, k tile 64, 3-stage
-// mbarrier pipeline (128-byte swizzle), 10 warps:
+// Persistent kernel, one CTA per SM, k tile 64 (128-byte swizzle), 10 warps:
 //   warp 0  TMA producer (one elected lane)
 //   warp 1  TMEM allocator + MMA issuer (one elected lane)
 //   warps 2-9 epilogue: two warps per TMEM lane quadrant, each thread one
 //             output row x 64 columns, accumulated in FP64 across K chunks
+// Two variants: one CTA per 128 x 128 output tile (3-stage mbarrier
+// pipeline), and for products of at least 256 rows a cluster pair of CTAs
+// per 256 x 128 tile (tcgen05 cta_group::2, 4 stages), which halves each
+// CTA's share of the B tile: 48 KB instead of 64 KB of operands per k tile
+// and CTA for the same products.  No copy uses cluster multicast.
 // Every mbarrier wait is bounded by a %globaltimer limit; on expiry the
 // kernel records an error code in g_tc_status, drains its own TMA copies,
 // waits for its issued products, releases TMEM and returns.
@@ -111,13 +115,24 @@ constexpr int TBM = 128, TBN = 128, TBK = ACES_TC_TBK;
 static_assert(TBK == 32 || TBK == 64, "k tile of 32 or 64 BF16");
 constexpr int kRowBytes = TBK * 2;                    // one swizzled smem row
 constexpr int kUnit = 64 / TBK;                       // k tiles per 64 K elements
-constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile
-constexpr int TILE_B = TBN * TBK * 2;
-constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // hi+lo of A and B
+constexpr int TILE_A = TBM * TBK * 2;                 // bytes of one BF16 plane tile of A
 constexpr int kSmemLimit = 227 * 1024;
-constexpr int STAGES = (kSmemLimit - 1024 - 256) / STAGE_BYTES;  // 3 (TBK 64) or 6/7 (TBK 32)
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment + barriers
-static_assert(SMEM_BYTES <= kSmemLimit && STAGES >= 3, "pipeline depth");
+// Per-CTA pipeline geometry of the two variants: CG = 1, one CTA per 128 x 128
+// output tile (A and B tiles of 128 rows); CG = 2, a CTA pair per 256 x 128
+// tile (tcgen05 cta_group::2), each CTA holding its 128 rows of A and half of
+// the B rows, so a k tile brings 48 KB per CTA into shared memory instead of
+// 64 KB for the same products.
+template <int CG>
+struct Geom {
+  static constexpr int kBRows = TBN / CG;                   // B rows per CTA
+  static constexpr int kTileB = kBRows * TBK * 2;
+  static constexpr int kStage = 2 * TILE_A + 2 * kTileB;    // hi+lo of A and B
+  static constexpr int kStages = (kSmemLimit - 1024 - 256) / kStage;
+  static constexpr int kSmem = kStages * kStage + 1024 + 256;  // + alignment + barriers
+  static_assert(kSmem <= kSmemLimit && kStages >= 3, "pipeline depth");
+  static_assert(3 * kStages * 8 + 64 + 8 <= 256, "barrier area");
+};
+// (3 stages at TBK 64 or 6/7 at TBK 32 for one CTA per tile, 4 at TBK 64 for pairs)
 // k tiles per FP32 accumulation chunk, by the contraction length K: 512 K
 // elements up to K = 36864, 256 up to 73728, 128 beyond
 inline int chunk_for(int kTilesTotal) {
@@ -183,6 +198,51 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   }
   return true;
 }
+// cluster-scope forms for the CTA pair: waits that acquire at cluster scope
+// (the phase is completed by arrivals of the other CTA), remote arrives,
+// the partner's address of a shared variable, the cluster barrier
+__device__ __forceinline__ bool mbar_try_cl(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, "
+      "%3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(20000u)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t bar, uint32_t parity) {
+  if (mbar_try_cl(bar, parity)) return true;
+  const unsigned long long t0 = gtimer(), limit = g_tc_wait_ns;
+  while (!mbar_try_cl(bar, parity)) {
+    if (gtimer() - t0 > limit) return false;
+  }
+  return true;
+}
+// waits on barriers that the other CTA of a pair may complete (tcgen05
+// commits multicast by rank 0, relayed copies, remote epilogue arrivals)
+template <int CG>
+__device__ __forceinline__ bool mbar_wait_g(uint32_t bar, uint32_t parity) {
+  return CG == 2 ? mbar_wait_cl(bar, parity) : mbar_wait(bar, parity);
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t mapa_rank(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
                                             uint32_t bar) {
   asm volatile(
@@ -206,23 +266,42 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
 // instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, N>>3, M>>4
 // (the N field, bits 17-22, is set per tile: a ragged last n tile multiplies
 // only its live columns rounded up to 16, the granularity of N at M = 128)
-constexpr uint32_t kIdescMK = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBM >> 4) << 24);
+// (M = 128 per CTA: 128 for one CTA, 256 for a CTA pair)
+constexpr uint32_t kIdescK = (1u << 4) | (1u << 7) | (1u << 10);
+// MMA N of a tile with n_live live columns (multiple of 16, at most TBN)
+__device__ __forceinline__ int mma_n(int n_live) { return min(TBN, (n_live + 15) & ~15); }
+template <int CG>
 __device__ __forceinline__ uint32_t idesc_for(int n_live) {
-  const int n = min(TBN, (n_live + 15) & ~15);
-  return kIdescMK | ((uint32_t)(n >> 3) << 17);
+  return kIdescK | ((uint32_t)((TBM * CG) >> 4) << 24) | ((uint32_t)(mma_n(n_live) >> 3) << 17);
 }
 
+template <int CG>
 __device__ __forceinline__ void umma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
                                      uint32_t acc) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-      "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+  if constexpr (CG == 1)
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+  else
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
 }
+// completion of this thread's issued products arrives on `bar` (for a CTA
+// pair: on the barrier at the same offset in both CTAs)
+template <int CG>
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   bar)
-               : "memory");
+  if constexpr (CG == 1)
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+  else
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+        " [%0], %1;" ::"r"(bar), "h"((unsigned short)3)
+        : "memory");
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -280,10 +359,12 @@ struct Launch {
   CUtensorMap bh[kMaxProb][kMaxSeg], bl[kMaxProb][kMaxSeg];
   Problem prob[kMaxProb];
   int nprob, nTiles;
+  int cg;  // CTAs per tile: 1, or 2 (a cluster pair on 256 x 128 tiles)
 };
 struct TileRef {
   int g, m0, n0, z, ktb, kTiles, b;
 };
+template <int CG>
 __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   TileRef r;
   r.g = 0;
@@ -317,7 +398,7 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
     tm = q % P.tilesM;
     r.z = q / P.tilesM;
   }
-  r.m0 = tm * TBM;
+  r.m0 = tm * TBM * CG;
   r.n0 = tn * TBN;
   r.ktb = r.z * P.ktc;
   r.kTiles = max(0, min(P.ktc, P.kTilesTotal - r.ktb));
@@ -326,56 +407,87 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
 
 // One CTA of 10 warps per SM: registers are allocated per SM sub-partition
 // (16384 each) and three of the warps share one, so a thread gets at most
-// 168 (the epilogue spills a few of its 64 FP64 column sums, L1-resident)
+// 168 (the epilogue spills a few of its 64 FP64 column sums, L1-resident).
+//
+// CG = 2: clusters of two CTAs (ranks 0 and 1) share 256 x 128 tiles.  Each
+// CTA's producer loads its 128 A rows and its half of the B rows (as many as
+// the tile's MMA N needs: rows n0 + rank * N/2 on) into its own shared memory
+// and its own `full` barrier; warp 1 of rank 1 relays the completion of each
+// of its stages to rank 0's `full2` barrier, and warp 1 of rank 0 issues the
+// cta_group::2 products (reading both CTAs' tiles) once both have landed.
+// Product completion is multicast to both CTAs' `empty`, `acc_full` and
+// `mma_done` barriers; both CTAs' epilogues drain their own TMEM rows and
+// arrive on rank 0's `acc_empty`.  Every CTA waits only on barriers it owns
+// for copies it issued, so a CTA never leaves with its own copies in flight.
+template <int CG>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
                   double *__restrict__ part) {
+  using Gm = Geom<CG>;
+  constexpr int kStages = Gm::kStages, kStage = Gm::kStage, kTileB = Gm::kTileB;
   const int nTiles = L.nTiles;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
-  uint64_t *full = bars;                      // [STAGES] TMA -> MMA
-  uint64_t *empty = bars + STAGES;            // [STAGES] MMA -> TMA
-  uint64_t *acc_full = bars + 2 * STAGES;             // [kNAcc] MMA -> epilogue
-  uint64_t *acc_empty = bars + 2 * STAGES + kNAcc;    // [kNAcc] epilogue -> MMA
-  uint64_t *mma_done = bars + 2 * STAGES + 2 * kNAcc;  // all products retired (teardown)
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 2 * kNAcc + 1);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * kStage);
+  uint64_t *full = bars;                               // [kStages] TMA -> MMA (own copies)
+  uint64_t *empty = bars + kStages;                    // [kStages] MMA -> TMA
+  uint64_t *full2 = bars + 2 * kStages;                // [kStages] rank 1's copies (rank 0)
+  uint64_t *acc_full = bars + 3 * kStages;             // [kNAcc] MMA -> epilogue
+  uint64_t *acc_empty = acc_full + kNAcc;              // [kNAcc] epilogue -> MMA
+  uint64_t *mma_done = acc_full + 2 * kNAcc;           // all products retired (teardown)
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = CG == 2 ? cluster_rank() : 0u;
+  // tile walk: by CTA (CG = 1) or by CTA pair (CG = 2)
+  const int t0 = CG == 2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int tstep = CG == 2 ? (int)(gridDim.x >> 1) : (int)gridDim.x;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
+      mbar_init(smem_u32(&full2[s]), 1);
     }
     for (int b = 0; b < kNAcc; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
-      mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);
+      mbar_init(smem_u32(&acc_empty[b]), CG * kEpiWarps);
     }
     mbar_init(smem_u32(mma_done), 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"(kTmemCols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if constexpr (CG == 1) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(kTmemCols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(kTmemCols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if constexpr (CG == 2) cluster_sync();  // both CTAs' barriers exist before any remote arrive
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- TMA producer (every CTA: its own tiles) ----------------
     int it = 0;  // k tiles issued by this CTA
     bool stop = *(volatile int *)&g_tc_inject != 0;  // injected fault: issue nothing
-    for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
-      const TileRef T = decode_tile(L, t);
+    for (int t = t0; t < nTiles && !stop; t += tstep) {
+      const TileRef T = decode_tile<CG>(L, t);
       const Problem &P = L.prob[T.g];
-      const int m0 = T.m0, n0 = T.n0, ktb = T.ktb, kTiles = T.kTiles;
+      const int kTiles = T.kTiles, ktb = T.ktb;
+      // this CTA's rows: A from m0 + 128 rank, B from n0 + rank * (MMA N) / 2
+      const int m0 = T.m0 + (int)rank * TBM;
+      const int n0 = T.n0 + (CG == 2 ? (int)rank * (mma_n(P.N - T.n0) >> 1) : 0);
       // row windows of a batched entry (one read per tile, 8 ints)
       int rA[kMaxSeg] = {0, 0, 0, 0}, rB[kMaxSeg] = {0, 0, 0, 0};
       if (P.batch) {
@@ -385,8 +497,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         rB[0] = b.x; rB[1] = b.y; rB[2] = b.z; rB[3] = b.w;
       }
       for (int kt = 0; kt < kTiles; ++kt) {
-        const int s = it % STAGES;
-        if (it >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((it / STAGES) - 1) & 1)) {
+        const int s = it % kStages;
+        if (it >= kStages && !mbar_wait_g<CG>(smem_u32(&empty[s]), ((it / kStages) - 1) & 1)) {
           atomicExch(&g_tc_status, 1);
           *(volatile int *)abort_flag = 1;
           stop = true;
@@ -397,8 +509,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         const uint32_t fb = smem_u32(&full[s]);
-        unsigned char *st = smem + s * STAGE_BYTES;
-        mbar_expect_tx(fb, STAGE_BYTES);
+        unsigned char *st = smem + s * kStage;
+        mbar_expect_tx(fb, kStage);
         const int gk = ktb + kt;  // global k tile -> segment and its local k offset
         int sg = 0;
         while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
@@ -413,41 +525,60 @@ __global__ void __launch_bounds__(kThreads, 1)
         tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb);
         tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb);
         tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, yb, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A + TILE_B), &L.bl[T.g][sg], kx, yb, fb);
+        tma_load_2d(smem_u32(st + 2 * TILE_A + kTileB), &L.bl[T.g][sg], kx, yb, fb);
         ++it;
       }
     }
     // drain: the most recent phase of every stage still possibly in flight
-    const int first = it > STAGES ? it - STAGES : 0;
+    const int first = it > kStages ? it - kStages : 0;
     for (int k = first; k < it; ++k)
-      if (!mbar_wait(smem_u32(&full[k % STAGES]), (k / STAGES) & 1)) atomicExch(&g_tc_status, 2);
+      if (!mbar_wait(smem_u32(&full[k % kStages]), (k / kStages) & 1))
+        atomicExch(&g_tc_status, 2);
+  } else if (warp == 1 && lane == 0 && rank == 1) {
+    // ---------------- relay (rank 1): its landed stages -> rank 0's full2 ----------------
+    int it = 0;
+    bool ok = *(volatile int *)&g_tc_inject == 0;
+    for (int t = t0; t < nTiles && ok; t += tstep) {
+      const int kTiles = decode_tile<CG>(L, t).kTiles;
+      for (int kt = 0; kt < kTiles; ++kt, ++it) {
+        const int s = it % kStages;
+        if (!mbar_wait(smem_u32(&full[s]), (it / kStages) & 1) || *(volatile int *)abort_flag) {
+          atomicExch(&g_tc_status, 7);
+          ok = false;
+          break;
+        }
+        mbar_arrive_cluster(mapa_rank(smem_u32(&full2[s]), 0));
+      }
+    }
+    if (!mbar_wait_g<CG>(smem_u32(mma_done), 0)) atomicExch(&g_tc_status, 6);
   } else if (warp == 1 && lane == 0) {
-    // ---------------- MMA issuer ----------------
+    // ---------------- MMA issuer (rank 0) ----------------
     int it = 0, gc = 0;  // k tiles consumed, accumulation chunks started
     bool stop = false;
-    for (int t = blockIdx.x; t < nTiles && !stop; t += gridDim.x) {
-      const TileRef T = decode_tile(L, t);
+    for (int t = t0; t < nTiles && !stop; t += tstep) {
+      const TileRef T = decode_tile<CG>(L, t);
       const int kTiles = T.kTiles, chunk = L.prob[T.g].chunk;
-      const uint32_t idesc = idesc_for(L.prob[T.g].N - T.n0);
+      const uint32_t idesc = idesc_for<CG>(L.prob[T.g].N - T.n0);
       for (int kt = 0; kt < kTiles; ++kt) {
         const int kin = kt % chunk, b = gc % kNAcc;
         if (kin == 0 && gc >= kNAcc &&
-            !mbar_wait(smem_u32(&acc_empty[b]), ((gc / kNAcc) - 1) & 1)) {
+            !mbar_wait_g<CG>(smem_u32(&acc_empty[b]), ((gc / kNAcc) - 1) & 1)) {
           atomicExch(&g_tc_status, 5);
           *(volatile int *)abort_flag = 1;
           stop = true;
           break;
         }
-        const int s = it % STAGES;
-        if (!mbar_wait(smem_u32(&full[s]), (it / STAGES) & 1)) {
+        const int s = it % kStages;
+        if (!mbar_wait(smem_u32(&full[s]), (it / kStages) & 1) ||
+            (CG == 2 && !mbar_wait_g<CG>(smem_u32(&full2[s]), (it / kStages) & 1))) {
           atomicExch(&g_tc_status, 3);
           *(volatile int *)abort_flag = 1;
           stop = true;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
-        const uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + TILE_B;
+        const uint32_t base = smem_u32(smem + s * kStage);
+        const uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + kTileB;
         const uint32_t acc_t = tmem + (uint32_t)(b * TBN);
         // the start address is the descriptor's low field (address >> 4): the
         // 32-byte K step (16 BF16) inside a swizzled row adds 2 to it
@@ -457,21 +588,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int kk = 0; kk < TBK / 16; ++kk) {
           const uint64_t o = 2 * kk;
           const uint32_t acc = (kin > 0 || kk > 0) ? 1u : 0u;
-          umma(acc_t, dah + o, dbh + o, idesc, acc);
-          umma(acc_t, dah + o, dbl + o, idesc, 1u);
-          umma(acc_t, dal + o, dbh + o, idesc, 1u);
+          umma<CG>(acc_t, dah + o, dbh + o, idesc, acc);
+          umma<CG>(acc_t, dah + o, dbl + o, idesc, 1u);
+          umma<CG>(acc_t, dal + o, dbh + o, idesc, 1u);
         }
-        umma_commit(smem_u32(&empty[s]));
+        umma_commit<CG>(smem_u32(&empty[s]));
         ++it;
         if (kin == chunk - 1 || kt == kTiles - 1) {
-          umma_commit(smem_u32(&acc_full[b]));
+          umma_commit<CG>(smem_u32(&acc_full[b]));
           ++gc;
         }
       }
     }
     // every product issued by this thread has retired before TMEM is released
-    umma_commit(smem_u32(mma_done));
-    if (!mbar_wait(smem_u32(mma_done), 0)) atomicExch(&g_tc_status, 6);
+    umma_commit<CG>(smem_u32(mma_done));
+    if (!mbar_wait_g<CG>(smem_u32(mma_done), 0)) atomicExch(&g_tc_status, 6);
   } else if (warp >= 2) {
     // ---------------- epilogue: FP64 accumulation of the chunks ----------------
     const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
@@ -479,11 +610,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int row = q * 32 + lane;
     int gc = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < nTiles && ok; t += gridDim.x) {
-      const TileRef T = decode_tile(L, t);
+    for (int t = t0; t < nTiles && ok; t += tstep) {
+      const TileRef T = decode_tile<CG>(L, t);
       const Problem &P = L.prob[T.g];
       const CView &C = P.C;
-      const int M = P.M, N = P.N, m0 = T.m0, n0 = T.n0, z = T.z;
+      const int M = P.M, N = P.N, m0 = T.m0 + (int)rank * TBM, n0 = T.n0, z = T.z;
       // lanes are consecutive output rows: with unit m stride a warp's stores coalesce
       const bool coalesced = C.sm0 == 1;
       const int nChunks = (T.kTiles + P.chunk - 1) / P.chunk;
@@ -493,7 +624,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int j = 0; j < kCols; ++j) acc[j] = 0.0;
       for (int c = 0; c < nChunks; ++c, ++gc) {
         const int b = gc % kNAcc;
-        const bool w = mbar_wait(smem_u32(&acc_full[b]), (gc / kNAcc) & 1);
+        const bool w = mbar_wait_g<CG>(smem_u32(&acc_full[b]), (gc / kNAcc) & 1);
         if (!w) atomicExch(&g_tc_status, 4);
         ok = __all_sync(0xffffffffu, w && !*(volatile int *)abort_flag);
         if (!ok) break;
@@ -512,7 +643,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+        if (lane == 0) {
+          if constexpr (CG == 2)  // rank 0's barrier counts both CTAs' warps
+            mbar_arrive_cluster(mapa_rank(smem_u32(&acc_empty[b]), 0));
+          else
+            mbar_arrive(smem_u32(&acc_empty[b]));
+        }
       }
       if (!ok) break;
       const int m = m0 + row;
@@ -576,10 +712,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  // a CTA of a pair leaves only when the other has no more product, copy
+  // relay or arrive aimed at it
+  if constexpr (CG == 2) cluster_sync();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(kTmemCols));
+    if constexpr (CG == 1)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"(kTmemCols));
+    else
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"(kTmemCols));
   }
 }
 
@@ -688,6 +831,7 @@ namespace {
 // fills problem g of a launch (maps, dims, chunk); tiles and split-K are set by the caller
 int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, int nseg, int M,
                 int N, const CView &C) {
+  const int cg = L.cg == 2 ? 2 : 1;
   if (nseg < 1 || nseg > kMaxSeg) {
     set_error("gemm_nt_bf16x3: %d K segments (1..%d)", nseg, kMaxSeg);
     return ACES_ERR_ARG;
@@ -709,15 +853,15 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
     const int kk = std::min(a.k, b.k) > 0 ? std::min(a.k, b.k) : a.k_pad;
     ACES_TRY(make_map(&L.ah[g][s], a.hi, a.rows_pad, a.k_pad, kk, TBM));
     ACES_TRY(make_map(&L.al[g][s], a.lo, a.rows_pad, a.k_pad, kk, TBM));
-    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, kk, TBN));
-    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, kk, TBN));
+    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, kk, TBN / cg));
+    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, kk, TBN / cg));
     P.kt0[s + 1] = P.kt0[s] + a.k_pad / TBK;
   }
   for (int s = nseg + 1; s <= kMaxSeg; ++s) P.kt0[s] = P.kt0[nseg];
   P.kTilesTotal = P.kt0[nseg];
   P.ktc = P.kTilesTotal;
   P.chunk = chunk_for(P.kTilesTotal);
-  P.tilesM = (M + TBM - 1) / TBM;
+  P.tilesM = (M + TBM * cg - 1) / (TBM * cg);
   P.tilesN = (N + TBN - 1) / TBN;
   // the side with fewer tiles runs fastest, so the CTAs working at the same
   // time share the row block of the larger operand (read from DRAM once,
@@ -725,6 +869,41 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
   P.mfast = P.tilesM < P.tilesN ? 1 : 0;
   return ACES_OK;
 }
+
+// CTA pairs the device keeps resident at once (the pair variant's grid is
+// twice that, at most the SM count)
+int max_pairs() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return num_sms() / 2;
+  if (!cached[dev]) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(num_sms() & ~1));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = Geom<2>::kSmem;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_gemm_bf16x3<2>, &cfg) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      n = num_sms() / 2;
+    }
+    cached[dev] = std::min(n, num_sms() / 2);
+  }
+  return cached[dev];
+}
+
+#ifndef ACES_TC_PAIRS
+#define ACES_TC_PAIRS 1
+#endif
+// the pair variant for launches whose every problem has at least 256 rows
+// (its tiles are 256 rows high) and enough tiles for the pairs
+bool pairs_for(int min_rows) { return ACES_TC_PAIRS && min_rows >= 2 * TBM; }
 
 int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
   // the shared-memory opt-in and the status word are per device
@@ -736,14 +915,33 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     return ACES_ERR_ARG;
   }
   if (!attr[dev]) {
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   SMEM_BYTES));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<1>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<2>::kSmem));
     int zero = 0;
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
     attr[dev] = true;
   }
-  const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
-  k_gemm_bf16x3<<<grid, kThreads, SMEM_BYTES, st>>>(L, alpha, beta, part);
+  if (L.cg == 2) {
+    const unsigned pairs = (unsigned)std::max(1, std::min(L.nTiles, max_pairs()));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(2 * pairs);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = Geom<2>::kSmem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2>, L, alpha, beta, part));
+  } else {
+    const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
+    k_gemm_bf16x3<1><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
+  }
   count_launch();
   ACES_CUDA(cudaGetLastError());
   return ACES_OK;
@@ -756,11 +954,12 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
   Launch L;
   memset(&L, 0, sizeof(L));
   L.nprob = 1;
+  L.cg = pairs_for(M) ? 2 : 1;
   ACES_TRY(set_problem(L, 0, A, B, nseg, M, N, C));
   Problem &P = L.prob[0];
-  // split K when the output has too few tiles to fill the SMs
+  // split K when the output has too few tiles to fill the SMs (CTA pairs)
   const long long tiles = (long long)P.tilesN * P.tilesM;
-  const int nsm = num_sms();
+  const int nsm = L.cg == 2 ? max_pairs() : num_sms();
   int Z = 1;
   double *part = nullptr;
   if (tiles < nsm && P.kTilesTotal >= 8 * kUnit) {
@@ -808,6 +1007,10 @@ int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha,
   }
   Launch L;
   memset(&L, 0, sizeof(L));
+  int min_rows = 1 << 30;
+  for (int g = 0; g < nprob; ++g)
+    if (probs[g].M > 0 && probs[g].N > 0) min_rows = std::min(min_rows, probs[g].M);
+  L.cg = pairs_for(min_rows) ? 2 : 1;
   long long tiles = 0;
   int n = 0;
   for (int g = 0; g < nprob; ++g) {
@@ -861,6 +1064,7 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
   Launch L;
   memset(&L, 0, sizeof(L));
   L.nprob = 1;
+  L.cg = pairs_for(M) ? 2 : 1;
   ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
   Problem &P = L.prob[0];
   P.batch = d_entries;
