@@ -170,9 +170,10 @@ const double *CCEngine::transposed(const double *src, int rows, int cols, long l
   if (cst && rows == cols && ld == cols)
     for (const double *sp : symmetric)
       if (sp == src) return src;
+  const auto key = std::make_tuple(src, rows, cols, ld);
   if (cst) {
-    auto it = tcache.find(src);
-    if (it != tcache.end() && it->second.n >= (size_t)rows * cols) return it->second.p;
+    auto it = tcache.find(key);
+    if (it != tcache.end()) return it->second.p;
   }
   DBuf *dst = &scratch;
   DBuf fresh;
@@ -187,7 +188,7 @@ const double *CCEngine::transposed(const double *src, int rows, int cols, long l
   s.t[0].s[0] = 0; s.t[0].s[1] = 0; s.t[0].s[2] = 1; s.t[0].s[3] = ld;
   if (permute(dst->p, s, st) != ACES_OK) return nullptr;
   if (cst) {
-    tcache[src] = fresh;
+    tcache[key] = fresh;
     return fresh.p;
   }
   return dst->p;

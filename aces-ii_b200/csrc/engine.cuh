@@ -5,6 +5,7 @@
 
 #include <deque>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "adjoint.cuh"
@@ -145,7 +146,9 @@ class CCEngine {
   bool recording = false;
   std::vector<DBuf *> active;
   std::map<DBuf *, DBuf> adjoint;
-  std::map<const double *, DBuf> tcache;     // transposes of constant operands
+  // transposes of constant operands, by (source, rows, cols, leading
+  // dimension): one array can be the operand of contractions of several shapes
+  std::map<std::tuple<const double *, int, int, long long>, DBuf> tcache;
   std::vector<const double *> symmetric;     // constant matrices equal to their transpose
   DBuf bwdA, bwdB, bwdC, bwdD;
   std::vector<DBuf *> registry();

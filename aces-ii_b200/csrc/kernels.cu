@@ -132,14 +132,17 @@ __global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long 
   }
 }
 
-// 32x32 shared-memory tiles over (i3, i_d) where every term reads i_d with
-// unit stride: reads coalesced along i_d, writes coalesced along i3.
-template <int D, bool S>
+// Shared-memory tiles of R (32 or 64) i3 x 32 i_d, where every term reads
+// i_d with unit stride: reads coalesced along i_d, writes coalesced along i3.
+// A 32 x 8 thread block; each thread loads R/8 elements per term (all issued
+// before the tile is used) and writes R/8 outputs.
+template <int D, bool S, int R>
 __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out, PermArgs a,
                                                        SplitOut so) {
-  __shared__ double tile[32][33];
+  __shared__ double tile[32][R + 1];
+  constexpr int kL = R / 8;  // loads per thread and term (rows i3 = ty + 8 k)
   const int nd = a.n[D];
-  const int t3 = (a.n[3] + 31) / 32, td = (nd + 31) / 32;
+  const int t3 = (a.n[3] + R - 1) / R, td = (nd + 31) / 32;
   long long b = blockIdx.x;
   int b3 = b % t3; b /= t3;
   int bd = b % td; b /= td;
@@ -150,38 +153,46 @@ __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out,
   int io1 = b % a.n[o1];
   int io0 = (int)(b / a.n[o1]);
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  double acc[4];
-  // output element (i3 = b3*32 + tx, id = bd*32 + ty + 8*k)
-  for (int k = 0; k < 4; ++k) acc[k] = 0.0;
+  // outputs of this thread: i3 = b3*R + tx + 32 h, id = bd*32 + ty + 8 k
+  double acc[R / 32][4];
+#pragma unroll
+  for (int h = 0; h < R / 32; ++h)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[h][k] = 0.0;
+  const int id_ld = bd * 32 + tx;
   for (int t = 0; t < a.nterms; ++t) {
+    const double *src = a.src[t] + (long long)io0 * a.s[t][o0] + (long long)io1 * a.s[t][o1] +
+                        (long long)id_ld * a.s[t][D];
+    double v[kL];
+#pragma unroll
+    for (int k = 0; k < kL; ++k) {
+      const int i3 = b3 * R + ty + 8 * k;
+      v[k] = (i3 < a.n[3] && id_ld < nd) ? __ldg(src + (long long)i3 * a.s[t][3]) : 0.0;
+    }
+    if (t) __syncthreads();  // the previous term's tile is consumed
+#pragma unroll
+    for (int k = 0; k < kL; ++k) tile[tx][ty + 8 * k] = v[k];
     __syncthreads();
-    // load: tile[id_local][i3_local] with coalesced id
+#pragma unroll
+    for (int h = 0; h < R / 32; ++h)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[h][k] += a.alpha[t] * tile[ty + 8 * k][tx + 32 * h];
+  }
+#pragma unroll
+  for (int h = 0; h < R / 32; ++h)
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-      int l3 = ty + 8 * k;        // i3 local
-      int ld = tx;                // id local (unit stride)
-      int i3 = b3 * 32 + l3, id = bd * 32 + ld;
-      double v = 0.0;
+      const int i3 = b3 * R + tx + 32 * h, id = bd * 32 + ty + 8 * k;
       if (i3 < a.n[3] && id < nd) {
-        long long off = (long long)io0 * a.s[t][o0] + (long long)io1 * a.s[t][o1] +
-                        (long long)i3 * a.s[t][3] + (long long)id * a.s[t][D];
-        v = __ldg(a.src[t] + off);
+        int idx_[4];
+        idx_[3] = i3; idx_[D] = id; idx_[o0] = io0; idx_[o1] = io1;
+        long long o =
+            (((long long)idx_[0] * a.n[1] + idx_[1]) * a.n[2] + idx_[2]) * a.n[3] + idx_[3];
+        const double val = (a.beta == 0.0 ? 0.0 : a.beta * out[o]) + acc[h][k];
+        if (!S || out) out[o] = val;
+        if (S) put_split(so, o, val);
       }
-      tile[ld][l3] = v;
     }
-    __syncthreads();
-    for (int k = 0; k < 4; ++k) acc[k] += a.alpha[t] * tile[ty + 8 * k][tx];
-  }
-  for (int k = 0; k < 4; ++k) {
-    int i3 = b3 * 32 + tx, id = bd * 32 + ty + 8 * k;
-    if (i3 < a.n[3] && id < nd) {
-      int idx_[4];
-      idx_[3] = i3; idx_[D] = id; idx_[o0] = io0; idx_[o1] = io1;
-      long long o = (((long long)idx_[0] * a.n[1] + idx_[1]) * a.n[2] + idx_[2]) * a.n[3] + idx_[3];
-      const double val = (a.beta == 0.0 ? 0.0 : a.beta * out[o]) + acc[k];
-      if (!S || out) out[o] = val;
-      if (S) put_split(so, o, val);
-    }
-  }
 }
 
 template <bool S>
@@ -202,13 +213,21 @@ static void permute_launch(double *out, PermArgs &a, const PermSpec &spec, long 
     }
   }
   if (D >= 0 && a.n[3] >= 8) {
-    long long nb = (long long)((a.n[3] + 31) / 32) * ((a.n[D] + 31) / 32);
+    // 64-row tiles (8 loads in flight per thread and term) unless i3 is short
+    const int R = a.n[3] >= 48 ? 64 : 32;
+    long long nb = (long long)((a.n[3] + R - 1) / R) * ((a.n[D] + 31) / 32);
     for (int k = 0; k < 3; ++k)
       if (k != D) nb *= a.n[k];
     dim3 blk(32, 8);
-    if (D == 0) k_permute_tiled<0, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
-    if (D == 1) k_permute_tiled<1, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
-    if (D == 2) k_permute_tiled<2, S><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+    if (R == 64) {
+      if (D == 0) k_permute_tiled<0, S, 64><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+      if (D == 1) k_permute_tiled<1, S, 64><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+      if (D == 2) k_permute_tiled<2, S, 64><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+    } else {
+      if (D == 0) k_permute_tiled<0, S, 32><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+      if (D == 1) k_permute_tiled<1, S, 32><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+      if (D == 2) k_permute_tiled<2, S, 32><<<(unsigned)nb, blk, 0, st>>>(out, a, so);
+    }
     count_launch();
   } else {
     long long nb = (total + 255) / 256;
