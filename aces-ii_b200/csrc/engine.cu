@@ -175,7 +175,16 @@ int CCEngine::perm_split(double *out, int rows, int K, bool consumer_splits, boo
     return ACES_ERR_ARG;
   }
   memo_written(out, total);
-  MemoEntry &m = memo_slot(out, K, rows, K);
+  MemoEntry *m = nullptr;
+  ACES_TRY(memo_planes(out, rows, K, &m));
+  ACES_TRY(permute_split(keep_fp64 ? out : nullptr, m->op.hi, m->op.lo, K, m->op.k_pad, s, st));
+  m->valid = true;
+  m->fp64 = keep_fp64;
+  return ACES_OK;
+}
+
+int CCEngine::memo_planes(const double *key, int rows, int K, MemoEntry **out) {
+  MemoEntry &m = memo_slot(key, K, rows, K);
   const int kp = (K + kSplitKPad - 1) / kSplitKPad * kSplitKPad;
   const size_t need = (size_t)rows * kp * 2 * 2;
   if (!m.op.hi || m.op.cap < need) {
@@ -189,9 +198,7 @@ int CCEngine::perm_split(double *out, int rows, int K, bool consumer_splits, boo
   m.op.k = K;
   m.op.k_pad = kp;
   m.op.lo = (char *)m.op.hi + (size_t)rows * kp * 2;
-  ACES_TRY(permute_split(keep_fp64 ? out : nullptr, m.op.hi, m.op.lo, K, kp, s, st));
-  m.valid = true;
-  m.fp64 = keep_fp64;
+  *out = &m;
   return ACES_OK;
 }
 
@@ -1126,7 +1133,25 @@ int CCEngine::ladder_packed(const double *in, double *out) {
   ACES_TRY(alloc(Ald, (size_t)oo * std::max(nm, 1)));
   memo_written(taup.p, (long long)oo * np);
   memo_written(taum.p, (long long)oo * std::max(nm, 1));
-  launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st);
+  if (memo_on && nm > 0 && splits(np, oo, np) && splits(nm, oo, nm)) {
+    // inside a residual pass whose grouped launch splits: tau+- straight
+    // into the planes of its B operands, no FP64 copy
+    MemoEntry *mp = nullptr, *mm = nullptr;
+    ACES_TRY(memo_planes(taup.p, oo, np, &mp));
+    ACES_TRY(memo_planes(taum.p, oo, nm, &mm));
+    LadderPlanes pl;
+    pl.hi_p = (__nv_bfloat16 *)mp->op.hi;
+    pl.lo_p = (__nv_bfloat16 *)mp->op.lo;
+    pl.hi_m = (__nv_bfloat16 *)mm->op.hi;
+    pl.lo_m = (__nv_bfloat16 *)mm->op.lo;
+    pl.kp_p = mp->op.k_pad;
+    pl.kp_m = mm->op.k_pad;
+    launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st, &pl);
+    mp->valid = mm->valid = true;
+    mp->fp64 = mm->fp64 = false;
+  } else {
+    launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st);
+  }
   // both products in one grouped launch (their tiles fill each other's last wave)
   const GArgs g[2] = {{np, oo, np, Up.p, np, taup.p, np, cview_colmajor(Sld.p, np), true, false},
                       {nm, oo, nm, Um.p, nm, taum.p, nm, cview_colmajor(Ald.p, nm), true, false}};

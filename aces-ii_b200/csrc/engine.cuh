@@ -104,6 +104,8 @@ class CCEngine {
   std::deque<MemoEntry> memo;
   bool memo_on = false;
   MemoEntry &memo_slot(const double *src, long long ld, int rows, int K);
+  // the entry of key as a rows x K operand (ld = K) with planes allocated
+  int memo_planes(const double *key, int rows, int K, MemoEntry **out);
   void memo_written(const void *p, long long n);
   void memo_written(const CView &C, int M, int N);
   bool fp64_missing(const double *p) const;

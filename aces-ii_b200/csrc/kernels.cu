@@ -1042,29 +1042,46 @@ void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pa
 
 // tau+[ij][p(c,d)] = tau[ij][cd] + tau[ij][dc] (c < d), tau[ij][cc];
 // tau-[ij][m(c,d)] = tau[ij][cd] - tau[ij][dc]
+// S: tau+ and tau- go straight to the BF16 planes of the ladder's B operands
+// (rows ij, k_pad apart) instead of FP64 arrays
+template <bool S>
 __global__ void k_ladder_pack_tau(double *__restrict__ tp, double *__restrict__ tm,
                                   const double *__restrict__ tau, const int *__restrict__ pairs,
-                                  int v, int noo) {
+                                  int v, int noo, LadderPlanes pl) {
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
   const size_t vv = (size_t)v * v;
   for (int ij = blockIdx.y; ij < noo; ij += gridDim.y) {
     const double *t = tau + (size_t)ij * vv;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np + nm; q += gridDim.x * blockDim.x) {
       const int c = pairs[2 * q], d = pairs[2 * q + 1];
-      if (q < np)
-        tp[(size_t)ij * np + q] = c == d ? t[(size_t)c * v + c]
-                                         : t[(size_t)c * v + d] + t[(size_t)d * v + c];
-      else
-        tm[(size_t)ij * nm + (q - np)] = t[(size_t)c * v + d] - t[(size_t)d * v + c];
+      const bool plus = q < np;
+      const double x = plus ? (c == d ? t[(size_t)c * v + c]
+                                      : t[(size_t)c * v + d] + t[(size_t)d * v + c])
+                            : t[(size_t)c * v + d] - t[(size_t)d * v + c];
+      if (!S) {
+        if (plus)
+          tp[(size_t)ij * np + q] = x;
+        else
+          tm[(size_t)ij * nm + (q - np)] = x;
+      } else {
+        __nv_bfloat16 h, l;
+        split_bf16(x, h, l);
+        const size_t at = plus ? (size_t)ij * pl.kp_p + q : (size_t)ij * pl.kp_m + (q - np);
+        (plus ? pl.hi_p : pl.hi_m)[at] = h;
+        (plus ? pl.lo_p : pl.lo_m)[at] = l;
+      }
     }
   }
 }
 
 void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
-                            int noo, cudaStream_t st) {
+                            int noo, cudaStream_t st, const LadderPlanes *planes) {
   const int n = v * v;
   dim3 grid((unsigned)std::min((n + 255) / 256, 64), (unsigned)std::min(noo, 65535));
-  k_ladder_pack_tau<<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo);
+  if (planes)
+    k_ladder_pack_tau<true><<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo, *planes);
+  else
+    k_ladder_pack_tau<false><<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo, LadderPlanes());
   count_launch();
 }
 

@@ -1,5 +1,6 @@
 // kernels.cuh -- launchers of the bandwidth-bound kernels of the CC engine.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -93,8 +94,14 @@ void launch_scatter_rpsq(const double *X, const DpdMap &m, cudaStream_t st);
 // antisymmetric pairs (c < d)
 void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pairs, int v,
                           cudaStream_t st);
+// BF16 planes (hi, lo; rows ij k_pad apart) of the packed tau+ / tau- operands
+struct LadderPlanes {
+  __nv_bfloat16 *hi_p = nullptr, *lo_p = nullptr, *hi_m = nullptr, *lo_m = nullptr;
+  int kp_p = 0, kp_m = 0;
+};
+// with planes: tau+ / tau- written only as the planes (tp, tm untouched)
 void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
-                            int noo, cudaStream_t st);
+                            int noo, cudaStream_t st, const LadderPlanes *planes = nullptr);
 void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
                           cudaStream_t st);
 
