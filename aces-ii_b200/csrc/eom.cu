@@ -16,7 +16,8 @@
 // for x in the pair-symmetric space of irrep h (amplitudes only on the
 // excitations whose orbital irreps multiply to h), and a Davidson iteration on
 // the device -- trial vectors and products as rows of two device matrices,
-// the subspace matrix V S^T by one FP64 contraction -- finds the lowest roots.
+// the subspace matrix V S^T grown by one row and column per new vector --
+// finds the lowest roots.
 // The subspace eigenproblem (a few tens of rows, non-symmetric) is solved on
 // the host: Householder reduction to Hessenberg form, complex shifted QR
 // with Wilkinson shifts for the eigenvalues, inverse iteration for the
@@ -100,6 +101,52 @@ __global__ void k_eom_precond(double *__restrict__ dvec, const double *__restric
   }
 }
 
+// c[r] = alpha sum_n A[r * lda + n] y[n] for r < m (m <= kMaxRows): y is read
+// once, each row once; every block owns chunks of 1024 elements (4 per
+// thread), a warp sums its lanes' products per row and lane 0 adds the sum to
+// the warp's shared slot (fixed order: deterministic), and one block of the
+// second kernel sums the blocks' partials in block order.
+constexpr int kMaxRows = 64, kDotBlocks = 592;
+__global__ void __launch_bounds__(256)
+    k_multidot(double *__restrict__ part, const double *__restrict__ A, long long lda,
+               const double *__restrict__ y, long long len, int m) {
+  __shared__ double sh[kMaxRows][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int r = 0; r < m; ++r) sh[r][wid] = 0.0;
+  const long long nchunk = (len + 1023) / 1024;
+  for (long long c = blockIdx.x; c < nchunk; c += gridDim.x) {
+    const long long n0 = c * 1024 + threadIdx.x;
+    double yv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) yv[u] = n0 + 256 * u < len ? y[n0 + 256 * u] : 0.0;
+    for (int r = 0; r < m; ++r) {
+      const double *a = A + (long long)r * lda;
+      double s = 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (n0 + 256 * u < len) s += a[n0 + 256 * u] * yv[u];
+      for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+      if (lane == 0) sh[r][wid] += s;
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += sh[r][w];
+    part[(long long)blockIdx.x * kMaxRows + r] = s;
+  }
+}
+
+__global__ void k_multidot_final(double *__restrict__ c, const double *__restrict__ part, int m,
+                                 double alpha) {
+  const int r = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < kDotBlocks; b += 32) s += part[(long long)b * kMaxRows + r];
+  for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if (threadIdx.x == 0) c[r] = alpha * s;
+}
+
 unsigned grid_for(long long n) {
   long long nb = (n + 255) / 256;
   if (nb > 148 * 16) nb = 148 * 16;
@@ -176,7 +223,7 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
   auto t_start = std::chrono::steady_clock::now();
   // the converged residual pass on the tape; its reverse replay is (dZ/dT)^T x
   ACES_TRY(E.record_residual(false));
-  DBuf Vm, Sm, xr, sr, rv, dv, cdev, irrbuf;
+  DBuf Vm, Sm, xr, sr, rv, dv, cdev, irrbuf, dpart;
   struct Release {
     CCEngine &E;
     std::vector<DBuf *> b;
@@ -185,7 +232,7 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
       for (DBuf *p : b)
         if (p->p) dev_free(p->p);
     }
-  } release{E, {&Vm, &Sm, &xr, &sr, &rv, &dv, &cdev, &irrbuf}};
+  } release{E, {&Vm, &Sm, &xr, &sr, &rv, &dv, &cdev, &irrbuf, &dpart}};
   ACES_TRY(E.alloc(Vm, (size_t)maxdim * len));
   ACES_TRY(E.alloc(Sm, (size_t)maxdim * len));
   ACES_TRY(E.alloc(xr, len));
@@ -194,6 +241,7 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
   ACES_TRY(E.alloc(dv, len));
   ACES_TRY(E.alloc(cdev, (size_t)maxdim * maxdim + 64));
   ACES_TRY(E.alloc(irrbuf, (size_t)(o + v + 1) / 2 + 1));
+  ACES_TRY(E.alloc(dpart, (size_t)kDotBlocks * kMaxRows));
   int *d_irr_o = reinterpret_cast<int *>(irrbuf.p), *d_irr_v = d_irr_o + o;
   {
     std::vector<int> irr(E.irr_o);
@@ -205,13 +253,15 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
       hev(E.eps_h.begin() + o, E.eps_h.end());
   auto row = [&](DBuf &M, int k) { return M.p + (size_t)k * len; };
   auto dots = [&](const double *A, int m, const double *y, double alpha, double *c) -> int {
-    // c[k] = alpha sum_n A[k*len + n] y[n], K = len (may exceed 2^31: split)
-    const long long kmax = 1LL << 30;
-    for (long long k0 = 0; k0 < len; k0 += kmax) {
-      const int kk = (int)std::min(kmax, len - k0);
-      ACES_TRY(gemv_f64(m, kk, alpha, A + k0, len, y + k0, k0 == 0 ? 0.0 : 1.0,
-                        cview_rowmajor(c, 1), false, E.st));
+    // c[k] = alpha sum_n A[k*len + n] y[n] for k < m, m <= kMaxRows at a time
+    for (int r0 = 0; r0 < m; r0 += kMaxRows) {
+      const int mr = std::min(kMaxRows, m - r0);
+      k_multidot<<<kDotBlocks, 256, 0, E.st>>>(dpart.p, A + (size_t)r0 * len, len, y, len, mr);
+      count_launch();
+      k_multidot_final<<<mr, 32, 0, E.st>>>(c + r0, dpart.p, mr, alpha);
+      count_launch();
     }
+    ACES_CUDA(cudaGetLastError());
     return ACES_OK;
   };
   // out = base + sum_k c[k] M[k] over m rows (c on the device)
@@ -264,14 +314,30 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
       ++m;
     }
     std::vector<double> w_old(k, 0.0), wsel(k, 0.0);
+    // subspace matrix G[i][j] = v_i . s_j, kept on the host (maxdim x maxdim):
+    // rows and columns 0..mk-1 are known, each new vector adds its row and
+    // column (two passes over the subspace instead of m per iteration)
+    std::vector<double> Gh((size_t)maxdim * maxdim, 0.0), colb(maxdim), rowb(maxdim);
+    int mk = 0;
     bool conv = false;
     int it;
     for (it = 1; it <= cfg->eom_maxcyc; ++it) {
-      // subspace matrix G[i][j] = v_i . s_j
+      for (int j = mk; j < m; ++j) {
+        ACES_TRY(dots(Vm.p, m, row(Sm, j), 1.0, cdev.p));             // v_i . s_j
+        ACES_TRY(dots(Sm.p, m, row(Vm, j), 1.0, cdev.p + maxdim));    // v_j . s_i
+        ACES_CUDA(cudaMemcpyAsync(colb.data(), cdev.p, m * 8, cudaMemcpyDeviceToHost, E.st));
+        ACES_CUDA(cudaMemcpyAsync(rowb.data(), cdev.p + maxdim, m * 8, cudaMemcpyDeviceToHost,
+                                  E.st));
+        ACES_CUDA(cudaStreamSynchronize(E.st));
+        for (int i = 0; i < m; ++i) {
+          Gh[(size_t)i * maxdim + j] = colb[i];
+          Gh[(size_t)j * maxdim + i] = rowb[i];
+        }
+      }
+      mk = m;
       std::vector<double> G((size_t)m * m);
-      for (int i = 0; i < m; ++i) ACES_TRY(dots(Sm.p, m, row(Vm, i), 1.0, cdev.p + (size_t)i * m));
-      ACES_CUDA(cudaMemcpyAsync(G.data(), cdev.p, G.size() * 8, cudaMemcpyDeviceToHost, E.st));
-      ACES_CUDA(cudaStreamSynchronize(E.st));
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) G[(size_t)i * m + j] = Gh[(size_t)i * maxdim + j];
       if (int tcs = tc_status_and_clear()) {
         set_error("xvee_run: tensor-core contraction gave up waiting (code %d)", tcs);
         return ACES_ERR_TIMEOUT;
@@ -356,6 +422,7 @@ extern "C" int xvee_run(aces_eom_config *cfg) {
         // Ritz vector r (row r, r >= m) moves to row m, is orthonormalised
         // against rows 0..m-1 and kept unless it was linearly dependent
         m = 0;
+        mk = 0;
         for (int r = 0; r < k; ++r) {
           if (m != r)
             ACES_CUDA(cudaMemcpyAsync(row(Vm, m), row(Vm, r), len * 8, cudaMemcpyDeviceToDevice,

@@ -201,14 +201,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 // cluster-scope forms for the CTA pair: waits that acquire at cluster scope
 // (the phase is completed by arrivals of the other CTA), remote arrives,
 // the partner's address of a shared variable, the cluster barrier
+// (ACES_TC_CL_HINT: suspend-time hint of these waits in ns; 0 = none, the
+// thread re-polls after the hardware's own short wait)
+#ifndef ACES_TC_CL_HINT
+#define ACES_TC_CL_HINT 20000
+#endif
 __device__ __forceinline__ bool mbar_try_cl(uint32_t bar, uint32_t parity) {
   uint32_t ok;
+#if ACES_TC_CL_HINT > 0
   asm volatile(
       "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, "
       "%3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity), "r"(20000u)
+      : "r"(bar), "r"(parity), "r"((uint32_t)ACES_TC_CL_HINT)
       : "memory");
+#else
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;"
+      "\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+#endif
   return ok != 0;
 }
 __device__ __forceinline__ bool mbar_wait_cl(uint32_t bar, uint32_t parity) {
