@@ -177,5 +177,7 @@ int tc_status_and_clear();
 // device, and the test-only fault injection (producer issues no copies).
 int tc_set_wait_limit(unsigned long long ns);
 int tc_set_inject(int on);
+// launches of products with >= 256 rows on CTA pairs (process-wide)
+void tc_set_pairs(int on);
 
 }  // namespace acesb200

@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -912,12 +913,14 @@ int max_pairs() {
   return cached[dev];
 }
 
-#ifndef ACES_TC_PAIRS
-#define ACES_TC_PAIRS 1
-#endif
-// the pair variant for launches whose every problem has at least 256 rows
-// (its tiles are 256 rows high) and enough tiles for the pairs
-bool pairs_for(int min_rows) { return ACES_TC_PAIRS && min_rows >= 2 * TBM; }
+// The pair variant passes the same tests as the 1-CTA kernel, but on B200 it
+// measured slower on the shapes that matter here (packed ladder of the
+// o = 20, v = 180 cycle: 1.72 ms against 1.47 ms; (T) classes of o = 6,
+// v = 128: 420 us against 404 us per launch), so it is off by default;
+// aces_set_tc_pairs(1) turns it on for launches whose every problem has at
+// least 256 rows (the height of its tiles).
+std::atomic<int> g_tc_pairs{0};
+bool pairs_for(int min_rows) { return g_tc_pairs.load() != 0 && min_rows >= 2 * TBM; }
 
 int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
   // the shared-memory opt-in and the status word are per device
@@ -1109,6 +1112,8 @@ int tc_set_wait_limit(unsigned long long ns) {
   ACES_CUDA(cudaMemcpyToSymbol(g_tc_wait_ns, &ns, sizeof(ns)));
   return ACES_OK;
 }
+
+void tc_set_pairs(int on) { g_tc_pairs.store(on ? 1 : 0); }
 
 int tc_set_inject(int on) {
   ACES_CUDA(cudaMemcpyToSymbol(g_tc_inject, &on, sizeof(on)));

@@ -97,6 +97,15 @@ extern "C" int aces_set_wait_limit(double seconds) {
   return tc_set_wait_limit((unsigned long long)(seconds * 1e9));
 }
 
+extern "C" int aces_set_tc_pairs(int on) {
+  if (on != 0 && on != 1) {
+    set_error("aces_set_tc_pairs: %d (0 or 1)", on);
+    return ACES_ERR_ARG;
+  }
+  tc_set_pairs(on);
+  return ACES_OK;
+}
+
 extern "C" int aces_debug_inject(int mode) {
   if (mode != 0 && mode != 1) {
     set_error("aces_debug_inject: mode %d (0 or 1)", mode);

@@ -172,6 +172,12 @@ int aces_set_wait_limit(double seconds);
  * ACES_ERR_TIMEOUT with no copy or product in flight; mode 0 restores normal
  * operation. */
 int aces_debug_inject(int mode);
+/* Tile variant of the tensor-core contractions (no counterpart in the
+ * reference): 1 = products of at least 256 rows run on CTA pairs (tcgen05
+ * cta_group::2, 256 x 128 tiles), 0 = one CTA per 128 x 128 tile (the
+ * default, faster on B200 for the CC contractions).  Both give the same
+ * error bound; process-wide. */
+int aces_set_tc_pairs(int on);
 
 /* ---- member programs ---------------------------------------------------- */
 

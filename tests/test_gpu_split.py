@@ -104,3 +104,49 @@ def test_ccsd_bf16x3_then_fp64_same_lists(lib):
     ref = ccsd.run_ccsd(ham, cc_conv=8, maxcyc=60)["e_final"]
     assert abs(exact - ref) < 1e-11
     assert abs(split - ref) < 1e-6
+
+
+# The CTA-pair tile variant (aces_set_tc_pairs(1): tcgen05 cta_group::2 on
+# 256 x 128 tiles for products of >= 256 rows) obeys the same bound.  Shapes:
+# ragged rows in the second CTA of a pair (300), split K (1000 x 260 x 777),
+# several pair tiles per CTA pair (2000 x 1300), a thin ragged N = 20 whose
+# B half per CTA is 16 rows, and multi-chunk K.
+@pytest.mark.parametrize("m,n,k", [(300, 200, 513), (1000, 260, 777), (2000, 1300, 200),
+                                   (70000, 20, 180), (256, 256, 40000)])
+@pytest.mark.parametrize("beta", [0.0, 1.0])
+def test_xgemm_bf16x3_pairs_error_bound(lib, m, n, k, beta):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(7 * m + n + k)
+    A = torch.randn((k, m), generator=g, dtype=torch.float64)
+    B = torch.randn((k, n), generator=g, dtype=torch.float64)
+    A = A * torch.exp(torch.randn(A.shape, generator=g, dtype=torch.float64))
+    Cm = torch.randn((m, n), generator=g, dtype=torch.float64)
+    ref = 1.1 * A.T @ B + beta * Cm
+    bound = 1.1 * A.T.abs() @ B.abs()
+    dA = A.T.contiguous().cuda()   # column-major (k x m) A: op(A) = A^T
+    dB = B.T.contiguous().cuda()
+    dC = Cm.T.contiguous().cuda()
+    lib.set_tc_pairs(1)
+    try:
+        lib.xgemm("T", "N", m, n, k, 1.1, dA.data_ptr(), k, dB.data_ptr(), k, beta,
+                  dC.data_ptr(), m, precision=ab.PREC_BF16X3)
+    finally:
+        lib.set_tc_pairs(0)
+    out = dC.cpu().T
+    err = (out - ref).abs()
+    assert torch.all(err <= 4e-5 * bound + 1e-12), (err / (bound + 1e-30)).max().item()
+    assert (err / (bound + 1e-30)).max().item() < 2e-5
+
+
+def test_ccsd_bf16x3_pairs_energy_within_1e6(lib):
+    """A split CCSD whose ladder, ring and (T)-free contractions run on CTA pairs."""
+    ham = synthetic(10, 90, 120, seed=2)
+    setup_lists(lib, ham)
+    lib.set_tc_pairs(1)
+    try:
+        cfg = lib.xvcc(cc_conv=8, cc_maxcyc=60, cc_exporder=5, precision=ab.PREC_BF16X3)
+    finally:
+        lib.set_tc_pairs(0)
+    ref = ccsd.run_ccsd(ham, cc_conv=8, maxcyc=60, exporder=5)
+    assert cfg.converged == 1
+    assert abs(cfg.e_ccsd - ref["e_final"]) < 1e-6, cfg.e_ccsd - ref["e_final"]
