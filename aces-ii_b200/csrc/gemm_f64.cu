@@ -417,7 +417,10 @@ __global__ void __launch_bounds__(LR_F)
                   ss0 = fast_is_m ? C.sn0 : C.sm0;
   double *const cf = C.p + cview_dim(fdiv, fs1, fs0, f);
   ViewWalk w(sdiv, ss1, ss0, s0);
-  const bool red = beta == 1.0 && fs0 == 1;
+#ifndef ACES_LR_RED
+#define ACES_LR_RED 1
+#endif
+  const bool red = ACES_LR_RED && beta == 1.0 && fs0 == 1;
   const double *fr = Fs + threadIdx.x * ks;
 #pragma unroll 1
   for (int sb = 0; sb < nsl; sb += 8) {

@@ -133,9 +133,10 @@ __global__ void k_permute_rows4(double *__restrict__ out, PermArgs a, long long 
 }
 
 // Shared-memory tiles of R (32 or 64) i3 x 32 i_d, where every term reads
-// i_d with unit stride: reads coalesced along i_d, writes coalesced along i3.
-// A 32 x 8 thread block; each thread loads R/8 elements per term (all issued
-// before the tile is used) and writes R/8 outputs.
+// either i_d with unit stride (transposed through the tile: reads coalesced
+// along i_d) or i3 with unit stride (read at the output positions directly);
+// writes coalesced along i3.  A 32 x 8 thread block; each thread loads R/8
+// elements per term (all issued before they are used) and writes R/8 outputs.
 template <int D, bool S, int R>
 __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out, PermArgs a,
                                                        SplitOut so) {
@@ -160,19 +161,38 @@ __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out,
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[h][k] = 0.0;
   const int id_ld = bd * 32 + tx;
+  bool tile_used = false;
   for (int t = 0; t < a.nterms; ++t) {
-    const double *src = a.src[t] + (long long)io0 * a.s[t][o0] + (long long)io1 * a.s[t][o1] +
-                        (long long)id_ld * a.s[t][D];
+    const double *base = a.src[t] + (long long)io0 * a.s[t][o0] + (long long)io1 * a.s[t][o1];
+    if (a.s[t][3] == 1) {
+      // a term with unit stride along i3 reads the output's own positions:
+      // coalesced along i3 without the shared-memory transpose
+      double v[R / 32][4];
+#pragma unroll
+      for (int h = 0; h < R / 32; ++h)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int i3 = b3 * R + tx + 32 * h, id = bd * 32 + ty + 8 * k;
+          v[h][k] = (i3 < a.n[3] && id < nd) ? __ldg(base + i3 + (long long)id * a.s[t][D]) : 0.0;
+        }
+#pragma unroll
+      for (int h = 0; h < R / 32; ++h)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[h][k] += a.alpha[t] * v[h][k];
+      continue;
+    }
+    const double *src = base + (long long)id_ld * a.s[t][D];
     double v[kL];
 #pragma unroll
     for (int k = 0; k < kL; ++k) {
       const int i3 = b3 * R + ty + 8 * k;
       v[k] = (i3 < a.n[3] && id_ld < nd) ? __ldg(src + (long long)i3 * a.s[t][3]) : 0.0;
     }
-    if (t) __syncthreads();  // the previous term's tile is consumed
+    if (tile_used) __syncthreads();  // the previous transposed term's tile is consumed
 #pragma unroll
     for (int k = 0; k < kL; ++k) tile[tx][ty + 8 * k] = v[k];
     __syncthreads();
+    tile_used = true;
 #pragma unroll
     for (int h = 0; h < R / 32; ++h)
 #pragma unroll
@@ -198,8 +218,8 @@ __global__ void __launch_bounds__(256) k_permute_tiled(double *__restrict__ out,
 template <bool S>
 static void permute_launch(double *out, PermArgs &a, const PermSpec &spec, long long total,
                            const SplitOut &so, cudaStream_t st) {
-  // tiled path when the innermost output index is strided in every source and
-  // some other index has unit stride in all of them
+  // tiled path when the innermost output index is strided in some source and
+  // another index D has unit stride in every source that is strided along i3
   int D = -1;
   bool all_unit3 = true;
   for (int t = 0; t < spec.nterms; ++t)
@@ -208,7 +228,7 @@ static void permute_launch(double *out, PermArgs &a, const PermSpec &spec, long 
     for (int d = 0; d < 3 && D < 0; ++d) {
       bool ok = true;
       for (int t = 0; t < spec.nterms; ++t)
-        if (a.s[t][d] != 1) ok = false;
+        if (a.s[t][d] != 1 && a.s[t][3] != 1) ok = false;
       if (ok && a.n[d] >= 8) D = d;
     }
   }
@@ -383,8 +403,9 @@ void launch_tau(double *tau, const double *t2, const double *t1, double c, int o
 // (z2[i,j,a,b] + z2[j,i,b,a]) / 2 / (e_i + e_j - e_a - e_b).  A unit is one
 // pair i <= j and one 32 x 32 (a, b) tile: the [i,j] tile (rows a) and the
 // [j,i] tile (rows b) are loaded together into shared memory (8 loads in
-// flight per thread), then both output tiles are written with coalesced
-// stores (the [j,i] one through the transposed shared-memory read).
+// flight per thread); each element is divided once and both output tiles
+// are written with coalesced stores (the [j,i] one through the transposed
+// shared-memory read of the results).
 __global__ void __launch_bounds__(256)
     k_newt(double *__restrict__ t2n, const double *__restrict__ z2, double *__restrict__ t1n,
            const double *__restrict__ z1, const double *__restrict__ eo,
@@ -423,20 +444,22 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     const double eij = eo[i] + eo[j];
+    const double evb = b0 + tx < v ? ev[b0 + tx] : 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int al = ty + 8 * k, a = a0 + al, b = b0 + tx;
-      if (a < v && b < v)
-        wij[(long long)a * v + b] =
-            0.5 * (tz[0][al][tx] + tz[1][tx][al]) / (eij - ev[a] - ev[b]);
+      if (a < v && b < v) {
+        const double x = 0.5 * (tz[0][al][tx] + tz[1][tx][al]) / (eij - ev[a] - evb);
+        wij[(long long)a * v + b] = x;
+        tz[0][al][tx] = x;  // this thread's own position: no other thread reads it
+      }
     }
     if (i == j) continue;  // block-uniform
+    __syncthreads();
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
-      if (a < v && b < v)
-        wji[(long long)b * v + a] =
-            0.5 * (tz[0][tx][bl] + tz[1][bl][tx]) / (eij - ev[a] - ev[b]);
+      if (a < v && b < v) wji[(long long)b * v + a] = tz[0][tx][bl];
     }
   }
 }
@@ -780,15 +803,20 @@ __global__ void __launch_bounds__(kPbThreads)
 #pragma unroll
     for (int q = 0; q < kPbPer; ++q) x1[q] = x2[q] = 0.0;
     for (int k = 0; k < n; ++k) {
+      // all loads of a history vector issued before its products are added
       const double *y = hp.p[k];
       const double ck = cs[k];
+      double y1[kPbPer], y2[kPbPer];
 #pragma unroll
       for (int q = 0; q < kPbPer; ++q) {
         const int ab = ab0 + q * kPbThreads;
-        if (ab < P.vv) {
-          x1[q] += ck * y[g1 + ab];
-          if (off) x2[q] += ck * y[g2 + ab];
-        }
+        y1[q] = ab < P.vv ? y[g1 + ab] : 0.0;
+        y2[q] = ab < P.vv && off ? y[g2 + ab] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < kPbPer; ++q) {
+        x1[q] += ck * y1[q];
+        x2[q] += ck * y2[q];
       }
     }
 #pragma unroll
