@@ -128,10 +128,11 @@ struct Geom {
   static constexpr int kBRows = TBN / CG;                   // B rows per CTA
   static constexpr int kTileB = kBRows * TBK * 2;
   static constexpr int kStage = 2 * TILE_A + 2 * kTileB;    // hi+lo of A and B
-  static constexpr int kStages = (kSmemLimit - 1024 - 256) / kStage;
-  static constexpr int kSmem = kStages * kStage + 1024 + 256;  // + alignment + barriers
+  static constexpr int kBarArea = 512;
+  static constexpr int kStages = (kSmemLimit - 1024 - kBarArea) / kStage;
+  static constexpr int kSmem = kStages * kStage + 1024 + kBarArea;  // + alignment + barriers
   static_assert(kSmem <= kSmemLimit && kStages >= 3, "pipeline depth");
-  static_assert(3 * kStages * 8 + 64 + 8 <= 256, "barrier area");
+  static_assert(3 * kStages * 8 + 64 + 8 <= kBarArea, "barrier area");
 };
 // (3 stages at TBK 64 or 6/7 at TBK 32 for one CTA per tile, 4 at TBK 64 for pairs)
 // k tiles per FP32 accumulation chunk, by the contraction length K: 512 K

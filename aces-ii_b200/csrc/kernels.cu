@@ -275,14 +275,35 @@ static void perm_args(PermArgs &a, const PermSpec &spec, long long &total) {
   }
   a.nterms = spec.nterms;
   a.beta = spec.beta;
-  a.fd1 = FastDiv((unsigned)a.n[1]);
-  a.fd2 = FastDiv((unsigned)a.n[2]);
-  a.fd3 = FastDiv((unsigned)a.n[3]);
   for (int t = 0; t < 4; ++t) {
     a.src[t] = t < spec.nterms ? spec.t[t].src : nullptr;
     a.alpha[t] = t < spec.nterms ? spec.t[t].alpha : 0.0;
     for (int k = 0; k < 4; ++k) a.s[t][k] = t < spec.nterms ? spec.t[t].s[k] : 0;
   }
+  // merge adjacent output indices k, k+1 that every source also reads as one
+  // run (s[k] = s[k+1] n[k+1]): e.g. tau[m,n,a,b] -> [a,b,(m,n)] becomes a
+  // plain 2-index transpose whose inner extent o^2 fills the resort tiles
+  int k = 2;
+  while (k >= 0) {
+    bool ok = a.n[k] > 1 && (long long)a.n[k] * a.n[k + 1] < (1LL << 31);
+    for (int t = 0; t < a.nterms && ok; ++t)
+      if (a.s[t][k] != a.s[t][k + 1] * a.n[k + 1]) ok = false;
+    if (!ok) {
+      --k;
+      continue;
+    }
+    a.n[k + 1] *= a.n[k];
+    for (int j = k; j > 0; --j) {
+      a.n[j] = a.n[j - 1];
+      for (int t = 0; t < 4; ++t) a.s[t][j] = a.s[t][j - 1];
+    }
+    a.n[0] = 1;
+    for (int t = 0; t < 4; ++t) a.s[t][0] = 0;
+    // the merged index (now at k + 1) may merge again with the one now at k
+  }
+  a.fd1 = FastDiv((unsigned)a.n[1]);
+  a.fd2 = FastDiv((unsigned)a.n[2]);
+  a.fd3 = FastDiv((unsigned)a.n[3]);
 }
 
 int permute(double *out, const PermSpec &spec, cudaStream_t st) {
