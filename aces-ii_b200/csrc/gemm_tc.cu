@@ -236,7 +236,7 @@ __device__ __forceinline__ bool mbar_wait_cl(uint32_t bar, uint32_t parity) {
   return true;
 }
 // waits on barriers that the other CTA of a pair may complete (tcgen05
-// commits multicast by rank 0, relayed copies, remote epilogue arrivals)
+// commits multicast by rank 0, its copies, remote epilogue arrivals)
 template <int CG>
 __device__ __forceinline__ bool mbar_wait_g(uint32_t bar, uint32_t parity) {
   return CG == 2 ? mbar_wait_cl(bar, parity) : mbar_wait(bar, parity);
@@ -258,6 +258,19 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
 __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::
                    : "memory");
+}
+// the same load issued by either CTA of a pair, completing on a barrier of
+// rank 0 (shared::cluster address); the data lands in the issuing CTA
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                                 uint32_t cluster_bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(cluster_bar)
+      : "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t cluster_addr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
 }
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
                                             uint32_t bar) {
@@ -427,14 +440,16 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
 //
 // CG = 2: clusters of two CTAs (ranks 0 and 1) share 256 x 128 tiles.  Each
 // CTA's producer loads its 128 A rows and its half of the B rows (as many as
-// the tile's MMA N needs: rows n0 + rank * N/2 on) into its own shared memory
-// and its own `full` barrier; warp 1 of rank 1 relays the completion of each
-// of its stages to rank 0's `full2` barrier, and warp 1 of rank 0 issues the
-// cta_group::2 products (reading both CTAs' tiles) once both have landed.
+// the tile's MMA N needs: rows n0 + rank * N/2 on) into its own shared memory;
+// all copies of a stage complete on rank 0's `full` barrier, which rank 0's
+// producer arms with both CTAs' bytes, and warp 1 of rank 0 issues the
+// cta_group::2 products (reading both CTAs' tiles) when it completes.
 // Product completion is multicast to both CTAs' `empty`, `acc_full` and
 // `mma_done` barriers; both CTAs' epilogues drain their own TMEM rows and
-// arrive on rank 0's `acc_empty`.  Every CTA waits only on barriers it owns
-// for copies it issued, so a CTA never leaves with its own copies in flight.
+// arrive on rank 0's `acc_empty`.  Teardown: rank 1 reports how many stages
+// it issued; after a cluster barrier rank 0 arms and waits out (bounded)
+// any of them it did not arm itself (only after a wait gave up), so neither
+// CTA leaves while a copy of the pair is in flight.
 template <int CG>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
@@ -447,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * kStage);
   uint64_t *full = bars;                               // [kStages] TMA -> MMA (own copies)
   uint64_t *empty = bars + kStages;                    // [kStages] MMA -> TMA
-  uint64_t *full2 = bars + 2 * kStages;                // [kStages] rank 1's copies (rank 0)
+  uint32_t *peer_issued = reinterpret_cast<uint32_t *>(bars + 2 * kStages);  // rank 1's stages
   uint64_t *acc_full = bars + 3 * kStages;             // [kNAcc] MMA -> epilogue
   uint64_t *acc_empty = acc_full + kNAcc;              // [kNAcc] epilogue -> MMA
   uint64_t *mma_done = acc_full + 2 * kNAcc;           // all products retired (teardown)
@@ -464,7 +479,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
-      mbar_init(smem_u32(&full2[s]), 1);
     }
     for (int b = 0; b < kNAcc; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
@@ -472,6 +486,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     mbar_init(smem_u32(mma_done), 1);
     *abort_flag = 0;
+    *peer_issued = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -526,7 +541,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const uint32_t fb = smem_u32(&full[s]);
         unsigned char *st = smem + s * kStage;
-        mbar_expect_tx(fb, kStage);
+        // a pair's stage completes on rank 0's barrier, armed with both halves
+        if (rank == 0) mbar_expect_tx(fb, CG * kStage);
         const int gk = ktb + kt;  // global k tile -> segment and its local k offset
         int sg = 0;
         while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
@@ -538,34 +554,34 @@ __global__ void __launch_bounds__(kThreads, 1)
             ya += rA[q];
             yb += rB[q];
           }
-        tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb);
-        tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, yb, fb);
-        tma_load_2d(smem_u32(st + 2 * TILE_A + kTileB), &L.bl[T.g][sg], kx, yb, fb);
+        if (CG == 1) {
+          tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb);
+          tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb);
+          tma_load_2d(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, yb, fb);
+          tma_load_2d(smem_u32(st + 2 * TILE_A + kTileB), &L.bl[T.g][sg], kx, yb, fb);
+        } else {
+          const uint32_t fb0 = mapa_rank(fb, 0);
+          tma_load_2d_pair(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb0);
+          tma_load_2d_pair(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb0);
+          tma_load_2d_pair(smem_u32(st + 2 * TILE_A), &L.bh[T.g][sg], kx, yb, fb0);
+          tma_load_2d_pair(smem_u32(st + 2 * TILE_A + kTileB), &L.bl[T.g][sg], kx, yb, fb0);
+        }
         ++it;
       }
     }
-    // drain: the most recent phase of every stage still possibly in flight
-    const int first = it > kStages ? it - kStages : 0;
-    for (int k = first; k < it; ++k)
-      if (!mbar_wait(smem_u32(&full[k % kStages]), (k / kStages) & 1))
-        atomicExch(&g_tc_status, 2);
-  } else if (warp == 1 && lane == 0 && rank == 1) {
-    // ---------------- relay (rank 1): its landed stages -> rank 0's full2 ----------------
-    int it = 0;
-    bool ok = *(volatile int *)&g_tc_inject == 0;
-    for (int t = t0; t < nTiles && ok; t += tstep) {
-      const int kTiles = decode_tile<CG>(L, t).kTiles;
-      for (int kt = 0; kt < kTiles; ++kt, ++it) {
-        const int s = it % kStages;
-        if (!mbar_wait(smem_u32(&full[s]), (it / kStages) & 1) || *(volatile int *)abort_flag) {
-          atomicExch(&g_tc_status, 7);
-          ok = false;
-          break;
-        }
-        mbar_arrive_cluster(mapa_rank(smem_u32(&full2[s]), 0));
-      }
+    if (rank == 0) {
+      // drain: the most recent phase of every stage still possibly in flight
+      const int first = it > kStages ? it - kStages : 0;
+      for (int k = first; k < it; ++k)
+        if (!mbar_wait_g<CG>(smem_u32(&full[k % kStages]), (k / kStages) & 1))
+          atomicExch(&g_tc_status, 2);
+      *(volatile int *)&peer_issued[1] = it;  // the stages this CTA armed
+    } else {
+      // rank 0 accounts for this CTA's copies at teardown
+      st_cluster_u32(mapa_rank(smem_u32(peer_issued), 0), (uint32_t)it);
     }
+  } else if (warp == 1 && lane == 0 && rank == 1) {
+    // rank 1 issues no products: its TMEM is released after rank 0's last one
     if (!mbar_wait_g<CG>(smem_u32(mma_done), 0)) atomicExch(&g_tc_status, 6);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer (rank 0) ----------------
@@ -585,8 +601,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         const int s = it % kStages;
-        if (!mbar_wait(smem_u32(&full[s]), (it / kStages) & 1) ||
-            (CG == 2 && !mbar_wait_g<CG>(smem_u32(&full2[s]), (it / kStages) & 1))) {
+        if (!mbar_wait_g<CG>(smem_u32(&full[s]), (it / kStages) & 1)) {
           atomicExch(&g_tc_status, 3);
           *(volatile int *)abort_flag = 1;
           stop = true;
@@ -728,9 +743,24 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  // a CTA of a pair leaves only when the other has no more product, copy
-  // relay or arrive aimed at it
-  if constexpr (CG == 2) cluster_sync();
+  if constexpr (CG == 2) {
+    cluster_sync();  // rank 1's count of issued stages is in peer_issued[0]
+    if (rank == 0 && threadIdx.x == 0) {
+      // stages rank 1 issued that this CTA never armed (possible only after
+      // a wait gave up): arm them with rank 1's bytes and wait them out
+      const int mine = (int)*(volatile uint32_t *)&peer_issued[1];
+      const int theirs = (int)*(volatile uint32_t *)&peer_issued[0];
+      for (int k = mine; k < theirs; ++k) {
+        const uint32_t fb = smem_u32(&full[k % kStages]);
+        mbar_expect_tx(fb, kStage);
+        if (!mbar_wait_g<CG>(fb, (k / kStages) & 1)) atomicExch(&g_tc_status, 8);
+      }
+    }
+    __syncthreads();
+    // a CTA of a pair leaves only when no copy, product or arrive of the pair
+    // can still reach its shared memory
+    cluster_sync();
+  }
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if constexpr (CG == 1)
