@@ -269,60 +269,6 @@ __device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(cluster_bar)
       : "memory");
 }
-// one 16-byte FP32 reduction (four consecutive elements, 16-byte aligned)
-__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
-               "f"(d)
-               : "memory");
-}
-// v[j0 + k] for a run-time k in 0..3 (selects, no local-memory indexing)
-template <int J0, int N>
-__device__ __forceinline__ float pick4(const float (&v)[N], int k) {
-  return k == 0 ? v[J0] : (k == 1 ? v[J0 + 1] : (k == 2 ? v[J0 + 2] : v[J0 + 3]));
-}
-// FP32 accumulation (beta = 1, RED) of one warp's 32 rows x kCols columns:
-// each group of four lanes (four consecutive rows) exchanges its values by
-// shuffles so that lane q holds the four rows of column j0 + q, and issues one
-// 16-byte RED per column when the group's rows are consecutive in memory and
-// 16-byte aligned; other columns and rows keep one RED per element.  Every
-// element is added once either way.
-template <int J0, int N>
-__device__ __forceinline__ void red_rows_group(const float (&acc)[N], float *base, float *cm,
-                                               const long long (&off)[4], bool live, bool grp,
-                                               int ncol, int q, int g0) {
-  float r[4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    // this lane gives column J0 + ((q - p) & 3) to lane g0 + ((q - p) & 3)
-    // and receives row (q + p) & 3 of column J0 + q
-    const float give = pick4<J0>(acc, (q - p) & 3);
-    const float got = __shfl_sync(0xffffffffu, give, g0 + ((q + p) & 3));
-    const int rr = (q + p) & 3;
-    r[0] = rr == 0 ? got : r[0];
-    r[1] = rr == 1 ? got : r[1];
-    r[2] = rr == 2 ? got : r[2];
-    r[3] = rr == 3 ? got : r[3];
-  }
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const bool vec = grp && (off[c] & 3) == 0 && J0 + c < ncol;
-    if (!vec && live && J0 + c < ncol) atomicAdd(cm + off[c], acc[J0 + c]);
-  }
-  const long long oq = q == 0 ? off[0] : (q == 1 ? off[1] : (q == 2 ? off[2] : off[3]));
-  if (grp && (oq & 3) == 0 && J0 + q < ncol) red_add_v4(base + oq, r[0], r[1], r[2], r[3]);
-}
-template <int J0, int N>
-__device__ __forceinline__ void red_rows(const float (&acc)[N], float *base, float *cm,
-                                         CViewNWalk &w, bool live, bool grp, int ncol, int q,
-                                         int g0) {
-  if constexpr (J0 < N) {
-    long long off[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c, w.next()) off[c] = w.off;
-    red_rows_group<J0>(acc, base, cm, off, live, grp, ncol, q, g0);
-    red_rows<J0 + 4>(acc, base, cm, w, live, grp, ncol, q, g0);
-  }
-}
 __device__ __forceinline__ void st_cluster_u32(uint32_t cluster_addr, uint32_t v) {
   asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
 }
@@ -504,7 +450,7 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
 // it issued; after a cluster barrier rank 0 arms and waits out (bounded)
 // any of them it did not arm itself (only after a wait gave up), so neither
 // CTA leaves while a copy of the pair is in flight.
-template <int CG, bool F32>
+template <int CG>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
                   double *__restrict__ part) {
@@ -737,38 +683,25 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (!ok) break;
       const int m = m0 + row;
-      if (ncol <= 0) continue;  // warp-uniform
+      if (m >= M || ncol <= 0) continue;
       const int nb = n0 + half * kCols;
-      if (F32 && beta != 0.0) {
-        // FP32 accumulate (batched (T) W, beta = 1): the whole warp takes part
-        const bool live = m < M;
-        const long long coff = P.batch ? __ldg(&P.batch[T.b].coff) : 0LL;
-        const long long mo = live ? cview_dim(C.mdiv, C.sm1, C.sm0, m) : -1;
-        const int q = lane & 3, g0 = lane & ~3;
-        const long long mo0 = __shfl_sync(0xffffffffu, mo, g0);
-        const bool mine = live && mo == mo0 + q && ((coff + mo0) & 3) == 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, mine);
-        const bool grp = ((bal >> g0) & 0xFu) == 0xFu;
-        float *const f = reinterpret_cast<float *>(C.p) + coff;
-        float fv[kCols];
-#pragma unroll
-        for (int j = 0; j < kCols; ++j) fv[j] = (float)(alpha * acc[j]);
-        CViewNWalk w(C, nb);
-        red_rows<0>(fv, f + mo0, f + (live ? mo : 0), w, live, grp, ncol, q, g0);
-        continue;
-      }
-      if (m >= M) continue;
-      if constexpr (F32) {
-        // FP32 output (batched (T) W), beta = 0: plain stores
+      if (P.f32out) {
+        // FP32 output (batched (T) W): plain stores for beta = 0, one RED per
+        // element for beta = 1 (single owner, so it equals load + add + store)
         float *const cm = reinterpret_cast<float *>(C.p) +
                           (P.batch ? __ldg(&P.batch[T.b].coff) : 0LL) +
                           cview_dim(C.mdiv, C.sm1, C.sm0, m);
         CViewNWalk w(C, nb);
+        if (beta == 0.0) {
 #pragma unroll
-        for (int j = 0; j < kCols; ++j, w.next())
-          if (j < ncol) cm[w.off] = (float)(alpha * acc[j]);
-      } else {
-      if (part) {
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) cm[w.off] = (float)(alpha * acc[j]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < kCols; ++j, w.next())
+            if (j < ncol) atomicAdd(cm + w.off, (float)(alpha * acc[j]));
+        }
+      } else if (part) {
         // split-K partial, [z][n][m]: lanes write consecutive m
         double *pz = part + (size_t)z * M * N + m;
 #pragma unroll
@@ -805,7 +738,6 @@ __global__ void __launch_bounds__(kThreads, 1)
               if (j0 + j < ncol) cm[off[j]] = alpha * acc[j0 + j] + beta * old[j];
           }
         }
-      }
       }
     }
   }
@@ -1003,8 +935,7 @@ int max_pairs() {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_gemm_bf16x3<2, false>, &cfg) != cudaSuccess ||
-        n <= 0) {
+    if (cudaOccupancyMaxActiveClusters(&n, k_gemm_bf16x3<2>, &cfg) != cudaSuccess || n <= 0) {
       cudaGetLastError();
       n = num_sms() / 2;
     }
@@ -1023,15 +954,6 @@ std::atomic<int> g_tc_pairs{0};
 bool pairs_for(int min_rows) { return g_tc_pairs.load() != 0 && min_rows >= 2 * TBM; }
 
 int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
-  // FP32 outputs (batched (T) W) run in their own instantiation, whose
-  // epilogue has only the FP32 paths (and the FP64 one only the FP64 paths)
-  bool f32 = false;
-  for (int g = 0; g < L.nprob; ++g) f32 = f32 || L.prob[g].f32out != 0;
-  for (int g = 0; g < L.nprob; ++g)
-    if ((L.prob[g].f32out != 0) != f32) {
-      set_error("gemm_nt_bf16x3: FP32 and FP64 outputs in one launch");
-      return ACES_ERR_ARG;
-    }
   // the shared-memory opt-in and the status word are per device
   static bool attr[64] = {false};
   int dev = 0;
@@ -1041,14 +963,10 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     return ACES_ERR_ARG;
   }
   if (!attr[dev]) {
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<1>::kSmem));
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2, false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<2>::kSmem));
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<1>::kSmem));
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2, true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<2>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<1>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<2>::kSmem));
     int zero = 0;
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
     attr[dev] = true;
@@ -1067,16 +985,10 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (f32)
-      ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2, true>, L, alpha, beta, part));
-    else
-      ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2, false>, L, alpha, beta, part));
+    ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2>, L, alpha, beta, part));
   } else {
     const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
-    if (f32)
-      k_gemm_bf16x3<1, true><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
-    else
-      k_gemm_bf16x3<1, false><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
+    k_gemm_bf16x3<1><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
   }
   count_launch();
   ACES_CUDA(cudaGetLastError());
