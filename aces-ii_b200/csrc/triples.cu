@@ -165,9 +165,6 @@ __device__ __forceinline__ void decode_set(int n, int &a, int &b, int &c) {
 // three distinct virtuals through the constant bilinear form, sets with a
 // repeated virtual through the general per-ordering sum.
 constexpr int kTile = 8;
-#ifndef ACES_TE_MINB
-#define ACES_TE_MINB 1
-#endif
 // kOrd[s][r] in device code: the first position is s / 2, the other two
 // follow in increasing order for even s and swapped for odd s
 __host__ __device__ __forceinline__ constexpr int ordpos(int s, int r) {
@@ -179,7 +176,7 @@ static_assert(ordpos(0, 2) == kOrd[0][2] && ordpos(3, 1) == kOrd[3][1] &&
                   ordpos(1, 1) == kOrd[1][1] && ordpos(2, 1) == kOrd[2][1],
               "ordpos restates kOrd");
 template <typename TW>
-__global__ void __launch_bounds__(128, ACES_TE_MINB)
+__global__ void __launch_bounds__(128)
     k_triples_energy_tiled(const TW *__restrict__ Wbase, long long wstride,
                            const int *__restrict__ trip3, const double *__restrict__ t1,
                            const double *__restrict__ Ioovv, const double *__restrict__ eo,
