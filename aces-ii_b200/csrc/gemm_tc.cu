@@ -181,14 +181,26 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 // try_wait with a suspend-time hint: a waiting thread sleeps until the phase
 // completes (or 20 us pass) instead of re-polling, which leaves the issue
 // slots of its SM sub-partition to the MMA and TMA threads
+#ifndef ACES_TC_HINT
+#define ACES_TC_HINT 20000
+#endif
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
+#if ACES_TC_HINT > 0
   asm volatile(
       "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity), "r"(20000u)
+      : "r"(bar), "r"(parity), "r"((uint32_t)ACES_TC_HINT)
       : "memory");
+#else
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+#endif
   return ok != 0;
 }
 // bounded wait: false on timeout
