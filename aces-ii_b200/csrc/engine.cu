@@ -1146,11 +1146,11 @@ int CCEngine::ladder_packed(const double *in, double *out) {
     pl.lo_m = (__nv_bfloat16 *)mm->op.lo;
     pl.kp_p = mp->op.k_pad;
     pl.kp_m = mm->op.k_pad;
-    launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st, &pl);
+    launch_ladder_pack_tau(taup.p, taum.p, in, v, oo, st, &pl);
     mp->valid = mm->valid = true;
     mp->fp64 = mm->fp64 = false;
   } else {
-    launch_ladder_pack_tau(taup.p, taum.p, in, (const int *)ladpairs.p, v, oo, st);
+    launch_ladder_pack_tau(taup.p, taum.p, in, v, oo, st);
   }
   // both products in one grouped launch (their tiles fill each other's last wave)
   const GArgs g[2] = {{np, oo, np, Up.p, np, taup.p, np, cview_colmajor(Sld.p, np), true, false},

@@ -1091,76 +1091,129 @@ void launch_ladder_pack_v(double *Up, double *Um, const double *V, const int *pa
 
 // tau+[ij][p(c,d)] = tau[ij][cd] + tau[ij][dc] (c < d), tau[ij][cc];
 // tau-[ij][m(c,d)] = tau[ij][cd] - tau[ij][dc]
-// S: tau+ and tau- go straight to the BF16 planes of the ladder's B operands
-// (rows ij, k_pad apart) instead of FP64 arrays
+// tau+[ij][p(c,d)] = tau[ij][c][d] + tau[ij][d][c] (c < d), tau[ij][c][c] (c = d) and
+// tau-[ij][m(c,d)] = tau[ij][c][d] - tau[ij][d][c] (c < d), with the packed
+// indices p(c,d) = d(d+1)/2 + c and m(c,d) = d(d-1)/2 + c.  A block takes one
+// ij and one 32 x 32 tile pair (c tile <= d tile): the [d][c] tile is read
+// with lanes along c (the packed outputs' order), the [c][d] tile with lanes
+// along d and transposed through shared memory, so every load and store is
+// coalesced.  S: tau+- go straight to the BF16 planes of the ladder's B
+// operands (rows ij, k_pad apart) instead of FP64 arrays.
 template <bool S>
-__global__ void k_ladder_pack_tau(double *__restrict__ tp, double *__restrict__ tm,
-                                  const double *__restrict__ tau, const int *__restrict__ pairs,
-                                  int v, int noo, LadderPlanes pl) {
+__global__ void __launch_bounds__(256)
+    k_ladder_pack_tau(double *__restrict__ tp, double *__restrict__ tm,
+                      const double *__restrict__ tau, int v, int noo, LadderPlanes pl) {
+  __shared__ double X[32][33];  // [c local][d local] of tau[ij][c][d]
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
   const size_t vv = (size_t)v * v;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  // tile pair index -> (ct <= dt), dt-major
+  int dt = (int)((sqrtf(8.0f * blockIdx.x + 1.0f) - 1.0f) * 0.5f);
+  while (dt * (dt + 1) / 2 > (int)blockIdx.x) --dt;
+  while ((dt + 1) * (dt + 2) / 2 <= (int)blockIdx.x) ++dt;
+  const int ct = blockIdx.x - dt * (dt + 1) / 2;
+  const int c0 = ct * 32, d0 = dt * 32;
   for (int ij = blockIdx.y; ij < noo; ij += gridDim.y) {
     const double *t = tau + (size_t)ij * vv;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np + nm; q += gridDim.x * blockDim.x) {
-      const int c = pairs[2 * q], d = pairs[2 * q + 1];
-      const bool plus = q < np;
-      const double x = plus ? (c == d ? t[(size_t)c * v + c]
-                                      : t[(size_t)c * v + d] + t[(size_t)d * v + c])
-                            : t[(size_t)c * v + d] - t[(size_t)d * v + c];
-      if (!S) {
-        if (plus)
-          tp[(size_t)ij * np + q] = x;
-        else
-          tm[(size_t)ij * nm + (q - np)] = x;
-      } else {
-        __nv_bfloat16 h, l;
-        split_bf16(x, h, l);
-        const size_t at = plus ? (size_t)ij * pl.kp_p + q : (size_t)ij * pl.kp_m + (q - np);
-        (plus ? pl.hi_p : pl.hi_m)[at] = h;
-        (plus ? pl.lo_p : pl.lo_m)[at] = l;
+    double y[4];  // tau[d][c], lanes along c
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int cl = ty + 8 * k, c = c0 + cl, d = d0 + tx;
+      X[cl][tx] = (c < v && d < v) ? t[(size_t)c * v + d] : 0.0;
+      const int dd = d0 + ty + 8 * k, cc = c0 + tx;
+      y[k] = (dd < v && cc < v) ? t[(size_t)dd * v + cc] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int dl = ty + 8 * k, d = d0 + dl, c = c0 + tx;
+      if (c < v && d < v && c <= d) {
+        const double cd = X[tx][dl], dc = y[k];
+        const double plus = c == d ? cd : cd + dc;
+        const size_t ip = (size_t)ij * np + (size_t)d * (d + 1) / 2 + c;
+        if (!S) {
+          tp[ip] = plus;
+          if (c < d) tm[(size_t)ij * nm + (size_t)d * (d - 1) / 2 + c] = cd - dc;
+        } else {
+          __nv_bfloat16 h, l;
+          split_bf16(plus, h, l);
+          const size_t ap = (size_t)ij * pl.kp_p + (size_t)d * (d + 1) / 2 + c;
+          pl.hi_p[ap] = h;
+          pl.lo_p[ap] = l;
+          if (c < d) {
+            split_bf16(cd - dc, h, l);
+            const size_t am = (size_t)ij * pl.kp_m + (size_t)d * (d - 1) / 2 + c;
+            pl.hi_m[am] = h;
+            pl.lo_m[am] = l;
+          }
+        }
       }
     }
+    __syncthreads();  // X is reused by the next ij
   }
 }
 
-void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
-                            int noo, cudaStream_t st, const LadderPlanes *planes) {
-  const int n = v * v;
-  dim3 grid((unsigned)std::min((n + 255) / 256, 64), (unsigned)std::min(noo, 65535));
+void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, int v, int noo,
+                            cudaStream_t st, const LadderPlanes *planes) {
+  const int tiles = (v + 31) / 32;
+  dim3 grid((unsigned)(tiles * (tiles + 1) / 2), (unsigned)std::min(noo, 65535));
   if (planes)
-    k_ladder_pack_tau<true><<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo, *planes);
+    k_ladder_pack_tau<true><<<grid, 256, 0, st>>>(tp, tm, tau, v, noo, *planes);
   else
-    k_ladder_pack_tau<false><<<grid, 256, 0, st>>>(tp, tm, tau, pairs, v, noo, LadderPlanes());
+    k_ladder_pack_tau<false><<<grid, 256, 0, st>>>(tp, tm, tau, v, noo, LadderPlanes());
   count_launch();
 }
 
-// Z2[ij][a][b] += S[ij][p] + A[ij][m] (a < b), S - A (a > b), S[ij][p(a,a)] (a = b)
-__global__ void k_ladder_unpack(double *__restrict__ Z2, const double *__restrict__ S,
-                                const double *__restrict__ A, int v, int noo) {
+// Z2[ij][a][b] += S[ij][p] + A[ij][m] (a < b), S - A (a > b), S[ij][p(a,a)] (a = b).
+// A block takes one ij and one 32 x 32 tile pair (a tile <= b tile): S and A
+// are read with lanes along a (their packed order), Z2[b][a] is updated with
+// lanes along a and Z2[a][b] through a shared-memory transpose with lanes
+// along b, so every access is coalesced.
+__global__ void __launch_bounds__(256)
+    k_ladder_unpack(double *__restrict__ Z2, const double *__restrict__ S,
+                    const double *__restrict__ A, int v, int noo) {
+  __shared__ double P[32][33];  // S + A at [b local][a local]
   const int np = v * (v + 1) / 2, nm = v * (v - 1) / 2;
   const size_t vv = (size_t)v * v;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  int bt = (int)((sqrtf(8.0f * blockIdx.x + 1.0f) - 1.0f) * 0.5f);
+  while (bt * (bt + 1) / 2 > (int)blockIdx.x) --bt;
+  while ((bt + 1) * (bt + 2) / 2 <= (int)blockIdx.x) ++bt;
+  const int at = blockIdx.x - bt * (bt + 1) / 2;
+  const int a0 = at * 32, b0 = bt * 32;
   for (int ij = blockIdx.y; ij < noo; ij += gridDim.y) {
     double *z = Z2 + (size_t)ij * vv;
     const double *s = S + (size_t)ij * np, *an = A + (size_t)ij * nm;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < v * v; e += gridDim.x * blockDim.x) {
-      const int a = e / v, b = e - a * v;
-      double x;
-      if (a == b) {
-        x = s[a * (a + 1) / 2 + a];
-      } else if (a < b) {
-        x = s[b * (b + 1) / 2 + a] + an[b * (b - 1) / 2 + a];
-      } else {
-        x = s[a * (a + 1) / 2 + b] - an[a * (a - 1) / 2 + b];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int bl = ty + 8 * k, b = b0 + bl, a = a0 + tx;
+      double plus = 0.0;
+      if (a < v && b < v && a <= b) {
+        const double sv = s[(size_t)b * (b + 1) / 2 + a];
+        if (a == b) {
+          z[(size_t)a * v + a] += sv;
+        } else {
+          const double av = an[(size_t)b * (b - 1) / 2 + a];
+          z[(size_t)b * v + a] += sv - av;  // Z[b][a], lanes along a
+          plus = sv + av;
+        }
       }
-      z[e] += x;
+      P[bl][tx] = plus;
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int al = ty + 8 * k, a = a0 + al, b = b0 + tx;
+      if (a < v && b < v && a < b) z[(size_t)a * v + b] += P[tx][al];  // Z[a][b], lanes along b
+    }
+    __syncthreads();
   }
 }
 
 void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
                           cudaStream_t st) {
-  const int n = v * v;
-  dim3 grid((unsigned)std::min((n + 255) / 256, 64), (unsigned)std::min(noo, 65535));
+  const int tiles = (v + 31) / 32;
+  dim3 grid((unsigned)(tiles * (tiles + 1) / 2), (unsigned)std::min(noo, 65535));
   k_ladder_unpack<<<grid, 256, 0, st>>>(Z2, S, A, v, noo);
   count_launch();
 }

@@ -99,9 +99,11 @@ struct LadderPlanes {
   __nv_bfloat16 *hi_p = nullptr, *lo_p = nullptr, *hi_m = nullptr, *lo_m = nullptr;
   int kp_p = 0, kp_m = 0;
 };
-// with planes: tau+ / tau- written only as the planes (tp, tm untouched)
-void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, const int *pairs, int v,
-                            int noo, cudaStream_t st, const LadderPlanes *planes = nullptr);
+// tau+ / tau- of the C1 ladder in the packed order p(c,d) = d(d+1)/2 + c,
+// m(c,d) = d(d-1)/2 + c (the order of `pairs` in launch_ladder_pack_v); with
+// planes: written only as the planes (tp, tm untouched)
+void launch_ladder_pack_tau(double *tp, double *tm, const double *tau, int v, int noo,
+                            cudaStream_t st, const LadderPlanes *planes = nullptr);
 void launch_ladder_unpack(double *Z2, const double *S, const double *A, int v, int noo,
                           cudaStream_t st);
 
