@@ -194,6 +194,43 @@ const double *CCEngine::transposed(const double *src, int rows, int cols, long l
   return dst->p;
 }
 
+const double *CCEngine::tape_transposed(const double *src, int rows, int cols, long long ld) {
+  const auto key = std::make_tuple(src, rows, cols, ld);
+  auto it = tape_tcache.find(key);
+  if (it != tape_tcache.end()) return it->second.p;
+  DBuf fresh;
+  if (alloc(fresh, (size_t)rows * cols) != ACES_OK) return nullptr;
+  PermSpec s;
+  s.n[0] = 1; s.n[1] = 1; s.n[2] = cols; s.n[3] = rows;
+  s.nterms = 1;
+  s.beta = 0.0;
+  s.t[0].src = src;
+  s.t[0].alpha = 1.0;
+  s.t[0].s[0] = 0; s.t[0].s[1] = 0; s.t[0].s[2] = 1; s.t[0].s[3] = ld;
+  if (permute(fresh.p, s, st) != ACES_OK) {
+    dev_free(fresh.p);
+    return nullptr;
+  }
+  tape_tcache[key] = fresh;
+  return fresh.p;
+}
+
+void CCEngine::tape_cache_clear() {
+  for (auto &kv : tape_tcache) {
+    const double *p = kv.second.p;
+    for (auto e = split_cache.begin(); e != split_cache.end();) {
+      if (e->src == p) {
+        if (e->op.hi) dev_free(e->op.hi);
+        e = split_cache.erase(e);
+      } else {
+        ++e;
+      }
+    }
+    if (kv.second.p) dev_free(kv.second.p);
+  }
+  tape_tcache.clear();
+}
+
 int CCEngine::backward() {
   // walk the tape in reverse; adjoint buffers already hold the seeds
   const bool rec = recording;
@@ -208,21 +245,25 @@ int CCEngine::backward() {
       if (op.a_act || op.b_act) {
         ACES_TRY(tmp(bwdC, (size_t)op.M * op.N));
         launch_view_gather(bwdC.p, cb, op.M, op.N, op.alpha, st);
+        // the forward operands are fixed for the tape's life (constants, or
+        // values recorded at the converged amplitudes): their transposes are
+        // cached, so are their splits
         if (op.a_act) {
           // A_bar[m,k] += sum_n Cd[m,n] B[n,k]
-          const double *Bt = transposed(op.B, op.N, op.K, op.ldb, !op.b_act, bwdB);
+          const double *Bt = op.b_act ? tape_transposed(op.B, op.N, op.K, op.ldb)
+                                      : transposed(op.B, op.N, op.K, op.ldb, true, bwdB);
           if (!Bt) return ACES_ERR_NOMEM;
-          // a constant operand's transpose is cached, so its split is too
           ACES_TRY(G(op.M, op.K, op.N, 1.0, bwdC.p, op.N, Bt, op.N, 1.0,
-                     cview_rowmajor(adj(op.A), op.lda), false, !op.b_act));
+                     cview_rowmajor(adj(op.A), op.lda), false, true));
         }
         if (op.b_act) {
           // B_bar[n,k] += sum_m Cd[m,n] A[m,k]
           const double *Cdt = transposed(bwdC.p, op.M, op.N, op.N, false, bwdD);
-          const double *At = transposed(op.A, op.M, op.K, op.lda, !op.a_act, bwdA);
+          const double *At = op.a_act ? tape_transposed(op.A, op.M, op.K, op.lda)
+                                      : transposed(op.A, op.M, op.K, op.lda, true, bwdA);
           if (!Cdt || !At) return ACES_ERR_NOMEM;
           ACES_TRY(G(op.N, op.K, op.M, 1.0, Cdt, op.M, At, op.M, 1.0,
-                     cview_rowmajor(adj(op.B), op.ldb), false, !op.a_act));
+                     cview_rowmajor(adj(op.B), op.ldb), false, true));
         }
       }
       if (op.beta == 0.0)

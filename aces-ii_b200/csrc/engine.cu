@@ -35,6 +35,8 @@ void CCEngine::release() {
   adjoint.clear();
   for (auto &kv : tcache) if (kv.second.p) dev_free(kv.second.p);
   tcache.clear();
+  for (auto &kv : tape_tcache) if (kv.second.p) dev_free(kv.second.p);
+  tape_tcache.clear();
   tape.clear();
   active.clear();
   for (DBuf *b : registry()) {

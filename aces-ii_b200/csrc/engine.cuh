@@ -151,6 +151,12 @@ class CCEngine {
   // transposes of constant operands, by (source, rows, cols, leading
   // dimension): one array can be the operand of contractions of several shapes
   std::map<std::tuple<const double *, int, int, long long>, DBuf> tcache;
+  // transposes of the recorded forward values the backward pass reads: fixed
+  // while the tape is (every Lambda iteration and EOM product replays the
+  // same tape), dropped with their cached splits when a pass is recorded
+  std::map<std::tuple<const double *, int, int, long long>, DBuf> tape_tcache;
+  const double *tape_transposed(const double *src, int rows, int cols, long long ld);
+  void tape_cache_clear();
   std::vector<const double *> symmetric;     // constant matrices equal to their transpose
   DBuf bwdA, bwdB, bwdC, bwdD;
   std::vector<DBuf *> registry();

@@ -22,6 +22,8 @@
 namespace acesb200 {
 
 int CCEngine::record_residual(bool fock_active) {
+  // the forward values the previous tape's backward pass cached may change
+  tape_cache_clear();
   tape.clear();
   active.clear();
   active.push_back(&X);
