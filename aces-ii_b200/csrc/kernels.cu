@@ -489,7 +489,17 @@ void launch_newt(double *t2n, const double *z2, double *t1n, const double *z1, c
                  const double *ev, int o, int v, cudaStream_t st) {
   const int tiles = (v + 31) / 32;
   const long long nunits = (long long)o * (o + 1) / 2 * tiles * tiles;
-  const unsigned grid = (unsigned)std::max(1LL, std::min(nunits, 148LL * 8));
+  // the blocks walk the units persistently: no more of them than stay
+  // resident together (a second wave would start its share late)
+  static int per_sm = 0;
+  if (!per_sm) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newt, 256, 0) != cudaSuccess ||
+        per_sm <= 0) {
+      cudaGetLastError();
+      per_sm = 4;
+    }
+  }
+  const unsigned grid = (unsigned)std::max(1LL, std::min(nunits, 148LL * per_sm));
   k_newt<<<grid, 256, 0, st>>>(t2n, z2, t1n, z1, eo, ev, o, v, tiles, nunits);
   count_launch();
 }
