@@ -244,6 +244,46 @@ __global__ void k_gemv_f64(int M, int K, double alpha, const double *__restrict_
   }
 }
 
+// Partial row sums for products with few rows: warp w takes row w / W and
+// the w % W-th K chunk of it (kc elements, a multiple of 128); the partials
+// go to part[row * W + chunk].
+__global__ void k_gemv_part(int M, int K, int W, int kc, const double *__restrict__ A,
+                            long long lda, const double *__restrict__ x,
+                            double *__restrict__ part) {
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= (long long)M * W) return;  // warp-uniform
+  const int m = (int)(warp / W), c = (int)(warp - (long long)m * W);
+  const int k0 = c * kc, k1 = min(K, k0 + kc);
+  const double *a = A + (long long)m * lda;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int k = k0 + lane;
+  for (; k + 96 < k1; k += 128) {
+    s0 += a[k] * __ldg(x + k);
+    s1 += a[k + 32] * __ldg(x + k + 32);
+    s2 += a[k + 64] * __ldg(x + k + 64);
+    s3 += a[k + 96] * __ldg(x + k + 96);
+  }
+  for (; k < k1; k += 32) s0 += a[k] * __ldg(x + k);
+  double t = (s0 + s1) + (s2 + s3);
+  for (int off = 16; off; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  if (lane == 0) part[warp] = t;
+}
+
+// y[m] = alpha * sum_c part[m * W + c] + beta * y[m], the chunks summed in order
+__global__ void k_gemv_final(int M, int W, double alpha, const double *__restrict__ part,
+                             double beta, CView C, bool transpose_out) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  double t = 0.0;
+  for (int c = 0; c < W; ++c) t += part[(long long)m * W + c];
+  const int mm = transpose_out ? 0 : m, nn = transpose_out ? m : 0;
+  double *cp = C.p + cview_off(C, mm, nn);
+  double r = alpha * t;
+  if (beta != 0.0) r += beta * *cp;
+  *cp = r;
+}
+
 // ---------------------------------------------------------------------------
 // Thin contractions (one output dimension S <= 32): out(l, s) = sum_k X[l,k] Y[s,k]
 // with X the long operand (L rows) and Y the short one.  64 x 32 output tile
@@ -526,6 +566,30 @@ int splitk_reduce(const CView &C, const double *part, int M, int N, int Z, doubl
 int gemv_f64(int M, int K, double alpha, const double *A, long long lda, const double *x,
              double beta, const CView &C, bool transpose_out, cudaStream_t st) {
   if (M <= 0) return ACES_OK;
+  // few rows: each row split over W warps (about 4736 warps in all, K chunks
+  // of at least 128), so the matrix streams with enough loads in flight
+  const long long kTargetWarps = 148 * 32;
+  if ((long long)M * 2 <= kTargetWarps && K >= 256) {
+    int W = (int)std::min<long long>(32, (kTargetWarps + M - 1) / M);
+    int kc = ((K + W - 1) / W + 127) / 128 * 128;
+    W = (K + kc - 1) / kc;
+    if (W > 1) {
+      double *part = splitk_workspace((size_t)M * W);
+      if (!part) {
+        set_error("gemv: partial-sum workspace allocation failed");
+        return ACES_ERR_NOMEM;
+      }
+      const long long nw = (long long)M * W;
+      k_gemv_part<<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(M, K, W, kc, A, lda, x,
+                                                                      part);
+      count_launch();
+      k_gemv_final<<<(unsigned)((M + 255) / 256), 256, 0, st>>>(M, W, alpha, part, beta, C,
+                                                                transpose_out);
+      count_launch();
+      ACES_CUDA(cudaGetLastError());
+      return ACES_OK;
+    }
+  }
   long long warps = M;
   long long nb = (warps * 32 + 255) / 256;
   if (nb > 148 * 32) nb = 148 * 32;
