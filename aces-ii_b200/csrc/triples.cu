@@ -175,48 +175,29 @@ static_assert(ordpos(0, 2) == kOrd[0][2] && ordpos(3, 1) == kOrd[3][1] &&
                   ordpos(4, 2) == kOrd[4][2] && ordpos(5, 0) == kOrd[5][0] &&
                   ordpos(1, 1) == kOrd[1][1] && ordpos(2, 1) == kOrd[2][1],
               "ordpos restates kOrd");
-// The staged data of one work item (a tile triple of one triplet).
 template <typename TW>
-struct EStage {
-  TW cube[6][kTile][kTile + 1][kTile + 1];
-  double It[3][6][kTile][kTile + 1];
-  double ts[3][3][kTile];  // [t_i, t_j, t_k][tile position][local]
-  double es[3][kTile];     // ev of the three tiles
-};
-
-// asynchronous global -> shared copies of 4 or 8 bytes; a false predicate
-// copies nothing and zero-fills (the source address is then not read)
-template <int B>
-__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool pred) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(B),
-               "r"(pred ? B : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait1() {
-  asm volatile("cp.async.wait_group 1;" ::: "memory");
-}
-
-// Issue the copies of work item w (triplet e = w / nblk, tile triple
-// w % nblk) into stage S.
-template <typename TW>
-__device__ __forceinline__ void estage_load(EStage<TW> &S, long long w, int nblk,
-                                            const TW *__restrict__ Wbase, long long wstride,
-                                            const int *__restrict__ trip3,
-                                            const double *__restrict__ t1,
-                                            const double *__restrict__ Ioovv,
-                                            const double *__restrict__ ev, int o, int v) {
-  const int e = (int)(w / nblk), tb = (int)(w - (long long)e * nblk);
-  const int i = __ldg(trip3 + 3 * e), j = __ldg(trip3 + 3 * e + 1), k = __ldg(trip3 + 3 * e + 2);
+__global__ void __launch_bounds__(128)
+    k_triples_energy_tiled(const TW *__restrict__ Wbase, long long wstride,
+                           const int *__restrict__ trip3, const double *__restrict__ t1,
+                           const double *__restrict__ Ioovv, const double *__restrict__ eo,
+                           const double *__restrict__ ev, int o, int v,
+                           double *__restrict__ part) {
+  __shared__ TW cube[6][kTile][kTile + 1][kTile + 1];
+  __shared__ double It[3][6][kTile][kTile + 1];
+  __shared__ double ts[3][3][kTile];   // [t_i, t_j, t_k][tile position][local]
+  __shared__ double es[3][kTile];      // ev of the three tiles
+  __shared__ double sh[2][4];
+  const int e = blockIdx.y;
+  const int i = trip3[3 * e], j = trip3[3 * e + 1], k = trip3[3 * e + 2];
   const TW *__restrict__ W = Wbase + (long long)e * wstride;
+  const int mult = (i == j && j == k) ? 6 : ((i == j || j == k) ? 2 : 1);
+  const double scale = 1.0 / (3.0 * mult);
   const long long v2 = (long long)v * v;
   int T[3];
-  decode_set(tb, T[0], T[1], T[2]);
+  decode_set((int)blockIdx.x, T[0], T[1], T[2]);
   const int b0[3] = {T[0] * kTile, T[1] * kTile, T[2] * kTile};
   const int tid = threadIdx.x;
+  // six cubes: cube s spans tiles (T[kOrd[s][0]], T[kOrd[s][1]], T[kOrd[s][2]])
 #pragma unroll
   for (int s = 0; s < 6; ++s) {
     const int c0 = b0[ordpos(s, 0)], c1 = b0[ordpos(s, 1)], c2 = b0[ordpos(s, 2)];
@@ -225,163 +206,82 @@ __device__ __forceinline__ void estage_load(EStage<TW> &S, long long w, int nblk
       const int idx = tid + 128 * q;
       const int x = idx >> 6, y = (idx >> 3) & 7, z = idx & 7;
       const int gx = c0 + x, gy = c1 + y, gz = c2 + z;
-      const bool in = gx < v && gy < v && gz < v;
-      cp_async_zfill<sizeof(TW)>(&S.cube[s][x][y][z],
-                                 in ? W + gx * v2 + (long long)gy * v + gz : W, in);
+      cube[s][x][y][z] = (gx < v && gy < v && gz < v) ? W[gx * v2 + (long long)gy * v + gz]
+                                                      : (TW)0;
     }
   }
+  // integral tiles: slab 0 = <jk|..>, 1 = <ik|..>, 2 = <ij|..>; ordered pair
+  // (x, y) of tile positions -> index x * 2 + (y > x ? y - 1 : y)
   const double *slab[3] = {Ioovv + ((long long)j * o + k) * v2, Ioovv + ((long long)i * o + k) * v2,
                            Ioovv + ((long long)i * o + j) * v2};
   for (int idx = tid; idx < 3 * 6 * 64; idx += 128) {
     const int sl = idx / 384, pr = (idx / 64) % 6, r = (idx >> 3) & 7, c = idx & 7;
     const int x = pr >> 1, yy = pr & 1, y = yy < x ? yy : yy + 1;
     const int gr = b0[x] + r, gc = b0[y] + c;
-    const bool in = gr < v && gc < v;
-    cp_async_zfill<8>(&S.It[sl][pr][r][c], in ? slab[sl] + (long long)gr * v + gc : slab[sl], in);
+    It[sl][pr][r][c] = (gr < v && gc < v) ? slab[sl][(long long)gr * v + gc] : 0.0;
   }
   if (tid < 72) {
-    const int wv = tid / 24, pos = (tid / 8) % 3, l = tid & 7;
-    const int occ = wv == 0 ? i : (wv == 1 ? j : k), g = b0[pos] + l;
-    cp_async_zfill<8>(&S.ts[wv][pos][l], g < v ? t1 + (long long)occ * v + g : t1, g < v);
+    const int w = tid / 24, pos = (tid / 8) % 3, l = tid & 7;
+    const int occ = w == 0 ? i : (w == 1 ? j : k), g = b0[pos] + l;
+    ts[w][pos][l] = g < v ? t1[(long long)occ * v + g] : 0.0;
   } else if (tid < 96) {
     const int pos = (tid - 72) / 8, l = tid & 7, g = b0[pos] + l;
-    cp_async_zfill<8>(&S.es[pos][l], g < v ? ev + g : ev, g < v);
+    es[pos][l] = g < v ? ev[g] : 0.0;
   }
-}
-
-// Persistent blocks walk the work items (tile triple x triplet of the batch);
-// the copies of the next item are in flight (double-buffered stages) while
-// the current one is evaluated.  Per item: the six permuted 8x8x8 cubes of W,
-// the 8x8 tiles of the three integral slabs, t1 rows and orbital energies,
-// then four sets {a >= b >= c} per thread from shared memory (sets of three
-// distinct virtuals through the constant bilinear form, sets with a repeated
-// virtual through the general per-ordering sum); per item one (E4, E5) pair
-// at slot e * nblk + tile triple.
-template <typename TW>
-__global__ void __launch_bounds__(128)
-    k_triples_energy_tiled(const TW *__restrict__ Wbase, long long wstride,
-                           const int *__restrict__ trip3, const double *__restrict__ t1,
-                           const double *__restrict__ Ioovv, const double *__restrict__ eo,
-                           const double *__restrict__ ev, int o, int v, int nblk, long long items,
-                           double *__restrict__ part) {
-  extern __shared__ __align__(16) unsigned char es_raw[];
-  EStage<TW> *stage = reinterpret_cast<EStage<TW> *>(es_raw);
-  __shared__ double sh[2][4];
-  const int tid = threadIdx.x;
-  long long w = blockIdx.x;
-  int b = 0;
-  if (w < items) estage_load(stage[0], w, nblk, Wbase, wstride, trip3, t1, Ioovv, ev, o, v);
-  cp_async_commit();
-  for (; w < items; w += gridDim.x, b ^= 1) {
-    const long long wn = w + gridDim.x;
-    if (wn < items)
-      estage_load(stage[b ^ 1], wn, nblk, Wbase, wstride, trip3, t1, Ioovv, ev, o, v);
-    cp_async_commit();
-    cp_async_wait1();  // the copies of item w have landed
-    __syncthreads();
-    const EStage<TW> &S = stage[b];
-    const int e = (int)(w / nblk), tb = (int)(w - (long long)e * nblk);
-    const int i = __ldg(trip3 + 3 * e), j = __ldg(trip3 + 3 * e + 1),
-              k = __ldg(trip3 + 3 * e + 2);
-    const int mult = (i == j && j == k) ? 6 : ((i == j || j == k) ? 2 : 1);
-    const double scale = 1.0 / (3.0 * mult);
-    int T[3];
-    decode_set(tb, T[0], T[1], T[2]);
-    const int b0[3] = {T[0] * kTile, T[1] * kTile, T[2] * kTile};
-    const double eijk = eo[i] + eo[j] + eo[k];
-    double s4 = 0.0, s5 = 0.0;
+  __syncthreads();
+  const double eijk = eo[i] + eo[j] + eo[k];
+  double s4 = 0.0, s5 = 0.0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int n = tid + 128 * q;
-      const int l[3] = {n >> 6, (n >> 3) & 7, n & 7};
-      const int a = b0[0] + l[0], bb = b0[1] + l[1], c = b0[2] + l[2];
-      if (a >= v || bb >= v || c >= v || a < bb || bb < c) continue;
-      double u[6], vd[6];
+  for (int q = 0; q < 4; ++q) {
+    const int n = tid + 128 * q;
+    const int l[3] = {n >> 6, (n >> 3) & 7, n & 7};
+    const int a = b0[0] + l[0], b = b0[1] + l[1], c = b0[2] + l[2];
+    if (a >= v || b >= v || c >= v || a < b || b < c) continue;
+    double u[6], vd[6];
 #pragma unroll
-      for (int s = 0; s < 6; ++s) {
-        const int P0 = ordpos(s, 0), P1 = ordpos(s, 1), P2 = ordpos(s, 2);
-        u[s] = (double)S.cube[s][l[P0]][l[P1]][l[P2]];
-        const int p12 = P1 * 2 + (P2 > P1 ? P2 - 1 : P2), p02 = P0 * 2 + (P2 > P0 ? P2 - 1 : P2),
-                  p01 = P0 * 2 + (P1 > P0 ? P1 - 1 : P1);
-        // V - W at (p0,p1,p2): t_i^p0 <jk|p1p2> + t_j^p1 <ik|p0p2> + t_k^p2 <ij|p0p1>
-        vd[s] = S.ts[0][P0][l[P0]] * S.It[0][p12][l[P1]][l[P2]] +
-                S.ts[1][P1][l[P1]] * S.It[1][p02][l[P0]][l[P2]] +
-                S.ts[2][P2][l[P2]] * S.It[2][p01][l[P0]][l[P1]];
-      }
-      const double D = eijk - S.es[0][l[0]] - S.es[1][l[1]] - S.es[2][l[2]];
-      double g4 = 0.0, g5 = 0.0;
-      if (a > bb && bb > c) {
-        form_apply(u, vd, g4, g5);
-      } else {
-        const bool ab = a == bb, bc = bb == c;
-        const bool use[6] = {true, !bc, !ab, !ab, !bc, !(ab || bc)};
-        accum_sets<0>(use, u, vd, g4, g5);
-      }
-      const double inv = 1.0 / D;
-      s4 += g4 * inv;
-      s5 += g5 * inv;
+    for (int s = 0; s < 6; ++s) {
+      const int P0 = ordpos(s, 0), P1 = ordpos(s, 1), P2 = ordpos(s, 2);
+      u[s] = (double)cube[s][l[P0]][l[P1]][l[P2]];
+      const int p12 = P1 * 2 + (P2 > P1 ? P2 - 1 : P2), p02 = P0 * 2 + (P2 > P0 ? P2 - 1 : P2),
+                p01 = P0 * 2 + (P1 > P0 ? P1 - 1 : P1);
+      // V - W at (p0,p1,p2): t_i^p0 <jk|p1p2> + t_j^p1 <ik|p0p2> + t_k^p2 <ij|p0p1>
+      vd[s] = ts[0][P0][l[P0]] * It[0][p12][l[P1]][l[P2]] +
+              ts[1][P1][l[P1]] * It[1][p02][l[P0]][l[P2]] +
+              ts[2][P2][l[P2]] * It[2][p01][l[P0]][l[P1]];
     }
-    for (int off = 16; off; off >>= 1) {
-      s4 += __shfl_down_sync(0xffffffffu, s4, off);
-      s5 += __shfl_down_sync(0xffffffffu, s5, off);
+    const double D = eijk - es[0][l[0]] - es[1][l[1]] - es[2][l[2]];
+    double g4 = 0.0, g5 = 0.0;
+    if (a > b && b > c) {
+      form_apply(u, vd, g4, g5);
+    } else {
+      const bool ab = a == b, bc = b == c;
+      const bool use[6] = {true, !bc, !ab, !ab, !bc, !(ab || bc)};
+      accum_sets<0>(use, u, vd, g4, g5);
     }
-    const int lane = tid & 31, wid = tid >> 5;
-    if (lane == 0) {
-      sh[0][wid] = s4;
-      sh[1][wid] = s5;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double a4 = 0.0, a5 = 0.0;
-      for (int q = 0; q < 4; ++q) {
-        a4 += sh[0][q];
-        a5 += sh[1][q];
-      }
-      const long long slot = (long long)e * nblk + tb;
-      part[2 * slot] = scale * a4;
-      part[2 * slot + 1] = scale * a5;
-    }
-    __syncthreads();  // stage b and sh are reused by the item after next
+    const double inv = 1.0 / D;
+    s4 += g4 * inv;
+    s5 += g5 * inv;
   }
-}
-
-// launch of the energy kernel over n triplets of W slots wstride apart
-template <typename TW>
-int launch_triples_energy(const TW *W, long long wstride, const int *trip3, int n,
-                          const double *t1, const double *Ioovv, const double *eo,
-                          const double *ev, int o, int v, int nblk, double *part,
-                          cudaStream_t st) {
-  const size_t smem = 2 * sizeof(EStage<TW>);
-  // shared-memory opt-in, resident blocks per SM and SM count, per device
-  static int per_sm[64] = {0}, nsm[64] = {0};
-  int dev = 0;
-  ACES_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) {
-    set_error("(T): device %d outside 0..63", dev);
-    return ACES_ERR_ARG;
+  for (int off = 16; off; off >>= 1) {
+    s4 += __shfl_down_sync(0xffffffffu, s4, off);
+    s5 += __shfl_down_sync(0xffffffffu, s5, off);
   }
-  if (!per_sm[dev]) {
-    ACES_CUDA(cudaFuncSetAttribute(k_triples_energy_tiled<TW>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int b = 0, m = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_triples_energy_tiled<TW>, 128,
-                                                      smem) != cudaSuccess ||
-        b <= 0) {
-      cudaGetLastError();
-      b = 2;
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) {
+    sh[0][wid] = s4;
+    sh[1][wid] = s5;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double a4 = 0.0, a5 = 0.0;
+    for (int w = 0; w < 4; ++w) {
+      a4 += sh[0][w];
+      a5 += sh[1][w];
     }
-    ACES_CUDA(cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev));
-    nsm[dev] = m > 0 ? m : 148;
-    per_sm[dev] = b;
+    const long long slot = (long long)e * gridDim.x + blockIdx.x;
+    part[2 * slot] = scale * a4;
+    part[2 * slot + 1] = scale * a5;
   }
-  const long long items = (long long)nblk * n;
-  if (items == 0) return ACES_OK;
-  const long long grid = std::min(items, (long long)nsm[dev] * per_sm[dev]);
-  k_triples_energy_tiled<TW><<<(unsigned)grid, 128, smem, st>>>(W, wstride, trip3, t1, Ioovv, eo,
-                                                                ev, o, v, nblk, items, part);
-  count_launch();
-  ACES_CUDA(cudaGetLastError());
-  return ACES_OK;
 }
 
 // sum of n (E4, E5) partial pairs: 1024 threads stride the list, then a
@@ -572,9 +472,11 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
       cv.p = Wb.p;
       ACES_TRY(gemm_nt_bf16x3_batched(Aa, Ba, 4, v * v, v, &byclass[(size_t)2 * ntrip + t0b],
                                       d_ent + 2 * ntrip + t0b, n, 1.0, 1.0, cv, true, st));
-      ACES_TRY(launch_triples_energy<float>(reinterpret_cast<const float *>(Wb.p), V3,
-                                            d_trip + 3 * t0b, n, t1(), I_oovv.p, eo.p, ev.p, o,
-                                            v, nblk, part.p + (size_t)t0b * nblk * 2, st));
+      k_triples_energy_tiled<float><<<dim3(nblk, n), 128, 0, st>>>(
+          reinterpret_cast<const float *>(Wb.p), V3, d_trip + 3 * t0b, t1(), I_oovv.p, eo.p,
+          ev.p, o, v, part.p + (size_t)t0b * nblk * 2);
+      count_launch();
+      ACES_CUDA(cudaGetLastError());
     }
     nparts = (long long)ntrip * nblk;
   } else {
@@ -622,9 +524,10 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
         const double *const B[4] = {T2p(j, i), T2p(j, k), Hp(k, j), Hp(i, j)};
         ACES_TRY(run_class(A, B, v * v, v, cv, 1.0));
       }
-      ACES_TRY(launch_triples_energy<double>(Wb.p, 0, d_trip + 3 * t, 1, t1(), I_oovv.p, eo.p,
-                                             ev.p, o, v, nblk, part.p + (size_t)t * nblk * 2,
-                                             st));
+      k_triples_energy_tiled<double><<<dim3(nblk, 1), 128, 0, st>>>(
+          Wb.p, 0, d_trip + 3 * t, t1(), I_oovv.p, eo.p, ev.p, o, v,
+          part.p + (size_t)t * nblk * 2);
+      count_launch();
     }
     nparts = (long long)ntrip * nblk;
   }
