@@ -569,7 +569,7 @@ int gemv_f64(int M, int K, double alpha, const double *A, long long lda, const d
   // few rows: each row split over W warps (about 4736 warps in all, K chunks
   // of at least 128), so the matrix streams with enough loads in flight
   const long long kTargetWarps = 148 * 32;
-  if ((long long)M * 2 <= kTargetWarps && K >= 256) {
+  if (M <= kTargetWarps && K >= 256) {
     int W = (int)std::min<long long>(32, (kTargetWarps + M - 1) / M);
     int kc = ((K + W - 1) / W + 127) / 128 * 128;
     W = (K + kc - 1) / kc;
