@@ -284,6 +284,32 @@ __global__ void k_gemv_final(int M, int W, double alpha, const double *__restric
   *cp = r;
 }
 
+// Tiny products (at most kTinyOut outputs): one thread per output, its K
+// sum in four independent FMA chains over L1-resident rows; threads run
+// along the output's unit-stride index.
+constexpr long long kTinyOut = 8192;
+__global__ void k_gemm_tiny_f64(int M, int N, int K, double alpha, const double *__restrict__ A,
+                                long long lda, const double *__restrict__ B, long long ldb,
+                                double beta, CView C, bool mfast) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= M * N) return;
+  const int m = mfast ? idx % M : idx / N, n = mfast ? idx / M : idx % N;
+  const double *a = A + (long long)m * lda, *b = B + (long long)n * ldb;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int k = 0;
+  for (; k + 3 < K; k += 4) {
+    s0 += __ldg(a + k) * __ldg(b + k);
+    s1 += __ldg(a + k + 1) * __ldg(b + k + 1);
+    s2 += __ldg(a + k + 2) * __ldg(b + k + 2);
+    s3 += __ldg(a + k + 3) * __ldg(b + k + 3);
+  }
+  for (; k < K; ++k) s0 += __ldg(a + k) * __ldg(b + k);
+  double *cp = C.p + cview_off(C, m, n);
+  double r = alpha * ((s0 + s1) + (s2 + s3));
+  if (beta != 0.0) r += beta * *cp;
+  *cp = r;
+}
+
 // ---------------------------------------------------------------------------
 // Thin contractions (one output dimension S <= 32): out(l, s) = sum_k X[l,k] Y[s,k]
 // with X the long operand (L rows) and Y the short one.  64 x 32 output tile
@@ -604,6 +630,15 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
   if (M <= 0 || N <= 0) return ACES_OK;
   if (K <= 0) {
     // C = beta*C: run with K = 0 is a scale; issue through the kernel with no k tiles
+  }
+  // a few thousand outputs: one thread each (no tiles, no split K)
+  if ((long long)M * N <= kTinyOut && K > 0 && K <= 8192) {
+    const bool mfast = C.sm0 == 1 || C.sn0 != 1;
+    k_gemm_tiny_f64<<<(unsigned)((M * N + 127) / 128), 128, 0, st>>>(M, N, K, alpha, A, lda, B,
+                                                                      ldb, beta, C, mfast);
+    count_launch();
+    ACES_CUDA(cudaGetLastError());
+    return ACES_OK;
   }
   // K <= 32: output-bound low-rank update
   if (K <= LR_K) return launch_lowrank(M, N, K, alpha, A, lda, B, ldb, beta, C, st);
