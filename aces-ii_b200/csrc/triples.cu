@@ -424,13 +424,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
       fr = 0;
     }
     const double slot = (double)V3 * sizeof(float);
-#ifndef ACES_T_L2MB
-#define ACES_T_L2MB 0
-#endif
-    // ACES_T_L2MB > 0: batches whose W slots fit that many MB (of the 126 MB
-    // L2), so the classes' accumulations and the energy pass hit L2
-    const double budget = ACES_T_L2MB > 0 ? ACES_T_L2MB * 1.0e6
-                                          : std::min(0.25 * (double)fr, 4.0e9);
+    const double budget = std::min(0.25 * (double)fr, 4.0e9);
     const int nb = (int)std::max(1.0, std::min((double)std::max(ntrip, 1), budget / slot));
     ACES_TRY(alloc(Wb, (size_t)((V3 * nb + 1) / 2)));  // FP32 slots in a double buffer
     // one entry per triplet and class: the windows of the four segments
