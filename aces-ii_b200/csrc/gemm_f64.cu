@@ -284,30 +284,35 @@ __global__ void k_gemv_final(int M, int W, double alpha, const double *__restric
   *cp = r;
 }
 
-// Tiny products (at most kTinyOut outputs): one thread per output, its K
-// sum in four independent FMA chains over L1-resident rows; threads run
-// along the output's unit-stride index.
+// Tiny products (at most kTinyOut outputs): one warp per output, its lanes
+// striding K (coalesced row reads, four independent partial sums per lane),
+// reduced by shuffles in a fixed order.
 constexpr long long kTinyOut = 8192;
 __global__ void k_gemm_tiny_f64(int M, int N, int K, double alpha, const double *__restrict__ A,
                                 long long lda, const double *__restrict__ B, long long ldb,
-                                double beta, CView C, bool mfast) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= M * N) return;
-  const int m = mfast ? idx % M : idx / N, n = mfast ? idx / M : idx % N;
+                                double beta, CView C) {
+  const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= M * N) return;  // warp-uniform
+  const int m = w % M, n = w / M;
   const double *a = A + (long long)m * lda, *b = B + (long long)n * ldb;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-  int k = 0;
-  for (; k + 3 < K; k += 4) {
+  int k = lane;
+  for (; k + 96 < K; k += 128) {
     s0 += __ldg(a + k) * __ldg(b + k);
-    s1 += __ldg(a + k + 1) * __ldg(b + k + 1);
-    s2 += __ldg(a + k + 2) * __ldg(b + k + 2);
-    s3 += __ldg(a + k + 3) * __ldg(b + k + 3);
+    s1 += __ldg(a + k + 32) * __ldg(b + k + 32);
+    s2 += __ldg(a + k + 64) * __ldg(b + k + 64);
+    s3 += __ldg(a + k + 96) * __ldg(b + k + 96);
   }
-  for (; k < K; ++k) s0 += __ldg(a + k) * __ldg(b + k);
-  double *cp = C.p + cview_off(C, m, n);
-  double r = alpha * ((s0 + s1) + (s2 + s3));
-  if (beta != 0.0) r += beta * *cp;
-  *cp = r;
+  for (; k < K; k += 32) s0 += __ldg(a + k) * __ldg(b + k);
+  double t = (s0 + s1) + (s2 + s3);
+  for (int off = 16; off; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  if (lane == 0) {
+    double *cp = C.p + cview_off(C, m, n);
+    double r = alpha * t;
+    if (beta != 0.0) r += beta * *cp;
+    *cp = r;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -631,11 +636,10 @@ int gemm_nt_f64(int M, int N, int K, double alpha, const double *A, long long ld
   if (K <= 0) {
     // C = beta*C: run with K = 0 is a scale; issue through the kernel with no k tiles
   }
-  // a few thousand outputs: one thread each (no tiles, no split K)
+  // a few thousand outputs: one warp each (no tiles, no split K)
   if ((long long)M * N <= kTinyOut && K > 0 && K <= 8192) {
-    const bool mfast = C.sm0 == 1 || C.sn0 != 1;
-    k_gemm_tiny_f64<<<(unsigned)((M * N + 127) / 128), 128, 0, st>>>(M, N, K, alpha, A, lda, B,
-                                                                      ldb, beta, C, mfast);
+    k_gemm_tiny_f64<<<(unsigned)(((long long)M * N * 32 + 255) / 256), 256, 0, st>>>(
+        M, N, K, alpha, A, lda, B, ldb, beta, C);
     count_launch();
     ACES_CUDA(cudaGetLastError());
     return ACES_OK;
