@@ -243,26 +243,54 @@ int CCEngine::backward() {
       CView cb = op.C;
       cb.p = cbar_base;
       if (op.a_act || op.b_act) {
-        ACES_TRY(tmp(bwdC, (size_t)op.M * op.N));
-        launch_view_gather(bwdC.p, cb, op.M, op.N, op.alpha, st);
+        // C_bar as an M x N row-major matrix (Cm, ldcm) and/or its transpose
+        // (Ct, ldct): a plain row- or column-major output view is read in
+        // place, any other view is gathered first; alpha goes to the products
+        const bool plain = cb.mdiv > 0x7fffffff && cb.ndiv > 0x7fffffff;
+        const double *Cm = nullptr, *Ct = nullptr;
+        long long ldcm = 0, ldct = 0;
+        if (plain && cb.sn0 == 1 && cb.sm0 >= op.N) {
+          Cm = cbar_base;
+          ldcm = cb.sm0;
+        } else if (plain && cb.sm0 == 1 && cb.sn0 >= op.M) {
+          Ct = cbar_base;
+          ldct = cb.sn0;
+        } else {
+          ACES_TRY(tmp(bwdC, (size_t)op.M * op.N));
+          launch_view_gather(bwdC.p, cb, op.M, op.N, 1.0, st);
+          Cm = bwdC.p;
+          ldcm = op.N;
+        }
         // the forward operands are fixed for the tape's life (constants, or
         // values recorded at the converged amplitudes): their transposes are
         // cached, so are their splits
         if (op.a_act) {
-          // A_bar[m,k] += sum_n Cd[m,n] B[n,k]
+          // A_bar[m,k] += alpha sum_n C_bar[m,n] B[n,k]
           const double *Bt = op.b_act ? tape_transposed(op.B, op.N, op.K, op.ldb)
                                       : transposed(op.B, op.N, op.K, op.ldb, true, bwdB);
           if (!Bt) return ACES_ERR_NOMEM;
-          ACES_TRY(G(op.M, op.K, op.N, 1.0, bwdC.p, op.N, Bt, op.N, 1.0,
+          const double *A_ = Cm;
+          long long lda_ = ldcm;
+          if (!A_) {
+            A_ = transposed(Ct, op.N, op.M, ldct, false, bwdC);
+            lda_ = op.N;
+          }
+          if (!A_) return ACES_ERR_NOMEM;
+          ACES_TRY(G(op.M, op.K, op.N, op.alpha, A_, lda_, Bt, op.N, 1.0,
                      cview_rowmajor(adj(op.A), op.lda), false, true));
         }
         if (op.b_act) {
-          // B_bar[n,k] += sum_m Cd[m,n] A[m,k]
-          const double *Cdt = transposed(bwdC.p, op.M, op.N, op.N, false, bwdD);
+          // B_bar[n,k] += alpha sum_m C_bar[m,n] A[m,k]
+          const double *T_ = Ct;
+          long long ldt_ = ldct;
+          if (!T_) {
+            T_ = transposed(Cm, op.M, op.N, ldcm, false, bwdD);
+            ldt_ = op.M;
+          }
           const double *At = op.a_act ? tape_transposed(op.A, op.M, op.K, op.lda)
                                       : transposed(op.A, op.M, op.K, op.lda, true, bwdA);
-          if (!Cdt || !At) return ACES_ERR_NOMEM;
-          ACES_TRY(G(op.N, op.K, op.M, 1.0, Cdt, op.M, At, op.M, 1.0,
+          if (!T_ || !At) return ACES_ERR_NOMEM;
+          ACES_TRY(G(op.N, op.K, op.M, op.alpha, T_, ldt_, At, op.M, 1.0,
                      cview_rowmajor(adj(op.B), op.ldb), false, true));
         }
       }
