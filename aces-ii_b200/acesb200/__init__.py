@@ -38,7 +38,7 @@ SYMBOLS = [
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
     "aces_intprc_df",
     "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
-    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "xvcc_run", "xlambda_run", "xdens_1pdm",
+    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "aces_set_tc_wide", "xvcc_run", "xlambda_run", "xdens_1pdm",
     "xvee_run",
 ]
 
@@ -245,6 +245,11 @@ class Lib:
         """Tensor-core tile variant: 1 = CTA pairs for products of >= 256 rows
         (aces_set_tc_pairs), 0 = one CTA per tile (default)."""
         self._chk("aces_set_tc_pairs", self.h.aces_set_tc_pairs(int(on)))
+
+    def set_tc_wide(self, on):
+        """Tile width of the single-chunk FP32-output launches: 1 = 128 x 256
+        (aces_set_tc_wide, default), 0 = 128 x 128."""
+        self._chk("aces_set_tc_wide", self.h.aces_set_tc_wide(int(on)))
 
     def debug_inject(self, mode):
         """Test hook: 1 = the tensor-core producer issues no copies (aces_debug_inject)."""

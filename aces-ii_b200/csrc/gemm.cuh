@@ -179,5 +179,10 @@ int tc_set_wait_limit(unsigned long long ns);
 int tc_set_inject(int on);
 // launches of products with >= 256 rows on CTA pairs (process-wide)
 void tc_set_pairs(int on);
+// 128 x 256 tiles for the single-chunk FP32-output launches (process-wide)
+void tc_set_wide(int on);
+// whether a batched FP32-output launch over these K segments runs on the
+// 128 x 256 tiles (the knob is on and the segments' k tiles form one chunk)
+bool bf16x3_wide_applies(const SplitOperand *A, int nseg);
 
 }  // namespace acesb200

@@ -123,18 +123,19 @@ constexpr int kSmemLimit = 227 * 1024;
 // tile (tcgen05 cta_group::2), each CTA holding its 128 rows of A and half of
 // the B rows, so a k tile brings 48 KB per CTA into shared memory instead of
 // 64 KB for the same products.
-template <int CG>
+template <int CG, int BN = TBN>
 struct Geom {
-  static constexpr int kBRows = TBN / CG;                   // B rows per CTA
+  static constexpr int kBRows = BN / CG;                    // B rows per CTA
   static constexpr int kTileB = kBRows * TBK * 2;
   static constexpr int kStage = 2 * TILE_A + 2 * kTileB;    // hi+lo of A and B
   static constexpr int kBarArea = 512;
   static constexpr int kStages = (kSmemLimit - 1024 - kBarArea) / kStage;
   static constexpr int kSmem = kStages * kStage + 1024 + kBarArea;  // + alignment + barriers
-  static_assert(kSmem <= kSmemLimit && kStages >= 3, "pipeline depth");
+  static_assert(kSmem <= kSmemLimit && kStages >= (BN > TBN ? 2 : 3), "pipeline depth");
   static_assert(3 * kStages * 8 + 64 + 8 <= kBarArea, "barrier area");
 };
-// (3 stages at TBK 64 or 6/7 at TBK 32 for one CTA per tile, 4 at TBK 64 for pairs)
+// (3 stages at TBK 64 or 6/7 at TBK 32 for one CTA per tile, 4 at TBK 64 for
+// pairs, 2 of 96 KB for the 128 x 256 tiles)
 // k tiles per FP32 accumulation chunk, by the contraction length K: 512 K
 // elements up to K = 36864, 256 up to 73728, 128 beyond
 inline int chunk_for(int kTilesTotal) {
@@ -145,12 +146,22 @@ inline int chunk_for(int kTilesTotal) {
 constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
 constexpr int kCols = 4 * TBN / kEpiWarps;            // accumulator columns per epilogue thread
 static_assert(kCols % 32 == 0 && kCols >= 32, "epilogue column span");
+// Wide tiles (128 x 256, one CTA): products whose every tile is a single
+// accumulation chunk with FP32 output (the batched (T) classes) -- no FP64
+// chunk sums to hold, so the epilogue streams the 256 TMEM columns straight
+// to the output, and each tcgen05.mma carries N = 256 (half the instructions
+// of the 128-wide tile for the same products).
+constexpr int TBN_WIDE = 256;
+#ifndef ACES_TC_WIDE
+#define ACES_TC_WIDE 1
+#endif
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 #ifndef ACES_TC_NACC
 #define ACES_TC_NACC 2
 #endif
 constexpr int kNAcc = ACES_TC_NACC;                   // TMEM accumulators in rotation
-constexpr int kTmemCols = kNAcc * TBN;
+template <int BN>
+constexpr int tmem_cols() { return kNAcc * BN; }
 // Bound on every mbarrier wait (ns), per device; aces_set_wait_limit changes it.
 __device__ unsigned long long g_tc_wait_ns = 4000000000ULL;
 // Fault injection for tests of the bounded waits (aces_debug_inject): when set,
@@ -309,11 +320,13 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
 // only its live columns rounded up to 16, the granularity of N at M = 128)
 // (M = 128 per CTA: 128 for one CTA, 256 for a CTA pair)
 constexpr uint32_t kIdescK = (1u << 4) | (1u << 7) | (1u << 10);
-// MMA N of a tile with n_live live columns (multiple of 16, at most TBN)
-__device__ __forceinline__ int mma_n(int n_live) { return min(TBN, (n_live + 15) & ~15); }
-template <int CG>
+// MMA N of a tile with n_live live columns (multiple of 16, at most BN)
+template <int BN = TBN>
+__device__ __forceinline__ int mma_n(int n_live) { return min(BN, (n_live + 15) & ~15); }
+template <int CG, int BN>
 __device__ __forceinline__ uint32_t idesc_for(int n_live) {
-  return kIdescK | ((uint32_t)((TBM * CG) >> 4) << 24) | ((uint32_t)(mma_n(n_live) >> 3) << 17);
+  return kIdescK | ((uint32_t)((TBM * CG) >> 4) << 24) |
+         ((uint32_t)(mma_n<BN>(n_live) >> 3) << 17);
 }
 
 template <int CG>
@@ -401,11 +414,12 @@ struct Launch {
   Problem prob[kMaxProb];
   int nprob, nTiles;
   int cg;  // CTAs per tile: 1, or 2 (a cluster pair on 256 x 128 tiles)
+  int bn;  // tile width: TBN, or TBN_WIDE (one CTA, single-chunk FP32 output)
 };
 struct TileRef {
   int g, m0, n0, z, ktb, kTiles, b;
 };
-template <int CG>
+template <int CG, int BN>
 __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
   TileRef r;
   r.g = 0;
@@ -440,10 +454,126 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
     r.z = q / P.tilesM;
   }
   r.m0 = tm * TBM * CG;
-  r.n0 = tn * TBN;
+  r.n0 = tn * BN;
   r.ktb = r.z * P.ktc;
   r.kTiles = max(0, min(P.ktc, P.kTilesTotal - r.ktb));
   return r;
+}
+
+// row windows of a batched entry (one read per tile, 8 ints)
+__device__ __forceinline__ void batch_rows(const Problem &P, int b, int (&rA)[kMaxSeg],
+                                           int (&rB)[kMaxSeg]) {
+  if (P.batch) {
+    const int4 *e = reinterpret_cast<const int4 *>(P.batch + b);
+    const int4 a = __ldg(e), c = __ldg(e + 1);
+    rA[0] = a.x; rA[1] = a.y; rA[2] = a.z; rA[3] = a.w;
+    rB[0] = c.x; rB[1] = c.y; rB[2] = c.z; rB[3] = c.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < kMaxSeg; ++q) rA[q] = rB[q] = 0;
+  }
+}
+// where k tile kt of tile T lies for this CTA: the K segment (tensor maps),
+// the K offset, and the A and B row coordinates (this CTA's rows: A from
+// m0 + 128 rank, B from n0 + rank * (MMA N) / 2)
+struct StageAt {
+  int sg, kx, ya, yb;
+};
+template <int CG, int BN>
+__device__ __forceinline__ StageAt stage_at(const Problem &P, const TileRef &T,
+                                            const int (&rA)[kMaxSeg], const int (&rB)[kMaxSeg],
+                                            int kt, uint32_t rank) {
+  const int gk = T.ktb + kt;
+  int sg = 0;
+  while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
+  StageAt s;
+  s.sg = sg;
+  s.kx = (gk - P.kt0[sg]) * TBK;
+  s.ya = T.m0 + (int)rank * TBM;
+  s.yb = T.n0 + (CG == 2 ? (int)rank * (mma_n<BN>(P.N - T.n0) >> 1) : 0);
+#pragma unroll
+  for (int q = 0; q < kMaxSeg; ++q)
+    if (q == sg) {
+      s.ya += rA[q];
+      s.yb += rB[q];
+    }
+  return s;
+}
+
+// Epilogue of the wide tiles (one accumulation chunk per tile, FP32 output):
+// each thread loads its row's 128 columns from TMEM (four 32-column loads),
+// hands the buffer back to the MMA thread, then writes them: plain stores for
+// beta = 0, one RED per element for beta = 1 (every element has one owner,
+// so the sum equals load + add + store).  Same arithmetic as the chunked
+// epilogue: (float)(alpha * (double)acc).
+template <int CG, int BN>
+__device__ __forceinline__ void epilogue_wide(const Launch &L, int t0, int tstep, uint32_t tmem,
+                                              uint64_t *acc_full, uint64_t *acc_empty,
+                                              int *abort_flag, double alpha, double beta,
+                                              int q, int half, int lane) {
+  constexpr int kC = 4 * BN / kEpiWarps;  // columns per thread
+  const int row = q * 32 + lane;
+  int gc = 0;
+  for (int t = t0; t < L.nTiles; t += tstep, ++gc) {
+    const TileRef T = decode_tile<CG, BN>(L, t);
+    const Problem &P = L.prob[T.g];
+    const int b = gc % kNAcc;
+    const bool w = mbar_wait_g<CG>(smem_u32(&acc_full[b]), (gc / kNAcc) & 1);
+    if (!w) atomicExch(&g_tc_status, 4);
+    if (!__all_sync(0xffffffffu, w && !*(volatile int *)abort_flag)) return;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int nb = T.n0 + half * kC;
+    const int ncol = min(kC, P.N - nb);  // live columns (may be <= 0)
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + half * kC);
+    uint32_t r[kC / 32][32];
+#pragma unroll
+    for (int h = 0; h < kC / 32; ++h)
+      if (ncol > h * 32) tmem_ld32(tbase + h * 32, r[h]);  // warp-uniform condition
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+    const int m = T.m0 + row;
+    if (m >= P.M || ncol <= 0) continue;
+    const CView &C = P.C;
+    float *const cm = reinterpret_cast<float *>(C.p) +
+                      (P.batch ? __ldg(&P.batch[T.b].coff) : 0LL) +
+                      cview_dim(C.mdiv, C.sm1, C.sm0, m);
+    CViewNWalk wk(C, nb);
+    float *const c0 = cm + wk.off;  // column nb
+    if (beta == 0.0 && C.ndiv > 0x7fffffff && C.sn0 == 1 && ((uintptr_t)c0 & 15) == 0) {
+      // unit n stride: the thread's columns are contiguous, 16-byte stores
+#pragma unroll
+      for (int h = 0; h < kC / 32; ++h)
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+          const int c = h * 32 + j;
+          float x[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) x[u] = (float)(alpha * (double)__uint_as_float(r[h][j + u]));
+          if (c + 3 < ncol) {
+            *reinterpret_cast<float4 *>(c0 + c) = make_float4(x[0], x[1], x[2], x[3]);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (c + u < ncol) c0[c + u] = x[u];
+          }
+        }
+    } else if (beta == 0.0) {
+#pragma unroll
+      for (int h = 0; h < kC / 32; ++h)
+#pragma unroll
+        for (int j = 0; j < 32; ++j, wk.next())
+          if (h * 32 + j < ncol) cm[wk.off] = (float)(alpha * (double)__uint_as_float(r[h][j]));
+    } else {
+#pragma unroll
+      for (int h = 0; h < kC / 32; ++h)
+#pragma unroll
+        for (int j = 0; j < 32; ++j, wk.next())
+          if (h * 32 + j < ncol)
+            atomicAdd(cm + wk.off, (float)(alpha * (double)__uint_as_float(r[h][j])));
+    }
+  }
 }
 
 // One CTA of 10 warps per SM: registers are allocated per SM sub-partition
@@ -462,11 +592,17 @@ __device__ __forceinline__ TileRef decode_tile(const Launch &L, int t) {
 // it issued; after a cluster barrier rank 0 arms and waits out (bounded)
 // any of them it did not arm itself (only after a wait gave up), so neither
 // CTA leaves while a copy of the pair is in flight.
-template <int CG>
+//
+// BN = 256 (one CTA, 128 x 256 tiles): the launch's every tile is a single
+// accumulation chunk with FP32 output; the epilogue streams each thread's 128
+// TMEM columns to the output (two stages of 96 KB in shared memory).
+template <int CG, int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
                   double *__restrict__ part) {
-  using Gm = Geom<CG>;
+  static_assert(BN == TBN || (BN == TBN_WIDE && CG == 1), "tile variants");
+  using Gm = Geom<CG, BN>;
+  constexpr int kTmemCols = tmem_cols<BN>();
   constexpr int kStages = Gm::kStages, kStage = Gm::kStage, kTileB = Gm::kTileB;
   const int nTiles = L.nTiles;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -525,20 +661,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     int it = 0;  // k tiles issued by this CTA
     bool stop = *(volatile int *)&g_tc_inject != 0;  // injected fault: issue nothing
     for (int t = t0; t < nTiles && !stop; t += tstep) {
-      const TileRef T = decode_tile<CG>(L, t);
+      const TileRef T = decode_tile<CG, BN>(L, t);
       const Problem &P = L.prob[T.g];
-      const int kTiles = T.kTiles, ktb = T.ktb;
-      // this CTA's rows: A from m0 + 128 rank, B from n0 + rank * (MMA N) / 2
-      const int m0 = T.m0 + (int)rank * TBM;
-      const int n0 = T.n0 + (CG == 2 ? (int)rank * (mma_n(P.N - T.n0) >> 1) : 0);
-      // row windows of a batched entry (one read per tile, 8 ints)
-      int rA[kMaxSeg] = {0, 0, 0, 0}, rB[kMaxSeg] = {0, 0, 0, 0};
-      if (P.batch) {
-        const int4 *e = reinterpret_cast<const int4 *>(P.batch + T.b);
-        const int4 a = __ldg(e), b = __ldg(e + 1);
-        rA[0] = a.x; rA[1] = a.y; rA[2] = a.z; rA[3] = a.w;
-        rB[0] = b.x; rB[1] = b.y; rB[2] = b.z; rB[3] = b.w;
-      }
+      const int kTiles = T.kTiles;
+      int rA[kMaxSeg], rB[kMaxSeg];
+      batch_rows(P, T.b, rA, rB);
       for (int kt = 0; kt < kTiles; ++kt) {
         const int s = it % kStages;
         if (it >= kStages && !mbar_wait_g<CG>(smem_u32(&empty[s]), ((it / kStages) - 1) & 1)) {
@@ -555,17 +682,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         unsigned char *st = smem + s * kStage;
         // a pair's stage completes on rank 0's barrier, armed with both halves
         if (rank == 0) mbar_expect_tx(fb, CG * kStage);
-        const int gk = ktb + kt;  // global k tile -> segment and its local k offset
-        int sg = 0;
-        while (sg + 1 < P.nseg && gk >= P.kt0[sg + 1]) ++sg;
-        const int kx = (gk - P.kt0[sg]) * TBK;
-        int ya = m0, yb = n0;
-#pragma unroll
-        for (int q = 0; q < kMaxSeg; ++q)
-          if (q == sg) {
-            ya += rA[q];
-            yb += rB[q];
-          }
+        const StageAt sa = stage_at<CG, BN>(P, T, rA, rB, kt, rank);
+        const int sg = sa.sg, kx = sa.kx, ya = sa.ya, yb = sa.yb;
         if (CG == 1) {
           tma_load_2d(smem_u32(st), &L.ah[T.g][sg], kx, ya, fb);
           tma_load_2d(smem_u32(st + TILE_A), &L.al[T.g][sg], kx, ya, fb);
@@ -600,9 +718,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     int it = 0, gc = 0;  // k tiles consumed, accumulation chunks started
     bool stop = false;
     for (int t = t0; t < nTiles && !stop; t += tstep) {
-      const TileRef T = decode_tile<CG>(L, t);
+      const TileRef T = decode_tile<CG, BN>(L, t);
       const int kTiles = T.kTiles, chunk = L.prob[T.g].chunk;
-      const uint32_t idesc = idesc_for<CG>(L.prob[T.g].N - T.n0);
+      const uint32_t idesc = idesc_for<CG, BN>(L.prob[T.g].N - T.n0);
       for (int kt = 0; kt < kTiles; ++kt) {
         const int kin = kt % chunk, b = gc % kNAcc;
         if (kin == 0 && gc >= kNAcc &&
@@ -622,7 +740,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t base = smem_u32(smem + s * kStage);
         const uint32_t ah = base, al = base + TILE_A, bh = base + 2 * TILE_A, bl = bh + kTileB;
-        const uint32_t acc_t = tmem + (uint32_t)(b * TBN);
+        const uint32_t acc_t = tmem + (uint32_t)(b * BN);
         // the start address is the descriptor's low field (address >> 4): the
         // 32-byte K step (16 BF16) inside a swizzled row adds 2 to it
         const uint64_t dah = umma_desc(ah), dal = umma_desc(al), dbh = umma_desc(bh),
@@ -653,8 +771,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int row = q * 32 + lane;
     int gc = 0;
     bool ok = true;
-    for (int t = t0; t < nTiles && ok; t += tstep) {
-      const TileRef T = decode_tile<CG>(L, t);
+    if constexpr (BN != TBN)
+      epilogue_wide<CG, BN>(L, t0, tstep, tmem, acc_full, acc_empty, abort_flag, alpha, beta, q,
+                            half, lane);
+    for (int t = t0; t < nTiles && ok && BN == TBN; t += tstep) {
+      const TileRef T = decode_tile<CG, BN>(L, t);
       const Problem &P = L.prob[T.g];
       const CView &C = P.C;
       const int M = P.M, N = P.N, m0 = T.m0 + (int)rank * TBM, n0 = T.n0, z = T.z;
@@ -890,6 +1011,7 @@ namespace {
 int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, int nseg, int M,
                 int N, const CView &C) {
   const int cg = L.cg == 2 ? 2 : 1;
+  const int bn = L.bn == TBN_WIDE ? TBN_WIDE : TBN;
   if (nseg < 1 || nseg > kMaxSeg) {
     set_error("gemm_nt_bf16x3: %d K segments (1..%d)", nseg, kMaxSeg);
     return ACES_ERR_ARG;
@@ -911,8 +1033,8 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
     const int kk = std::min(a.k, b.k) > 0 ? std::min(a.k, b.k) : a.k_pad;
     ACES_TRY(make_map(&L.ah[g][s], a.hi, a.rows_pad, a.k_pad, kk, TBM));
     ACES_TRY(make_map(&L.al[g][s], a.lo, a.rows_pad, a.k_pad, kk, TBM));
-    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, kk, TBN / cg));
-    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, kk, TBN / cg));
+    ACES_TRY(make_map(&L.bh[g][s], b.hi, b.rows_pad, b.k_pad, kk, bn / cg));
+    ACES_TRY(make_map(&L.bl[g][s], b.lo, b.rows_pad, b.k_pad, kk, bn / cg));
     P.kt0[s + 1] = P.kt0[s] + a.k_pad / TBK;
   }
   for (int s = nseg + 1; s <= kMaxSeg; ++s) P.kt0[s] = P.kt0[nseg];
@@ -920,7 +1042,7 @@ int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, 
   P.ktc = P.kTilesTotal;
   P.chunk = chunk_for(P.kTilesTotal);
   P.tilesM = (M + TBM * cg - 1) / (TBM * cg);
-  P.tilesN = (N + TBN - 1) / TBN;
+  P.tilesN = (N + bn - 1) / bn;
   // the side with fewer tiles runs fastest, so the CTAs working at the same
   // time share the row block of the larger operand (read from DRAM once,
   // then from L2): with a few m tiles and many n tiles, B is the large operand
@@ -947,7 +1069,8 @@ int max_pairs() {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_gemm_bf16x3<2>, &cfg) != cudaSuccess || n <= 0) {
+    if (cudaOccupancyMaxActiveClusters(&n, k_gemm_bf16x3<2, TBN>, &cfg) != cudaSuccess ||
+        n <= 0) {
       cudaGetLastError();
       n = num_sms() / 2;
     }
@@ -964,6 +1087,8 @@ int max_pairs() {
 // least 256 rows (the height of its tiles).
 std::atomic<int> g_tc_pairs{0};
 bool pairs_for(int min_rows) { return g_tc_pairs.load() != 0 && min_rows >= 2 * TBM; }
+// wide tiles for the single-chunk FP32-output launches (aces_set_tc_wide)
+std::atomic<int> g_tc_wide{ACES_TC_WIDE};
 
 int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStream_t st) {
   // the shared-memory opt-in and the status word are per device
@@ -975,10 +1100,13 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     return ACES_ERR_ARG;
   }
   if (!attr[dev]) {
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   Geom<1>::kSmem));
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   Geom<2>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, TBN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<1>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2, TBN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<2>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, TBN_WIDE>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<1, TBN_WIDE>::kSmem));
     int zero = 0;
     ACES_CUDA(cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int)));
     attr[dev] = true;
@@ -997,10 +1125,14 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2>, L, alpha, beta, part));
+    ACES_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16x3<2, TBN>, L, alpha, beta, part));
+  } else if (L.bn == TBN_WIDE) {
+    const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
+    k_gemm_bf16x3<1, TBN_WIDE>
+        <<<grid, kThreads, Geom<1, TBN_WIDE>::kSmem, st>>>(L, alpha, beta, part);
   } else {
     const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
-    k_gemm_bf16x3<1><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
+    k_gemm_bf16x3<1, TBN><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
   }
   count_launch();
   ACES_CUDA(cudaGetLastError());
@@ -1105,8 +1237,8 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
     set_error("gemm_nt_bf16x3_batched: FP32 output takes beta 0 or 1 (%g)", beta);
     return ACES_ERR_ARG;
   }
-  if (f32out && C.sm0 != 1) {
-    set_error("gemm_nt_bf16x3_batched: FP32 output needs unit m stride");
+  if (f32out && C.sm0 != 1 && !(beta == 0.0 && C.sn0 == 1)) {
+    set_error("gemm_nt_bf16x3_batched: FP32 output needs unit m stride (or n, for beta = 0)");
     return ACES_ERR_ARG;
   }
   // every live row of every window inside its parent: the TMA coordinates of
@@ -1125,7 +1257,13 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
   memset(&L, 0, sizeof(L));
   L.nprob = 1;
   L.cg = pairs_for(M) ? 2 : 1;
+  // FP32 output whose every tile is one accumulation chunk: wide tiles
+  L.bn = f32out && L.cg == 1 && g_tc_wide.load() ? TBN_WIDE : TBN;
   ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  if (L.bn == TBN_WIDE && L.prob[0].kTilesTotal > L.prob[0].chunk) {
+    L.bn = TBN;
+    ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  }
   Problem &P = L.prob[0];
   P.batch = d_entries;
   P.nbatch = nbatch;
@@ -1157,6 +1295,15 @@ int tc_set_wait_limit(unsigned long long ns) {
 }
 
 void tc_set_pairs(int on) { g_tc_pairs.store(on ? 1 : 0); }
+
+void tc_set_wide(int on) { g_tc_wide.store(on ? 1 : 0); }
+
+bool bf16x3_wide_applies(const SplitOperand *A, int nseg) {
+  if (!g_tc_wide.load() || pairs_for(1 << 30) || nseg < 1 || nseg > kMaxSeg) return false;
+  int kt = 0;
+  for (int s = 0; s < nseg; ++s) kt += A[s].k_pad / TBK;
+  return kt <= chunk_for(kt);
+}
 
 int tc_set_inject(int on) {
   ACES_CUDA(cudaMemcpyToSymbol(g_tc_inject, &on, sizeof(on)));

@@ -400,6 +400,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
   const int *d_trip = reinterpret_cast<const int *>(dtrip.p);
   const bool use_split = prec == ACES_PREC_BF16X3 && v >= 128;
   const CView vc{nullptr, kHugeView, 0, 1, V, V2, V};   // m = c, n = (a,b)
+  const CView vcT{nullptr, kHugeView, 0, V, kHugeView, 0, 1};  // m = (a,b), n = c
   const CView va{nullptr, V, V, 1, kHugeView, 0, V2};   // m = (b,c), n = a
   const CView vb{nullptr, V, V2, 1, kHugeView, 0, V};   // m = (a,c), n = b
   long long nparts = 0;
@@ -427,6 +428,12 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
     const double budget = std::min(0.25 * (double)fr, 4.0e9);
     const int nb = (int)std::max(1.0, std::min((double)std::max(ntrip, 1), budget / slot));
     ACES_TRY(alloc(Wb, (size_t)((V3 * nb + 1) / 2)));  // FP32 slots in a double buffer
+    // class c runs transposed on the 128 x 256 tiles (M = (a,b), N = c: the
+    // ragged side is the one whose MMA N is cut to the live columns, where on
+    // 128-row tiles M = c = v would leave 256 - v rows idle), and stores W
+    // rows of v contiguous floats
+    const SplitOperand Ac[4] = {sT2, sT2, sHn, sHn}, Bc[4] = {sGv, sGvT, sT2P, sT2Q};
+    const bool c_wide = bf16x3_wide_applies(Bc, 4);
     // one entry per triplet and class: the windows of the four segments
     auto T2r = [&](int x, int y) { return (x * o + y) * v; };   // rows of sT2 / sHn
     auto Pr = [&](int z) { return z * v * v; };                  // rows of sGv/sGvT/sT2P/sT2Q
@@ -436,8 +443,10 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
       const long long coff = (long long)(t % nb) * V3;
       BatchEntry &c = ent[(size_t)3 * t], &a = ent[(size_t)3 * t + 1],
                  &b = ent[(size_t)3 * t + 2];
-      c = BatchEntry{{T2r(k, i), T2r(k, j), T2r(j, k), T2r(i, k)},
-                     {Pr(j), Pr(i), Pr(i), Pr(j)}, coff};
+      c = c_wide ? BatchEntry{{Pr(j), Pr(i), Pr(i), Pr(j)},
+                              {T2r(k, i), T2r(k, j), T2r(j, k), T2r(i, k)}, coff}
+                 : BatchEntry{{T2r(k, i), T2r(k, j), T2r(j, k), T2r(i, k)},
+                              {Pr(j), Pr(i), Pr(i), Pr(j)}, coff};
       a = BatchEntry{{Pr(k), Pr(j), Pr(j), Pr(k)},
                      {T2r(i, j), T2r(i, k), T2r(k, i), T2r(j, i)}, coff};
       b = BatchEntry{{Pr(k), Pr(i), Pr(i), Pr(k)},
@@ -453,17 +462,20 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
       ACES_CUDA(cudaMemcpyAsync(dent.p, byclass.data(), byclass.size() * sizeof(BatchEntry),
                                 cudaMemcpyHostToDevice, st));
     const BatchEntry *d_ent = reinterpret_cast<const BatchEntry *>(dent.p);
-    const SplitOperand Ac[4] = {sT2, sT2, sHn, sHn}, Bc[4] = {sGv, sGvT, sT2P, sT2Q};
     const SplitOperand Aa[4] = {sGv, sGvT, sT2P, sT2Q}, Ba[4] = {sT2, sT2, sHn, sHn};
     const int nt = (v + kTile - 1) / kTile;
     const int nblk = nt * (nt + 1) * (nt + 2) / 6;   // tile triples A >= B >= C
     ACES_TRY(alloc(part, (size_t)std::max(ntrip, 1) * nblk * 2));
     for (int t0b = 0; t0b < ntrip; t0b += nb) {
       const int n = std::min(nb, ntrip - t0b);
-      CView cv = vc;
+      CView cv = c_wide ? vcT : vc;
       cv.p = Wb.p;
-      ACES_TRY(gemm_nt_bf16x3_batched(Ac, Bc, 4, v, v * v, &byclass[(size_t)t0b],
-                                      d_ent + t0b, n, 1.0, 0.0, cv, true, st));
+      if (c_wide)
+        ACES_TRY(gemm_nt_bf16x3_batched(Bc, Ac, 4, v * v, v, &byclass[(size_t)t0b], d_ent + t0b,
+                                        n, 1.0, 0.0, cv, true, st));
+      else
+        ACES_TRY(gemm_nt_bf16x3_batched(Ac, Bc, 4, v, v * v, &byclass[(size_t)t0b],
+                                        d_ent + t0b, n, 1.0, 0.0, cv, true, st));
       cv = va;
       cv.p = Wb.p;
       ACES_TRY(gemm_nt_bf16x3_batched(Aa, Ba, 4, v * v, v, &byclass[(size_t)ntrip + t0b],

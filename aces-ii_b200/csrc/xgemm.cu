@@ -106,6 +106,15 @@ extern "C" int aces_set_tc_pairs(int on) {
   return ACES_OK;
 }
 
+extern "C" int aces_set_tc_wide(int on) {
+  if (on != 0 && on != 1) {
+    set_error("aces_set_tc_wide: %d (0 or 1)", on);
+    return ACES_ERR_ARG;
+  }
+  tc_set_wide(on);
+  return ACES_OK;
+}
+
 extern "C" int aces_debug_inject(int mode) {
   if (mode != 0 && mode != 1) {
     set_error("aces_debug_inject: mode %d (0 or 1)", mode);

@@ -178,6 +178,11 @@ int aces_debug_inject(int mode);
  * default, faster on B200 for the CC contractions).  Both give the same
  * error bound; process-wide. */
 int aces_set_tc_pairs(int on);
+/* Tile width of the tensor-core launches whose every output tile is one
+ * accumulation chunk with FP32 output (the batched (T) classes; no
+ * counterpart in the reference): 1 = 128 x 256 tiles (the default),
+ * 0 = 128 x 128 tiles.  Same arithmetic either way; process-wide. */
+int aces_set_tc_wide(int on);
 
 /* ---- member programs ---------------------------------------------------- */
 

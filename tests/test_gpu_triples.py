@@ -54,6 +54,24 @@ def test_triples_split_matches_fp64(lib):
     assert abs(split.e_st5 - exact.e_st5) < 1e-9 + 1e-6 * abs(exact.e_st5)
 
 
+def test_triples_wide_tiles_match_narrow_tiles(lib):
+    """The (T) class launches on 128 x 256 tiles (aces_set_tc_wide(1), the
+    default for single-chunk FP32 output) against 128 x 128 tiles: v = 136
+    makes both sides ragged (class a/b N = 136 in one tile, class c N = v^2
+    ending in a partial tile); the W sums differ only in FP32 rounding order."""
+    ham = synthetic(4, 136, 60, seed=12, bscale=0.5)
+    setup_lists(lib, ham)
+    wide = lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=ab.PREC_BF16X3)
+    lib.set_tc_wide(0)
+    try:
+        narrow = lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=ab.PREC_BF16X3)
+    finally:
+        lib.set_tc_wide(1)
+    assert wide.e_ccsd == narrow.e_ccsd
+    assert abs(wide.e_t4 - narrow.e_t4) < 1e-14 + 1e-9 * abs(narrow.e_t4)
+    assert abs(wide.e_st5 - narrow.e_st5) < 1e-15 + 1e-9 * abs(narrow.e_st5)
+
+
 @pytest.mark.parametrize("prec", [ab.PREC_FP64, ab.PREC_BF16X3])
 def test_triplet_shards_add_up_to_the_full_triples(lib, prec):
     """The per-GPU (T) shards (triples_rank / triples_nranks), evaluated here one
