@@ -48,28 +48,43 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// The copies of one operand tile (BM rows x BK doubles) in VEC-double chunks:
+// thread t always takes the chunks of k offset kc = (t % CPR) * VEC in rows
+// t / CPR + i * RS, so the row pointers, their bounds and the shared-memory
+// offsets are computed once per block; a k tile then adds its k0 and tests
+// one K bound.
 template <int VEC>
-__device__ __forceinline__ void load_stage(double *sA, double *sB, const double *__restrict__ A,
-                                           long long lda, const double *__restrict__ B,
-                                           long long ldb, int M, int N, int K, int m0, int n0,
-                                           int k0) {
-  constexpr int CPR = BK / VEC;              // chunks per row
-  constexpr int CHUNKS = BM * CPR;           // per operand
-  for (int c = threadIdx.x; c < CHUNKS; c += kThreads) {
-    int r = c / CPR, kc = (c % CPR) * VEC;
-    int gm = m0 + r, gk = k0 + kc;
-    bool v = gm < M && gk < K;
-    const double *src = v ? A + (long long)gm * lda + gk : A;
-    cp_async<VEC>(sA + r * LDS + kc, src, v);
+struct CopyPlan {
+  static constexpr int CPR = BK / VEC;          // chunks per row
+  static constexpr int RS = kThreads / CPR;     // row step between a thread's chunks
+  static constexpr int kPer = BM / RS;          // chunks per thread and operand
+  const double *row[kPer];                      // &X[row][kc] (X itself for rows past the end)
+  unsigned live;                                // bit i: row i inside the operand
+  int kc, soff0;                                // k offset; shared offset of chunk 0
+  __device__ __forceinline__ CopyPlan(const double *X, long long ld, int rows, int r0base) {
+    const int t = threadIdx.x;
+    kc = (t % CPR) * VEC;
+    const int r0 = t / CPR;
+    soff0 = r0 * LDS + kc;
+    live = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int gr = r0base + r0 + i * RS;
+      const bool ok = gr < rows;
+      row[i] = ok ? X + (long long)gr * ld + kc : X;
+      live |= ok ? 1u << i : 0u;
+    }
   }
-  for (int c = threadIdx.x; c < CHUNKS; c += kThreads) {
-    int r = c / CPR, kc = (c % CPR) * VEC;
-    int gn = n0 + r, gk = k0 + kc;
-    bool v = gn < N && gk < K;
-    const double *src = v ? B + (long long)gn * ldb + gk : B;
-    cp_async<VEC>(sB + r * LDS + kc, src, v);
+  __device__ __forceinline__ void issue(double *stage, const double *X, int k0, int ke) const {
+    const bool kok = k0 + kc < ke;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const bool v = kok && ((live >> i) & 1u);
+      cp_async<VEC>(stage + soff0 + i * RS * LDS, v ? row[i] + k0 : X, v);
+    }
   }
-}
+};
+static_assert(BM == BN, "one copy plan shape for both operands");
 
 template <int VEC>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -93,11 +108,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
   auto stA = [&](int s) { return smem + s * kStageDoubles; };
   auto stB = [&](int s) { return smem + s * kStageDoubles + BM * LDS; };
+  const CopyPlan<VEC> pa(A, lda, M, m0), pb(B, ldb, N, n0);
   // prologue: k tiles 0 .. kStages-2 in flight (one commit group each, empty
   // groups past the end keep the count uniform)
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
-    if (s < nk) load_stage<VEC>(stA(s), stB(s), A, lda, B, ldb, M, N, ke, m0, n0, kb + s * BK);
+    if (s < nk) {
+      pa.issue(stA(s), A, kb + s * BK, ke);
+      pb.issue(stB(s), B, kb + s * BK, ke);
+    }
     cp_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
@@ -106,9 +125,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     // refill the slot computed in the previous iteration (every thread is past it)
     const int nxt = kt + kStages - 1;
-    if (nxt < nk)
-      load_stage<VEC>(stA(nxt % kStages), stB(nxt % kStages), A, lda, B, ldb, M, N, ke, m0, n0,
-                      kb + nxt * BK);
+    if (nxt < nk) {
+      pa.issue(stA(nxt % kStages), A, kb + nxt * BK, ke);
+      pb.issue(stB(nxt % kStages), B, kb + nxt * BK, ke);
+    }
     cp_commit();
     const double *a_s = stA(kt % kStages) + (wm * 64) * LDS;
     const double *b_s = stB(kt % kStages) + (wn * 32) * LDS;
