@@ -1257,8 +1257,12 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
   memset(&L, 0, sizeof(L));
   L.nprob = 1;
   L.cg = pairs_for(M) ? 2 : 1;
-  // FP32 output whose every tile is one accumulation chunk: wide tiles
-  L.bn = f32out && L.cg == 1 && g_tc_wide.load() ? TBN_WIDE : TBN;
+  // FP32 output whose every tile is one accumulation chunk, with 128 < N <=
+  // 256: one wide tile instead of a full and a ragged 128-wide one.  Where
+  // N is a multiple of 128 or much larger, the 3-stage 128-wide tiles win
+  // (o = 6, v = 128 class launches: 32 % slower with N = 128 on wide tiles,
+  // 3 % slower with N = 16384)
+  L.bn = f32out && L.cg == 1 && N > TBN && N <= TBN_WIDE && g_tc_wide.load() ? TBN_WIDE : TBN;
   ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
   if (L.bn == TBN_WIDE && L.prob[0].kTilesTotal > L.prob[0].chunk) {
     L.bn = TBN;
@@ -1298,8 +1302,10 @@ void tc_set_pairs(int on) { g_tc_pairs.store(on ? 1 : 0); }
 
 void tc_set_wide(int on) { g_tc_wide.store(on ? 1 : 0); }
 
-bool bf16x3_wide_applies(const SplitOperand *A, int nseg) {
-  if (!g_tc_wide.load() || pairs_for(1 << 30) || nseg < 1 || nseg > kMaxSeg) return false;
+bool bf16x3_wide_applies(const SplitOperand *A, int nseg, int N) {
+  if (!g_tc_wide.load() || pairs_for(1 << 30) || N <= TBN || N > TBN_WIDE || nseg < 1 ||
+      nseg > kMaxSeg)
+    return false;
   int kt = 0;
   for (int s = 0; s < nseg; ++s) kt += A[s].k_pad / TBK;
   return kt <= chunk_for(kt);

@@ -433,7 +433,7 @@ int CCEngine::triples(double *e4, double *e5, double *seconds, int rank, int nra
     // 128-row tiles M = c = v would leave 256 - v rows idle), and stores W
     // rows of v contiguous floats
     const SplitOperand Ac[4] = {sT2, sT2, sHn, sHn}, Bc[4] = {sGv, sGvT, sT2P, sT2Q};
-    const bool c_wide = bf16x3_wide_applies(Bc, 4);
+    const bool c_wide = bf16x3_wide_applies(Bc, 4, v);
     // one entry per triplet and class: the windows of the four segments
     auto T2r = [&](int x, int y) { return (x * o + y) * v; };   // rows of sT2 / sHn
     auto Pr = [&](int z) { return z * v * v; };                  // rows of sGv/sGvT/sT2P/sT2Q

@@ -70,8 +70,9 @@ def args():
                    help="run one small case for ncu captures and exit: a contraction "
                         "shape through aces_xgemm (ladder-small, ladder-packed, thin-t1, "
                         "lowrank-t1) or "
-                        "CCSD(T) on a small system (triples-o10-v180, triples-o6-v128) or "
-                        "split CCSD cycles (ccsd-o40-v100)")
+                        "CCSD(T) on a small system (triples-o10-v180, triples-o6-v128, "
+                        "triples-o4-v136), split CCSD cycles (ccsd-o40-v100) or Lambda + "
+                        "density (lambda-c4)")
     a = p.parse_args()
     if a.use_graph is None:
         a.use_graph = 0 if a.workload == "c5" else 1
@@ -889,6 +890,8 @@ PROGRAM_CASES = {
     "triples-o10-v180": dict(nocc=10, nvir=180, naux=540, seed=5, bscale=0.25),
     # the same kernels on a few GB of device memory (56 triplets, one batch)
     "triples-o6-v128": dict(nocc=6, nvir=128, naux=300, seed=5, bscale=0.25),
+    # v = 136 > 128: the (T) classes on 128 x 256 tiles, a few GB on the device
+    "triples-o4-v136": dict(nocc=4, nvir=136, naux=200, seed=5, bscale=0.25),
     # Lambda + density on the convergent C4 system (split precision)
     "lambda-c4": dict(nocc=20, nvir=180, naux=600, seed=3, bscale=0.25, lam=True),
     # split CCSD cycles of a system whose o^2 v^2 arrays (128 MB) exceed L2 while
