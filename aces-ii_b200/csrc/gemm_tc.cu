@@ -113,6 +113,14 @@ namespace {
 #define ACES_TC_TBK 64
 #endif
 constexpr int TBM = 128, TBN = 128, TBK = ACES_TC_TBK;
+// Tile width of the default one-CTA kernel: 144 columns (o^2 = 400 in three
+// tiles, 3600 and 32400 in whole tiles, where 128-wide tiles leave a 16-wide
+// remainder that costs nearly a full tile); TBN = 128 is the CTA-pair width.
+#ifndef ACES_TC_NARROW
+#define ACES_TC_NARROW 144
+#endif
+constexpr int TBN_1 = ACES_TC_NARROW;
+static_assert(TBN_1 == 128 || TBN_1 == 144, "one-CTA tile width");
 static_assert(TBK == 32 || TBK == 64, "k tile of 32 or 64 BF16");
 constexpr int kRowBytes = TBK * 2;                    // one swizzled smem row
 constexpr int kUnit = 64 / TBK;                       // k tiles per 64 K elements
@@ -131,7 +139,7 @@ struct Geom {
   static constexpr int kBarArea = 512;
   static constexpr int kStages = (kSmemLimit - 1024 - kBarArea) / kStage;
   static constexpr int kSmem = kStages * kStage + 1024 + kBarArea;  // + alignment + barriers
-  static_assert(kSmem <= kSmemLimit && kStages >= (BN > TBN ? 2 : 3), "pipeline depth");
+  static_assert(kSmem <= kSmemLimit && kStages >= (BN > 160 ? 2 : 3), "pipeline depth");
   static_assert(3 * kStages * 8 + 64 + 8 <= kBarArea, "barrier area");
 };
 // (3 stages at TBK 64 or 6/7 at TBK 32 for one CTA per tile, 4 at TBK 64 for
@@ -143,9 +151,17 @@ inline int chunk_for(int kTilesTotal) {
   if (kTilesTotal <= 1152 * kUnit) return 4 * kUnit;
   return 2 * kUnit;
 }
-constexpr int kEpiWarps = 8;                          // 2 per TMEM lane quadrant
-constexpr int kCols = 4 * TBN / kEpiWarps;            // accumulator columns per epilogue thread
-static_assert(kCols % 32 == 0 && kCols >= 32, "epilogue column span");
+// Epilogue warps of a tile width: 2 per TMEM lane quadrant (64 or 128 columns
+// each), or 3 per quadrant for the 144-wide tiles (48 columns each, whose
+// FP64 sums fit the registers of a 14-warp block)
+template <int BN>
+constexpr int epi_warps() { return BN % 64 == 0 ? 8 : 12; }
+template <int BN>
+constexpr int epi_cols() { return 4 * BN / epi_warps<BN>(); }  // columns per epilogue thread
+template <int BN>
+constexpr int block_threads() { return 32 * (2 + epi_warps<BN>()); }
+static_assert(epi_cols<128>() == 64 && epi_cols<144>() == 48 && epi_cols<256>() == 128,
+              "epilogue column spans");
 // Wide tiles (128 x 256, one CTA): products whose every tile is a single
 // accumulation chunk with FP32 output (the batched (T) classes) -- no FP64
 // chunk sums to hold, so the epilogue streams the 256 TMEM columns straight
@@ -155,13 +171,16 @@ constexpr int TBN_WIDE = 256;
 #ifndef ACES_TC_WIDE
 #define ACES_TC_WIDE 1
 #endif
-constexpr int kThreads = 32 * (2 + kEpiWarps);
 #ifndef ACES_TC_NACC
 #define ACES_TC_NACC 2
 #endif
 constexpr int kNAcc = ACES_TC_NACC;                   // TMEM accumulators in rotation
 template <int BN>
-constexpr int tmem_cols() { return kNAcc * BN; }
+constexpr int tmem_cols() {  // a power of two >= 32 (allocation unit)
+  int c = 32;
+  while (c < kNAcc * BN) c *= 2;
+  return c;
+}
 // Bound on every mbarrier wait (ns), per device; aces_set_wait_limit changes it.
 __device__ unsigned long long g_tc_wait_ns = 4000000000ULL;
 // Fault injection for tests of the bounded waits (aces_debug_inject): when set,
@@ -357,6 +376,15 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
         " [%0], %1;" ::"r"(bar), "h"((unsigned short)3)
         : "memory");
 }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
@@ -414,7 +442,8 @@ struct Launch {
   Problem prob[kMaxProb];
   int nprob, nTiles;
   int cg;  // CTAs per tile: 1, or 2 (a cluster pair on 256 x 128 tiles)
-  int bn;  // tile width: TBN, or TBN_WIDE (one CTA, single-chunk FP32 output)
+  int bn;  // tile width: TBN_1 (one CTA), TBN (CTA pair), TBN_WIDE (one CTA,
+           // single-chunk FP32 output)
 };
 struct TileRef {
   int g, m0, n0, z, ktb, kTiles, b;
@@ -511,7 +540,7 @@ __device__ __forceinline__ void epilogue_wide(const Launch &L, int t0, int tstep
                                               uint64_t *acc_full, uint64_t *acc_empty,
                                               int *abort_flag, double alpha, double beta,
                                               int q, int half, int lane) {
-  constexpr int kC = 4 * BN / kEpiWarps;  // columns per thread
+  constexpr int kC = epi_cols<BN>();  // columns per thread
   const int row = q * 32 + lane;
   int gc = 0;
   for (int t = t0; t < L.nTiles; t += tstep, ++gc) {
@@ -597,10 +626,13 @@ __device__ __forceinline__ void epilogue_wide(const Launch &L, int t0, int tstep
 // accumulation chunk with FP32 output; the epilogue streams each thread's 128
 // TMEM columns to the output (two stages of 96 KB in shared memory).
 template <int CG, int BN>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(block_threads<BN>(), 1)
     k_gemm_bf16x3(const __grid_constant__ Launch L, double alpha, double beta,
                   double *__restrict__ part) {
-  static_assert(BN == TBN || (BN == TBN_WIDE && CG == 1), "tile variants");
+  static_assert((CG == 2 && BN == TBN) || (CG == 1 && (BN == TBN_1 || BN == TBN_WIDE)),
+                "tile variants");
+  constexpr int kEpiWarps = epi_warps<BN>(), kCols = epi_cols<BN>();
+  constexpr int kPiece = kCols % 32 == 0 ? 32 : 16;  // columns per TMEM load
   using Gm = Geom<CG, BN>;
   constexpr int kTmemCols = tmem_cols<BN>();
   constexpr int kStages = Gm::kStages, kStage = Gm::kStage, kTileB = Gm::kTileB;
@@ -767,14 +799,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp >= 2) {
     // ---------------- epilogue: FP64 accumulation of the chunks ----------------
     const int q = warp & 3;                 // TMEM lane quadrant accessible to this warp
-    const int half = (warp - 2) >> 2;      // which kCols accumulator columns
+    const int half = (warp - 2) >> 2;      // which kCols accumulator columns (0 .. kEpiWarps/4-1)
     const int row = q * 32 + lane;
     int gc = 0;
     bool ok = true;
-    if constexpr (BN != TBN)
+    if constexpr (BN == TBN_WIDE)
       epilogue_wide<CG, BN>(L, t0, tstep, tmem, acc_full, acc_empty, abort_flag, alpha, beta, q,
                             half, lane);
-    for (int t = t0; t < nTiles && ok && BN == TBN; t += tstep) {
+    for (int t = t0; t < nTiles && ok && BN != TBN_WIDE; t += tstep) {
       const TileRef T = decode_tile<CG, BN>(L, t);
       const Problem &P = L.prob[T.g];
       const CView &C = P.C;
@@ -794,15 +826,19 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tbase =
-            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TBN + half * kCols);
+            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + half * kCols);
 #pragma unroll
-        for (int h = 0; h < kCols / 32; ++h) {
-          if (ncol > h * 32) {  // warp-uniform: skip column groups past N
+        for (int h = 0; h < kCols / kPiece; ++h) {
+          if (ncol > h * kPiece) {  // warp-uniform: skip column groups past N
             uint32_t r[32];
-            tmem_ld32(tbase + h * 32, r);
+            if constexpr (kPiece == 32)
+              tmem_ld32(tbase + h * 32, r);
+            else
+              tmem_ld16(tbase + h * kPiece, r);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < 32; ++j) acc[h * 32 + j] += (double)__uint_as_float(r[j]);
+            for (int j = 0; j < kPiece; ++j)
+              acc[h * kPiece + j] += (double)__uint_as_float(r[j]);
           }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1011,7 +1047,7 @@ namespace {
 int set_problem(Launch &L, int g, const SplitOperand *A, const SplitOperand *B, int nseg, int M,
                 int N, const CView &C) {
   const int cg = L.cg == 2 ? 2 : 1;
-  const int bn = L.bn == TBN_WIDE ? TBN_WIDE : TBN;
+  const int bn = cg == 2 ? TBN : (L.bn == TBN_WIDE ? TBN_WIDE : TBN_1);
   if (nseg < 1 || nseg > kMaxSeg) {
     set_error("gemm_nt_bf16x3: %d K segments (1..%d)", nseg, kMaxSeg);
     return ACES_ERR_ARG;
@@ -1064,7 +1100,7 @@ int max_pairs() {
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3((unsigned)(num_sms() & ~1));
-    cfg.blockDim = dim3(kThreads);
+    cfg.blockDim = dim3(block_threads<TBN>());
     cfg.dynamicSmemBytes = Geom<2>::kSmem;
     cfg.attrs = at;
     cfg.numAttrs = 1;
@@ -1100,8 +1136,9 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     return ACES_ERR_ARG;
   }
   if (!attr[dev]) {
-    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, TBN>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<1>::kSmem));
+    ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, TBN_1>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Geom<1, TBN_1>::kSmem));
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<2, TBN>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<2>::kSmem));
     ACES_CUDA(cudaFuncSetAttribute(k_gemm_bf16x3<1, TBN_WIDE>,
@@ -1120,7 +1157,7 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(2 * pairs);
-    cfg.blockDim = dim3(kThreads);
+    cfg.blockDim = dim3(block_threads<TBN>());
     cfg.dynamicSmemBytes = Geom<2>::kSmem;
     cfg.stream = st;
     cfg.attrs = at;
@@ -1129,10 +1166,12 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
   } else if (L.bn == TBN_WIDE) {
     const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
     k_gemm_bf16x3<1, TBN_WIDE>
-        <<<grid, kThreads, Geom<1, TBN_WIDE>::kSmem, st>>>(L, alpha, beta, part);
+        <<<grid, block_threads<TBN_WIDE>(), Geom<1, TBN_WIDE>::kSmem, st>>>(L, alpha, beta,
+                                                                             part);
   } else {
     const unsigned grid = (unsigned)std::min(L.nTiles, num_sms());
-    k_gemm_bf16x3<1, TBN><<<grid, kThreads, Geom<1>::kSmem, st>>>(L, alpha, beta, part);
+    k_gemm_bf16x3<1, TBN_1>
+        <<<grid, block_threads<TBN_1>(), Geom<1, TBN_1>::kSmem, st>>>(L, alpha, beta, part);
   }
   count_launch();
   ACES_CUDA(cudaGetLastError());
@@ -1262,10 +1301,12 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
   // N is a multiple of 128 or much larger, the 3-stage 128-wide tiles win
   // (o = 6, v = 128 class launches: 32 % slower with N = 128 on wide tiles,
   // 3 % slower with N = 16384)
-  L.bn = f32out && L.cg == 1 && N > TBN && N <= TBN_WIDE && g_tc_wide.load() ? TBN_WIDE : TBN;
+  L.bn = f32out && L.cg == 1 && N > TBN_1 && N <= TBN_WIDE && g_tc_wide.load()
+             ? TBN_WIDE
+             : (L.cg == 2 ? TBN : TBN_1);
   ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
   if (L.bn == TBN_WIDE && L.prob[0].kTilesTotal > L.prob[0].chunk) {
-    L.bn = TBN;
+    L.bn = TBN_1;
     ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
   }
   Problem &P = L.prob[0];
@@ -1303,7 +1344,7 @@ void tc_set_pairs(int on) { g_tc_pairs.store(on ? 1 : 0); }
 void tc_set_wide(int on) { g_tc_wide.store(on ? 1 : 0); }
 
 bool bf16x3_wide_applies(const SplitOperand *A, int nseg, int N) {
-  if (!g_tc_wide.load() || pairs_for(1 << 30) || N <= TBN || N > TBN_WIDE || nseg < 1 ||
+  if (!g_tc_wide.load() || pairs_for(1 << 30) || N <= TBN_1 || N > TBN_WIDE || nseg < 1 ||
       nseg > kMaxSeg)
     return false;
   int kt = 0;

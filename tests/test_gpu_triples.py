@@ -56,10 +56,11 @@ def test_triples_split_matches_fp64(lib):
 
 def test_triples_wide_tiles_match_narrow_tiles(lib):
     """The (T) class launches on 128 x 256 tiles (aces_set_tc_wide(1), the
-    default for single-chunk FP32 output) against 128 x 128 tiles: v = 136
-    makes both sides ragged (class a/b N = 136 in one tile, class c N = v^2
-    ending in a partial tile); the W sums differ only in FP32 rounding order."""
-    ham = synthetic(4, 136, 60, seed=12, bscale=0.5)
+    default for single-chunk FP32 output with 144 < N <= 256) against the
+    144-wide tiles: v = 160 puts classes a/b (N = 160) and the transposed
+    class c (N = c = 160) on one wide tile each, where the narrow tiles split
+    N into 144 + 16; the W sums differ only in FP32 rounding order."""
+    ham = synthetic(4, 160, 60, seed=12, bscale=0.5)
     setup_lists(lib, ham)
     wide = lib.xvcc(cc_conv=9, cc_maxcyc=60, triples=1, precision=ab.PREC_BF16X3)
     lib.set_tc_wide(0)
