@@ -8,16 +8,18 @@
 // dropped), which gives ~16 significant bits per product and FP32 sums that
 // are promoted to FP64 every CHUNK = 512 K elements (fewer for very long K).
 //
-// Persistent kernel, one CTA per SM, k tile 64 (128-byte swizzle), 10 warps:
+// Persistent kernel, one CTA per SM, k tile 64 (128-byte swizzle):
 //   warp 0  TMA producer (one elected lane)
 //   warp 1  TMEM allocator + MMA issuer (one elected lane)
-//   warps 2-9 epilogue: two warps per TMEM lane quadrant, each thread one
-//             output row x 64 columns, accumulated in FP64 across K chunks
-// Two variants: one CTA per 128 x 128 output tile (3-stage mbarrier
-// pipeline), and for products of at least 256 rows a cluster pair of CTAs
-// per 256 x 128 tile (tcgen05 cta_group::2, 4 stages), which halves each
-// CTA's share of the B tile: 48 KB instead of 64 KB of operands per k tile
-// and CTA for the same products.  No copy uses cluster multicast.
+//   warps 2.. epilogue: two or three warps per TMEM lane quadrant, each
+//             thread one output row x 48, 64 or 128 columns, accumulated in
+//             FP64 across K chunks
+// Three variants: one CTA per 128 x 144 output tile (14 warps, 3-stage
+// mbarrier pipeline; the default), one CTA per 128 x 256 tile for launches
+// whose tiles are single FP32-output chunks (10 warps, 2 stages), and for
+// products of at least 256 rows a cluster pair of CTAs per 256 x 128 tile
+// (tcgen05 cta_group::2, 10 warps, 4 stages), which halves each CTA's share
+// of the B tile.  No copy uses cluster multicast.
 // Every mbarrier wait is bounded by a %globaltimer limit; on expiry the
 // kernel records an error code in g_tc_status, drains its own TMA copies,
 // waits for its issued products, releases TMEM and returns.
@@ -605,9 +607,11 @@ __device__ __forceinline__ void epilogue_wide(const Launch &L, int t0, int tstep
   }
 }
 
-// One CTA of 10 warps per SM: registers are allocated per SM sub-partition
-// (16384 each) and three of the warps share one, so a thread gets at most
-// 168 (the epilogue spills a few of its 64 FP64 column sums, L1-resident).
+// One CTA per SM: registers are allocated per SM sub-partition (16384 each);
+// with 10 warps three share one, so a thread gets at most 168 (the 128-wide
+// epilogue spills a few of its 64 FP64 column sums, L1-resident), with 14
+// warps four share one: 128 (the 144-wide epilogue's 48 sums fit, with a few
+// spilled temporaries).
 //
 // CG = 2: clusters of two CTAs (ranks 0 and 1) share 256 x 128 tiles.  Each
 // CTA's producer loads its 128 A rows and its half of the B rows (as many as
