@@ -182,7 +182,7 @@ void tc_set_pairs(int on);
 // 128 x 256 tiles for the single-chunk FP32-output launches (process-wide)
 void tc_set_wide(int on);
 // whether a batched FP32-output launch over these K segments with N output
-// columns runs on the 128 x 256 tiles (the knob is on, 128 < N <= 256 and
+// columns runs on the 128 x 256 tiles (the knob is on, 144 < N <= 256 and
 // the segments' k tiles form one chunk)
 bool bf16x3_wide_applies(const SplitOperand *A, int nseg, int N);
 

@@ -1300,11 +1300,11 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
   memset(&L, 0, sizeof(L));
   L.nprob = 1;
   L.cg = pairs_for(M) ? 2 : 1;
-  // FP32 output whose every tile is one accumulation chunk, with 128 < N <=
-  // 256: one wide tile instead of a full and a ragged 128-wide one.  Where
-  // N is a multiple of 128 or much larger, the 3-stage 128-wide tiles win
-  // (o = 6, v = 128 class launches: 32 % slower with N = 128 on wide tiles,
-  // 3 % slower with N = 16384)
+  // FP32 output whose every tile is one accumulation chunk, with 144 < N <=
+  // 256: one wide tile instead of a full and a ragged narrow one.  Where N
+  // fits one narrow tile or is much larger, the 3-stage narrow tiles win
+  // (o = 6, v = 128 class launches against 128-wide tiles: 32 % slower with
+  // N = 128 on wide tiles, 3 % slower with N = 16384)
   L.bn = f32out && L.cg == 1 && N > TBN_1 && N <= TBN_WIDE && g_tc_wide.load()
              ? TBN_WIDE
              : (L.cg == 2 ? TBN : TBN_1);

@@ -179,9 +179,9 @@ int aces_debug_inject(int mode);
  * error bound; process-wide. */
 int aces_set_tc_pairs(int on);
 /* Tile width of the tensor-core launches whose every output tile is one
- * accumulation chunk with FP32 output and 128 < N <= 256 (the batched (T)
- * classes for 128 < v <= 192; no counterpart in the reference): 1 = one
- * 128 x 256 tile across N (the default), 0 = 128 x 128 tiles.  Same
+ * accumulation chunk with FP32 output and 144 < N <= 256 (the batched (T)
+ * classes for 144 < v <= 192; no counterpart in the reference): 1 = one
+ * 128 x 256 tile across N (the default), 0 = 128 x 144 tiles.  Same
  * arithmetic either way; process-wide. */
 int aces_set_tc_wide(int on);
 
