@@ -566,9 +566,14 @@ def run_ours(a, rank, world, local_rank):
 # DRAM bytes (read + write) of one packed ladder (its launches summed), from
 # an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the grouped
 # ladder launch at c2
-LADDER_TRAFFIC = {"c2": 2637.7e6 + 98.1e6}
-LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped ladder "
-                         "launch in the c2 cycle (one-pass launch list)")
+# DRAM bytes of the grouped packed-ladder launch of the c2 cycle: an ncu
+# capture of its symmetric product alone (--kernel-case ladder-packed, M = K =
+# 16290, N = 400: 1161.2 MB read + 45.4 MB written) scaled by the units the
+# grouped launch processes, (16290^2 + 16110^2) / 16290^2
+LADDER_TRAFFIC = {"c2": (1161.2e6 + 45.4e6) * (16290 ** 2 + 16110 ** 2) / 16290 ** 2}
+LADDER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the symmetric ladder "
+                         "product (--kernel-case ladder-packed) scaled to the grouped launch by "
+                         "(n+^2 + n-^2) / n+^2")
 
 
 def cublas_fp64_reference(o, v, dev, reps=5):
