@@ -151,11 +151,12 @@ int aces_xgemm(char transa, char transb, int m, int n, int k, double alpha, cons
  * allocating library routine: its scratch (m*k doubles when transa = 'N',
  * n*k when transb = 'T', plus optional split-K partials) comes from one
  * static device array of 2^20 doubles (8 MiB) that every GPU loading the
- * library holds until exit; larger requests return ACES_ERR_ARG.  The array's
- * device address is looked up on the first call on each device.  Every call
- * is synchronous on the legacy default stream of the current device, so it
- * must not be made while a stream is being captured into a CUDA graph.  Calls
- * share the array: calls that overlap on the GPU race.  FP64 only. */
+ * library holds until exit; larger requests return ACES_ERR_ARG.  The first
+ * call on each device looks up the array's device address (set-up); make
+ * that first call before any stream capture.  Every call runs on the legacy
+ * default stream of the current device and returns when the product is
+ * done.  Calls share the array: calls that overlap on the GPU race.  FP64
+ * only. */
 int aces_xgemm_static(char transa, char transb, int m, int n, int k, double alpha,
                       const double *A, int lda, const double *B, int ldb, double beta,
                       double *Cmat, int ldc);
