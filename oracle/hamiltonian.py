@@ -107,7 +107,84 @@ def from_fixture(path):
     ham.e_nuc = float(d["e_nuc"])
     ham.dipole = d["dipole"]
     ham.nucdip = d["nucdip"]
+    ham.hcore = d["hcore"]
     return ham
+
+
+def scf_in_field(ham, field, axis=2, tol=1e-12, maxit=200):
+    """RHF of a fixture molecule in a uniform electric field along ``axis``
+    (test infrastructure for finite-field dipoles).
+
+    The one-electron operator becomes h + field * r_axis (r the electronic
+    position; the field's interaction with the nuclei, -field * sum_A Z_A
+    R_A,axis, is a constant left out, so the dipole is nucdip - dE/dfield).
+    Works in the basis of the zero-field MOs, which is orthonormal and spans
+    the AO space, from the fixture's core Hamiltonian, MO integrals and MO
+    dipole integrals; Roothaan steps with DIIS (8 vectors), each irrep's
+    block diagonalised on its own so the orbitals keep their irreps (a field
+    along the C2 axis of a C2v molecule is totally symmetric), the lowest
+    pop[h] orbitals of irrep h occupied.  The reference's SCF program
+    (vscf/) is out of scope of the engine; this restates plain RHF only to
+    make the field-dependent orbitals of a finite-difference check.
+
+    Returns (E_SCF electronic + nuclear repulsion, MOHamiltonian in the
+    field's canonical orbitals, DPD order: occupied by irrep, then virtual by
+    irrep, energy order within)."""
+    n, o = ham.nmo, ham.nocc
+    g = ham._eri
+    hF = ham.hcore + field * ham.dipole[axis]
+    irr = np.asarray(ham.irrep)
+    pop, _ = ham.pop_vrt()
+    blocks = [np.where(irr == h)[0] for h in range(ham.nirrep)]
+
+    def canonical(F):
+        eps = np.zeros(n)
+        C = np.zeros((n, n))
+        for idx in blocks:
+            w, v = np.linalg.eigh(F[np.ix_(idx, idx)])
+            C[np.ix_(idx, idx)] = v
+            eps[idx] = w
+        occ = [i for h, idx in enumerate(blocks) for i in idx[:pop[h]]]
+        vir = [i for h, idx in enumerate(blocks) for i in idx[pop[h]:]]
+        order = occ + vir
+        return eps[order], C[:, order]
+
+    Cocc = np.eye(n)[:, :o]
+    focks, errs = [], []
+    for _ in range(maxit):
+        D = 2.0 * Cocc @ Cocc.T
+        F = hF + np.einsum("pqrs,rs->pq", g, D) - 0.5 * np.einsum("prqs,rs->pq", g, D)
+        err = F @ D - D @ F
+        if np.abs(err).max() < tol:
+            break
+        focks.append(F)
+        errs.append(err)
+        focks, errs = focks[-8:], errs[-8:]
+        m = len(focks)
+        Bm = -np.ones((m + 1, m + 1))
+        Bm[m, m] = 0.0
+        for i in range(m):
+            for j in range(m):
+                Bm[i, j] = np.sum(errs[i] * errs[j])
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        c = np.linalg.solve(Bm, rhs)
+        _, C = canonical(sum(c[i] * focks[i] for i in range(m)))
+        Cocc = C[:, :o]
+    else:
+        raise RuntimeError("scf_in_field: no convergence")
+    e_scf = 0.5 * np.sum(D * (hF + F)) + ham.e_nuc
+    eps, C = canonical(F)
+    eri = np.einsum("pqrs,pi,qj,rk,sl->ijkl", g, C, C, C, C, optimize=True)
+    out = MOHamiltonian(o, np.diag(eps), irrep=irr[np.argmax(np.abs(C), axis=0)], eri=eri,
+                        nirrep=ham.nirrep)
+    out.e_scf = e_scf
+    return e_scf, out
+
+
+def five_point_derivative(f, delta):
+    """df/dx at 0 from f(+-delta), f(+-2 delta) (error O(delta^4))."""
+    return (8.0 * (f(delta) - f(-delta)) - (f(2 * delta) - f(-2 * delta))) / (12.0 * delta)
 
 
 def synthetic_factors(nocc, nvir, naux, seed, irreps=None, bscale=1.0):

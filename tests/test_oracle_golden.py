@@ -231,3 +231,36 @@ def test_ccpvdz_config1_fixture():
     h = ccsd.run_ccsd(ham, cc_conv=10, maxcyc=60, exporder=5)
     assert h["converged"]
     assert -0.22 < h["e_final"] < -0.19
+
+
+# out.zmat.026 (H2O/DZP, CCSD first-order properties, PROPS=1): the dipole of
+# the SCF density (:762-763) and of the correlated density after the
+# orbital-relaxation ("iterative expansion of D(ai)", :745) step (:794-795),
+# z along the C2 axis, atomic units
+GOLD_026_DIPOLE_SCF = 0.8647256373
+GOLD_026_DIPOLE_CCSD = 0.8197061290
+
+
+def test_dipoles_match_reference_026():
+    """The fixture's MO dipole integrals and SCF orbitals give the reference's
+    SCF dipole, and the central finite difference of the oracle's total
+    CCSD energy in a field along z, with the SCF re-solved at each field
+    (orbital-relaxed), gives the reference's correlated dipole: the relaxed
+    CCSD density's dipole is -dE/dF.  Five-point difference at F = +-1e-3,
+    +-2e-3 a.u., CCSD to max|dT| < 1e-11."""
+    from oracle.hamiltonian import five_point_derivative, scf_in_field
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat026.npz"))
+    o = ham.nocc
+    mu_scf = ham.nucdip[2] - 2.0 * np.trace(ham.dipole[2][:o, :o])
+    assert abs(mu_scf - GOLD_026_DIPOLE_SCF) < 1e-8, mu_scf
+    # the field-free SCF of the finite-field code is the fixture's
+    e0, h0 = scf_in_field(ham, 0.0)
+    assert abs(e0 - ham.e_scf) < 1e-11
+    np.testing.assert_allclose(h0.eps, ham.eps, atol=1e-10)
+
+    def e_total(field):
+        e_scf, hf = scf_in_field(ham, field)
+        return e_scf + ccsd.run_ccsd(hf, cc_conv=11, maxcyc=100, exporder=5)["e_final"]
+
+    mu_ccsd = ham.nucdip[2] - five_point_derivative(e_total, 1e-3)
+    assert abs(mu_ccsd - GOLD_026_DIPOLE_CCSD) < 3e-8, mu_ccsd - GOLD_026_DIPOLE_CCSD
