@@ -38,7 +38,7 @@ SYMBOLS = [
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
     "aces_intprc_df",
     "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
-    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "aces_set_tc_wide", "xvcc_run", "xlambda_run", "xdens_1pdm",
+    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "aces_set_tc_wide", "aces_set_autotune", "aces_autotune_stats", "xvcc_run", "xlambda_run", "xdens_1pdm",
     "xvee_run",
 ]
 
@@ -248,8 +248,22 @@ class Lib:
 
     def set_tc_wide(self, on):
         """Tile width of the single-chunk FP32-output launches: 1 = 128 x 256
-        (aces_set_tc_wide, default), 0 = 128 x 128."""
+        (aces_set_tc_wide, default), 0 = 128 x 144."""
         self._chk("aces_set_tc_wide", self.h.aces_set_tc_wide(int(on)))
+
+    def set_autotune(self, mode):
+        """Tile autotuner (aces_set_autotune): 1 = time the applicable tile
+        variants on the first product of each shape class and reuse the
+        fastest, 0 = built-in rules (default), 2 = forget the cached choices."""
+        self._chk("aces_set_autotune", self.h.aces_set_autotune(int(mode)))
+
+    def autotune_stats(self):
+        """(classes tuned, classes that left the built-in rule, device ms of
+        the timed trial runs) -- aces_autotune_stats."""
+        n, c, ms = C.c_longlong(), C.c_longlong(), C.c_double()
+        self._chk("aces_autotune_stats",
+                  self.h.aces_autotune_stats(C.byref(n), C.byref(c), C.byref(ms)))
+        return n.value, c.value, ms.value
 
     def debug_inject(self, mode):
         """Test hook: 1 = the tensor-core producer issues no copies (aces_debug_inject)."""

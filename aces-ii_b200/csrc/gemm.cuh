@@ -185,5 +185,12 @@ void tc_set_wide(int on);
 // columns runs on the 128 x 256 tiles (the knob is on, 144 < N <= 256 and
 // the segments' k tiles form one chunk)
 bool bf16x3_wide_applies(const SplitOperand *A, int nseg, int N);
+// tile autotuner of the tensor-core launches (process-wide switch; choices
+// cached per device and shape class): on/off, forget every choice, and the
+// number of classes tuned, how many of them left the default variant, and the
+// device ms their timed runs took
+void tc_set_autotune(int on);
+void tc_autotune_reset();
+void tc_autotune_stats(long long *classes, long long *changed, double *ms);
 
 }  // namespace acesb200

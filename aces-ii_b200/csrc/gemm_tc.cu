@@ -1183,27 +1183,163 @@ int launch_prepared(Launch &L, double alpha, double beta, double *part, cudaStre
 }
 }  // namespace
 
-int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
-                         double alpha, double beta, const CView &C, cudaStream_t st) {
-  if (M <= 0 || N <= 0) return ACES_OK;
-  Launch L;
-  memset(&L, 0, sizeof(L));
-  L.nprob = 1;
-  L.cg = pairs_for(M) ? 2 : 1;
-  ACES_TRY(set_problem(L, 0, A, B, nseg, M, N, C));
-  Problem &P = L.prob[0];
-  // split K when the output has too few tiles to fill the SMs (CTA pairs)
-  const long long tiles = (long long)P.tilesN * P.tilesM;
-  const int nsm = L.cg == 2 ? max_pairs() : num_sms();
+namespace {
+// ---- tile autotuner -------------------------------------------------------
+// With aces_set_autotune(1), the first product of each shape class on a
+// device times the tile variants that apply to it and caches the fastest;
+// later products of the class launch the cached variant directly.  Variants:
+// one CTA per 128 x TBN_1 tile or CTA pairs (single and grouped products of
+// >= 256 rows), split K at the wave-efficiency slice count or none (single
+// products), and for batched FP32-output launches 128 x TBN_1 or 128 x 256
+// tiles.  A class is the launch
+// kind, the K segment (or problem) count, FP32 output, eligibility for pairs,
+// and the output tile counts and k tile count rounded to two significant
+// bits.  Each candidate runs once untimed and three times timed (CUDA events)
+// on the product's stream, into the product's own output when beta = 0 and
+// into a zeroed scratch array otherwise; batched launches with beta != 0 are
+// not tuned (they take a cached choice or the default).  Nothing is tuned
+// while the stream is being captured.  Every variant meets the same error
+// bound (same K order and FP32 chunks); one replaces the default only when at
+// least 3 % faster, so timing noise keeps the default.
+struct TuneChoice {
+  int cg = 1;       // CTAs per tile
+  int bn = 0;       // batched FP32 output: tile width (0 = the default rule)
+  int nosplit = 0;  // single products: 1 = no split K
+};
+struct TuneKey {
+  int dev, kind, nseg, flags, tm, tn, kt;
+  bool operator==(const TuneKey &o) const {
+    return dev == o.dev && kind == o.kind && nseg == o.nseg && flags == o.flags &&
+           tm == o.tm && tn == o.tn && kt == o.kt;
+  }
+};
+struct TuneKeyHash {
+  size_t operator()(const TuneKey &k) const {
+    const int v[7] = {k.dev, k.kind, k.nseg, k.flags, k.tm, k.tn, k.kt};
+    size_t h = 1469598103934665603ULL;
+    for (int x : v) h = (h ^ (size_t)(unsigned)x) * 1099511628211ULL;
+    return h;
+  }
+};
+struct TuneState {
+  std::mutex mu;
+  std::unordered_map<TuneKey, TuneChoice, TuneKeyHash> cache;
+  long long classes = 0, changed = 0;
+  double ms = 0.0;  // device time spent in timed candidate runs
+};
+TuneState &tune_state() {
+  static TuneState s;
+  return s;
+}
+std::atomic<int> g_autotune{0};
+// largest scratch output of a tuning run (larger products keep the default)
+constexpr size_t kTuneScratchMax = size_t(1) << 30;
+
+// x rounded to its two leading bits below the top one (4 classes per octave)
+int bucket2(long long x) {
+  if (x < 4) return (int)x;
+  const int b = 63 - __builtin_clzll((unsigned long long)x);
+  return (b << 2) | (int)((x >> (b - 2)) & 3);
+}
+
+bool tune_lookup(const TuneKey &key, TuneChoice *out) {
+  TuneState &s = tune_state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.cache.find(key);
+  if (it == s.cache.end()) return false;
+  *out = it->second;
+  return true;
+}
+void tune_store(const TuneKey &key, const TuneChoice &ch, bool changed, double ms) {
+  TuneState &s = tune_state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (s.cache.emplace(key, ch).second) {
+    ++s.classes;
+    if (changed) ++s.changed;
+    s.ms += ms;
+  }
+}
+// whether candidates may be timed on st now (not while it is captured)
+bool can_time(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cs == cudaStreamCaptureStatusNone;
+}
+// mean device ms of three runs after an untimed one
+int time_runs(const std::function<int()> &run, cudaStream_t st, float *ms) {
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  int rc = ACES_OK;
+  for (int i = 0; i < 2 && rc == ACES_OK; ++i)
+    if (cudaEventCreate(&e[i]) != cudaSuccess) {
+      set_error("autotune: cudaEventCreate failed");
+      rc = ACES_ERR_CUDA;
+    }
+  if (rc == ACES_OK) rc = run();
+  if (rc == ACES_OK && cudaEventRecord(e[0], st) != cudaSuccess) rc = ACES_ERR_CUDA;
+  for (int r = 0; r < 3 && rc == ACES_OK; ++r) rc = run();
+  if (rc == ACES_OK && (cudaEventRecord(e[1], st) != cudaSuccess ||
+                        cudaEventSynchronize(e[1]) != cudaSuccess ||
+                        cudaEventElapsedTime(ms, e[0], e[1]) != cudaSuccess)) {
+    set_error("autotune: event timing failed");
+    rc = ACES_ERR_CUDA;
+  }
+  if (rc == ACES_OK) *ms /= 3.0f;
+  for (int i = 0; i < 2; ++i)
+    if (e[i]) cudaEventDestroy(e[i]);
+  return rc;
+}
+// times the candidates (cands[0] = the default) with run(choice, scratch
+// output or nullptr); returns the index of the one to keep
+int tune_pick(const std::vector<TuneChoice> &cands,
+              const std::function<int(const TuneChoice &)> &run, cudaStream_t st, int *pick,
+              double *total_ms) {
+  float t_def = 0.0f, best = 0.0f;
+  *pick = 0;
+  *total_ms = 0.0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    float ms = 0.0f;
+    ACES_TRY(time_runs([&] { return run(cands[i]); }, st, &ms));
+    *total_ms += 4.0 * ms;
+    if (i == 0) {
+      t_def = best = ms;
+    } else if (ms < best) {
+      best = ms;
+      *pick = (int)i;
+    }
+  }
+  if (*pick != 0 && best > 0.97f * t_def) *pick = 0;
+  return ACES_OK;
+}
+// RAII scratch output of the tuning runs (zeroed, so accumulating trial runs
+// read finite values)
+struct TuneScratch {
+  double *p = nullptr;
+  ~TuneScratch() {
+    if (p) dev_free(p);
+  }
+  int get(size_t doubles, cudaStream_t st) {
+    if (dev_alloc((void **)&p, doubles * sizeof(double)) != cudaSuccess || !p) {
+      p = nullptr;
+      set_error("autotune: scratch allocation of %zu doubles failed", doubles);
+      return ACES_ERR_NOMEM;
+    }
+    ACES_CUDA(cudaMemsetAsync(p, 0, doubles * sizeof(double), st));
+    return ACES_OK;
+  }
+};
+
+// split-K slice count of a single product: the count (at least 256 K elements
+// each, at most ~4 waves of tiles) whose tiles fill the SMs' waves best, ties
+// to fewer slices (less partial traffic); 1 when the tiles fill the SMs
+int split_slices(long long tiles, int kTilesTotal, int nsm) {
   int Z = 1;
-  double *part = nullptr;
-  if (tiles < nsm && P.kTilesTotal >= 8 * kUnit) {
-    // the slice count (at least 256 K elements each, at most ~4 waves of
-    // tiles) whose tiles fill the SMs' waves best; ties go to fewer slices
-    // (less partial traffic)
+  if (tiles < nsm && kTilesTotal >= 8 * kUnit) {
     double best = 0.0;
     const long long zmax =
-        std::min<long long>(P.kTilesTotal / (4 * kUnit), (4LL * nsm + tiles - 1) / tiles);
+        std::min<long long>(kTilesTotal / (4 * kUnit), (4LL * nsm + tiles - 1) / tiles);
     for (int z = 2; z <= zmax; ++z) {
       const double waves = (double)(tiles * z) / nsm;
       const double eff = waves / std::ceil(waves);
@@ -1212,14 +1348,30 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
         Z = z;
       }
     }
-    if (Z > 1) {
-      P.ktc = (P.kTilesTotal + Z - 1) / Z;
-      Z = (P.kTilesTotal + P.ktc - 1) / P.ktc;
-      part = splitk_workspace((size_t)Z * M * N);
-      if (!part) {
-        set_error("gemm_nt_bf16x3: split-K workspace allocation failed");
-        return ACES_ERR_NOMEM;
-      }
+  }
+  return Z;
+}
+
+int multi_run(const TuneChoice &ch, const SplitOperand *A, const SplitOperand *B, int nseg,
+              int M, int N, double alpha, double beta, const CView &C, cudaStream_t st) {
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.nprob = 1;
+  L.cg = ch.cg == 2 ? 2 : 1;
+  ACES_TRY(set_problem(L, 0, A, B, nseg, M, N, C));
+  Problem &P = L.prob[0];
+  // split K when the output has too few tiles to fill the SMs (CTA pairs)
+  const long long tiles = (long long)P.tilesN * P.tilesM;
+  const int nsm = L.cg == 2 ? max_pairs() : num_sms();
+  int Z = ch.nosplit ? 1 : split_slices(tiles, P.kTilesTotal, nsm);
+  double *part = nullptr;
+  if (Z > 1) {
+    P.ktc = (P.kTilesTotal + Z - 1) / Z;
+    Z = (P.kTilesTotal + P.ktc - 1) / P.ktc;
+    part = splitk_workspace((size_t)Z * M * N);
+    if (!part) {
+      set_error("gemm_nt_bf16x3: split-K workspace allocation failed");
+      return ACES_ERR_NOMEM;
     }
   }
   const long long nTiles = tiles * Z;
@@ -1234,18 +1386,11 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
   return ACES_OK;
 }
 
-int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha, double beta,
-                           cudaStream_t st) {
-  if (nprob < 1 || nprob > kMaxProb) {
-    set_error("gemm_nt_bf16x3_grouped: %d problems (1..%d)", nprob, kMaxProb);
-    return ACES_ERR_ARG;
-  }
+int grouped_run(int cg, const GroupedProblem *probs, int nprob, double alpha, double beta,
+                cudaStream_t st) {
   Launch L;
   memset(&L, 0, sizeof(L));
-  int min_rows = 1 << 30;
-  for (int g = 0; g < nprob; ++g)
-    if (probs[g].M > 0 && probs[g].N > 0) min_rows = std::min(min_rows, probs[g].M);
-  L.cg = pairs_for(min_rows) ? 2 : 1;
+  L.cg = cg == 2 ? 2 : 1;
   long long tiles = 0;
   int n = 0;
   for (int g = 0; g < nprob; ++g) {
@@ -1266,6 +1411,159 @@ int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha,
   return launch_prepared(L, alpha, beta, nullptr, st);
 }
 
+int batched_run(const TuneChoice &ch, const SplitOperand *Apar, const SplitOperand *Bpar,
+                int nseg, int M, int N, const BatchEntry *d_entries, int nbatch, double alpha,
+                double beta, const CView &C, bool f32out, cudaStream_t st) {
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.nprob = 1;
+  L.cg = ch.cg == 2 ? 2 : 1;
+  // FP32 output whose every tile is one accumulation chunk, with 144 < N <=
+  // 256: one wide tile instead of a full and a ragged narrow one.  Where N
+  // fits one narrow tile or is much larger, the 3-stage narrow tiles win
+  // (o = 6, v = 128 class launches against 128-wide tiles: 32 % slower with
+  // N = 128 on wide tiles, 3 % slower with N = 16384)
+  if (L.cg == 2)
+    L.bn = TBN;
+  else if (ch.bn)
+    L.bn = f32out ? ch.bn : TBN_1;
+  else
+    L.bn = f32out && N > TBN_1 && N <= TBN_WIDE && g_tc_wide.load() ? TBN_WIDE : TBN_1;
+  ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  if (L.bn == TBN_WIDE && L.prob[0].kTilesTotal > L.prob[0].chunk) {
+    L.bn = TBN_1;
+    ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  }
+  Problem &P = L.prob[0];
+  P.batch = d_entries;
+  P.nbatch = nbatch;
+  P.f32out = f32out ? 1 : 0;
+  const long long tiles = (long long)P.tilesM * P.tilesN * nbatch;
+  if (tiles > (1LL << 31) - 1) {
+    set_error("gemm_nt_bf16x3_batched: %lld output tiles exceed the scheduler range", tiles);
+    return ACES_ERR_ARG;
+  }
+  P.tile0 = 0;
+  L.nTiles = (int)tiles;
+  return launch_prepared(L, alpha, beta, nullptr, st);
+}
+
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return dev;
+}
+}  // namespace
+
+int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg, int M, int N,
+                         double alpha, double beta, const CView &C, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return ACES_OK;
+  TuneChoice def;
+  def.cg = pairs_for(M) ? 2 : 1;
+  if (!g_autotune.load() || nseg < 1 || nseg > kMaxSeg)
+    return multi_run(def, A, B, nseg, M, N, alpha, beta, C, st);
+  int kt = 0;
+  for (int s = 0; s < nseg; ++s) kt += A[s].k_pad / TBK;
+  const long long tm = (M + TBM - 1) / TBM, tn = (N + TBN_1 - 1) / TBN_1;
+  const TuneKey key{current_device(), 0, nseg, M >= 2 * TBM ? 1 : 0, bucket2(tm), bucket2(tn),
+                    bucket2(kt)};
+  TuneChoice ch;
+  if (tune_lookup(key, &ch)) return multi_run(ch, A, B, nseg, M, N, alpha, beta, C, st);
+  std::vector<TuneChoice> cands{def};
+  if (def.cg == 1 && split_slices(tm * tn, kt, num_sms()) > 1) {
+    TuneChoice c;
+    c.nosplit = 1;
+    cands.push_back(c);
+  }
+  if (M >= 2 * TBM) {
+    TuneChoice c;
+    c.cg = def.cg == 2 ? 1 : 2;
+    cands.push_back(c);
+  }
+  const bool scratch_out = beta != 0.0;
+  if (cands.size() == 1 || (scratch_out && (size_t)M * N * sizeof(double) > kTuneScratchMax)) {
+    tune_store(key, def, false, 0.0);
+    return multi_run(def, A, B, nseg, M, N, alpha, beta, C, st);
+  }
+  if (!can_time(st)) return multi_run(def, A, B, nseg, M, N, alpha, beta, C, st);
+  int pick = 0;
+  double ms = 0.0;
+  {
+    TuneScratch scr;
+    CView Ct = C;
+    if (scratch_out) {
+      ACES_TRY(scr.get((size_t)M * N, st));
+      Ct = cview_rowmajor(scr.p, N);
+    }
+    ACES_TRY(tune_pick(
+        cands,
+        [&](const TuneChoice &c) { return multi_run(c, A, B, nseg, M, N, alpha, beta, Ct, st); },
+        st, &pick, &ms));
+  }
+  tune_store(key, cands[pick], pick != 0, ms);
+  return multi_run(cands[pick], A, B, nseg, M, N, alpha, beta, C, st);
+}
+
+int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha, double beta,
+                           cudaStream_t st) {
+  if (nprob < 1 || nprob > kMaxProb) {
+    set_error("gemm_nt_bf16x3_grouped: %d problems (1..%d)", nprob, kMaxProb);
+    return ACES_ERR_ARG;
+  }
+  int min_rows = 1 << 30;
+  long long tiles = 0, outs = 0;
+  int kt = 0;
+  for (int g = 0; g < nprob; ++g) {
+    const GroupedProblem &q = probs[g];
+    if (q.M <= 0 || q.N <= 0) continue;
+    min_rows = std::min(min_rows, q.M);
+    tiles += (long long)((q.M + TBM - 1) / TBM) * ((q.N + TBN_1 - 1) / TBN_1);
+    outs += (long long)q.M * q.N;
+    if (q.nseg >= 1 && q.nseg <= kMaxSeg)
+      for (int s = 0; s < q.nseg; ++s) kt = std::max(kt, q.A[s].k_pad / TBK);
+  }
+  const int def = pairs_for(min_rows) ? 2 : 1;
+  if (!g_autotune.load() || tiles == 0 || min_rows < 2 * TBM)
+    return grouped_run(def, probs, nprob, alpha, beta, st);
+  const TuneKey key{current_device(), 1, nprob, 1, bucket2(tiles), 0, bucket2(kt)};
+  TuneChoice ch;
+  if (tune_lookup(key, &ch)) return grouped_run(ch.cg, probs, nprob, alpha, beta, st);
+  const bool scratch_out = beta != 0.0;
+  if (scratch_out && (size_t)outs * sizeof(double) > kTuneScratchMax) {
+    ch.cg = def;
+    tune_store(key, ch, false, 0.0);
+    return grouped_run(def, probs, nprob, alpha, beta, st);
+  }
+  if (!can_time(st)) return grouped_run(def, probs, nprob, alpha, beta, st);
+  std::vector<TuneChoice> cands(2);
+  cands[0].cg = def;
+  cands[1].cg = def == 2 ? 1 : 2;
+  int pick = 0;
+  double ms = 0.0;
+  {
+    TuneScratch scr;
+    GroupedProblem tp[kMaxProb];
+    for (int g = 0; g < nprob; ++g) tp[g] = probs[g];
+    if (scratch_out) {
+      ACES_TRY(scr.get((size_t)outs, st));
+      size_t off = 0;
+      for (int g = 0; g < nprob; ++g) {
+        if (tp[g].M <= 0 || tp[g].N <= 0) continue;
+        tp[g].C = cview_rowmajor(scr.p + off, tp[g].N);
+        off += (size_t)tp[g].M * tp[g].N;
+      }
+    }
+    ACES_TRY(tune_pick(
+        cands, [&](const TuneChoice &c) { return grouped_run(c.cg, tp, nprob, alpha, beta, st); },
+        st, &pick, &ms));
+  }
+  tune_store(key, cands[pick], pick != 0, ms);
+  return grouped_run(cands[pick].cg, probs, nprob, alpha, beta, st);
+}
+
 int gemm_nt_bf16x3(const SplitOperand &A, const SplitOperand &B, int M, int N, double alpha,
                    double beta, const CView &C, cudaStream_t st) {
   return gemm_nt_bf16x3_multi(&A, &B, 1, M, N, alpha, beta, C, st);
@@ -1284,6 +1582,10 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
     set_error("gemm_nt_bf16x3_batched: FP32 output needs unit m stride (or n, for beta = 0)");
     return ACES_ERR_ARG;
   }
+  if (nseg < 1 || nseg > kMaxSeg) {
+    set_error("gemm_nt_bf16x3_batched: %d K segments (1..%d)", nseg, kMaxSeg);
+    return ACES_ERR_ARG;
+  }
   // every live row of every window inside its parent: the TMA coordinates of
   // live rows stay in range, rows past a window read its neighbours (or the
   // zero fill past the parent) and only reach discarded outputs
@@ -1296,35 +1598,68 @@ int gemm_nt_bf16x3_batched(const SplitOperand *Apar, const SplitOperand *Bpar, i
         return ACES_ERR_ARG;
       }
     }
-  Launch L;
-  memset(&L, 0, sizeof(L));
-  L.nprob = 1;
-  L.cg = pairs_for(M) ? 2 : 1;
-  // FP32 output whose every tile is one accumulation chunk, with 144 < N <=
-  // 256: one wide tile instead of a full and a ragged narrow one.  Where N
-  // fits one narrow tile or is much larger, the 3-stage narrow tiles win
-  // (o = 6, v = 128 class launches against 128-wide tiles: 32 % slower with
-  // N = 128 on wide tiles, 3 % slower with N = 16384)
-  L.bn = f32out && L.cg == 1 && N > TBN_1 && N <= TBN_WIDE && g_tc_wide.load()
-             ? TBN_WIDE
-             : (L.cg == 2 ? TBN : TBN_1);
-  ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
-  if (L.bn == TBN_WIDE && L.prob[0].kTilesTotal > L.prob[0].chunk) {
-    L.bn = TBN_1;
-    ACES_TRY(set_problem(L, 0, Apar, Bpar, nseg, M, N, C));
+  TuneChoice def;
+  def.cg = pairs_for(M) ? 2 : 1;
+  if (!g_autotune.load())
+    return batched_run(def, Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha, beta, C, f32out,
+                       st);
+  int kt = 0;
+  for (int s = 0; s < nseg; ++s) kt += Apar[s].k_pad / TBK;
+  const long long tm = (M + TBM - 1) / TBM, tn = (N + TBN_1 - 1) / TBN_1;
+  const TuneKey key{current_device(), 2, nseg,
+                    (M >= 2 * TBM ? 1 : 0) | (f32out ? 2 : 0) | (N > TBN_1 ? 4 : 0) |
+                        (N > TBN_WIDE ? 8 : 0),
+                    bucket2(tm * nbatch), bucket2(tn), bucket2(kt)};
+  TuneChoice ch;
+  if (tune_lookup(key, &ch))
+    return batched_run(ch, Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha, beta, C, f32out,
+                       st);
+  // the trial runs write the product's own output: only for beta = 0
+  if (beta != 0.0 || !can_time(st))
+    return batched_run(def, Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha, beta, C, f32out,
+                       st);
+  // both widths of the one-CTA tile (cands[0] keeps the default rule); the
+  // CTA pairs stay with the aces_set_tc_pairs switch here
+  std::vector<TuneChoice> cands{def};
+  if (def.cg == 1 && f32out && N > TBN_1 && N <= TBN_WIDE && kt <= chunk_for(kt)) {
+    TuneChoice c;
+    c.bn = g_tc_wide.load() ? TBN_1 : TBN_WIDE;
+    cands.push_back(c);
   }
-  Problem &P = L.prob[0];
-  P.batch = d_entries;
-  P.nbatch = nbatch;
-  P.f32out = f32out ? 1 : 0;
-  const long long tiles = (long long)P.tilesM * P.tilesN * nbatch;
-  if (tiles > (1LL << 31) - 1) {
-    set_error("gemm_nt_bf16x3_batched: %lld output tiles exceed the scheduler range", tiles);
-    return ACES_ERR_ARG;
+  if (cands.size() == 1) {
+    tune_store(key, def, false, 0.0);
+    return batched_run(def, Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha, beta, C, f32out,
+                       st);
   }
-  P.tile0 = 0;
-  L.nTiles = (int)tiles;
-  return launch_prepared(L, alpha, beta, nullptr, st);
+  int pick = 0;
+  double ms = 0.0;
+  ACES_TRY(tune_pick(cands,
+                     [&](const TuneChoice &c) {
+                       return batched_run(c, Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha,
+                                          beta, C, f32out, st);
+                     },
+                     st, &pick, &ms));
+  tune_store(key, cands[pick], pick != 0, ms);
+  return batched_run(cands[pick], Apar, Bpar, nseg, M, N, d_entries, nbatch, alpha, beta, C,
+                     f32out, st);
+}
+
+void tc_set_autotune(int on) { g_autotune.store(on ? 1 : 0); }
+
+void tc_autotune_reset() {
+  TuneState &s = tune_state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  s.cache.clear();
+  s.classes = s.changed = 0;
+  s.ms = 0.0;
+}
+
+void tc_autotune_stats(long long *classes, long long *changed, double *ms) {
+  TuneState &s = tune_state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (classes) *classes = s.classes;
+  if (changed) *changed = s.changed;
+  if (ms) *ms = s.ms;
 }
 
 SplitOperand split_view(const SplitOperand &p, int row0, int rows) {

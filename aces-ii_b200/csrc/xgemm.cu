@@ -115,6 +115,24 @@ extern "C" int aces_set_tc_wide(int on) {
   return ACES_OK;
 }
 
+extern "C" int aces_set_autotune(int mode) {
+  if (mode < 0 || mode > 2) {
+    set_error("aces_set_autotune: mode %d (0, 1 or 2)", mode);
+    return ACES_ERR_ARG;
+  }
+  if (mode == 2) {
+    tc_autotune_reset();
+    return ACES_OK;
+  }
+  tc_set_autotune(mode);
+  return ACES_OK;
+}
+
+extern "C" int aces_autotune_stats(long long *classes, long long *changed, double *tune_ms) {
+  tc_autotune_stats(classes, changed, tune_ms);
+  return ACES_OK;
+}
+
 extern "C" int aces_debug_inject(int mode) {
   if (mode != 0 && mode != 1) {
     set_error("aces_debug_inject: mode %d (0 or 1)", mode);

@@ -62,6 +62,11 @@ def args():
                    help="1: replay each cycle's residual pass from a CUDA graph captured on "
                         "the second cycle, 0: launch every kernel from the host (default 1, "
                         "and 0 for the c5 batch, whose short solves do not amortise a capture)")
+    p.add_argument("--autotune", type=int, default=None,
+                   help="1: tensor-core tile variants timed once per shape class and the "
+                        "fastest reused (aces_set_autotune), 0: built-in tile rules (default "
+                        "1 for the c5 batch, after an untimed tuning pass over its systems; "
+                        "0 otherwise)")
     p.add_argument("--batch-bscale", type=float, default=1.0,
                    help="scale of the DF factors of the 64-system batch (--workload c5)")
     p.add_argument("--no-lambda", action="store_true",
@@ -263,6 +268,21 @@ def run_batch(a, rank=0, world=1, local_rank=0):
     tot = {"bf16x3": 0.0, "fp64": 0.0}
     flops_ladder = 0.0
     flops_exec = 0.0
+    # tile autotuner: one untimed split-precision cycle of every system of
+    # this rank times the tile variants of each shape class the batch meets,
+    # so the timed solves launch the cached choices
+    tune = 1 if a.autotune is None else a.autotune
+    lib.init(local_rank)
+    lib.set_autotune(2)
+    lib.set_autotune(tune)
+    if tune:
+        for k in mine:
+            eps, B, irr = synthetic_df(**systems[k], bscale=a.batch_bscale)
+            lib.init(local_rank)
+            put_lists_dpd(lib, eps, B, irr, systems[k]["nocc"], systems[k]["nvir"], dev)
+            lib.xvcc(cc_conv=7, cc_maxcyc=1, cc_exporder=5, precision=ab.PREC_BF16X3,
+                     allow_noconv=True, use_graph=0)
+    tuned_before = lib.autotune_stats()
     # warm-up, untimed: the heaviest of this rank's systems once in each
     # precision, so the timed solves find every kernel loaded and the device
     # pool holding blocks of the largest sizes (as in a long batch)
@@ -303,6 +323,8 @@ def run_batch(a, rank=0, world=1, local_rank=0):
                          "seconds": t, "setup_seconds": c.seconds_setup,
                          "seconds_per_iter": c.seconds_per_iter}
         rows.append(row)
+    tuned_after = lib.autotune_stats()
+    lib.set_autotune(0)
     lib.fin()
     dE = [abs(r["bf16x3"]["e"] - r["fp64"]["e"]) for r in rows]
     conv = all(r["bf16x3"]["converged"] and r["fp64"]["converged"] for r in rows)
@@ -328,7 +350,14 @@ def run_batch(a, rank=0, world=1, local_rank=0):
                        "execution": "sequential xvcc_run calls"
                                     + (f", systems split over {world} ranks by flop weight"
                                        if world > 1 else ""),
-                       "use_graph": a.use_graph},
+                       "use_graph": a.use_graph,
+                       "autotune": {"on": bool(tune), "classes": tuned_after[0],
+                                    "classes_off_default": tuned_after[1],
+                                    "tuning_ms_untimed_pass": tuned_before[2],
+                                    "classes_tuned_in_timed_solves":
+                                        tuned_after[0] - tuned_before[0],
+                                    "tuning_ms_in_timed_solves":
+                                        tuned_after[2] - tuned_before[2]}},
             "scaling": "strong",
             "fp64_seconds": tot["fp64"], "speedup_split_vs_fp64": tot["fp64"] / tot["bf16x3"],
             "max_abs_dE": max(dE), "all_converged": conv,

@@ -176,7 +176,7 @@ int aces_set_wait_limit(double seconds);
 int aces_debug_inject(int mode);
 /* Tile variant of the tensor-core contractions (no counterpart in the
  * reference): 1 = products of at least 256 rows run on CTA pairs (tcgen05
- * cta_group::2, 256 x 128 tiles), 0 = one CTA per 128 x 128 tile (the
+ * cta_group::2, 256 x 128 tiles), 0 = one CTA per 128 x 144 tile (the
  * default, faster on B200 for the CC contractions).  Both give the same
  * error bound; process-wide. */
 int aces_set_tc_pairs(int on);
@@ -186,6 +186,24 @@ int aces_set_tc_pairs(int on);
  * 128 x 256 tile across N (the default), 0 = 128 x 144 tiles.  Same
  * arithmetic either way; process-wide. */
 int aces_set_tc_wide(int on);
+/* Tile autotuner of the tensor-core contractions (no counterpart in the
+ * reference; the reference's XGEMM calls take whatever its BLAS does).
+ * mode 1: the first product of each shape class on a device times the tile
+ * variants that apply to it -- one CTA per tile or CTA pairs and split K or
+ * not for single and grouped products, 144- or 256-wide tiles for the
+ * FP32-output batched (T) launches -- with CUDA
+ * events on the product's stream (the call then waits for the device), and
+ * later products of the class reuse the fastest; mode 0 (default): the
+ * built-in rules; mode 2: forget every cached choice (the on/off state is
+ * kept).  A class is the launch kind, segment count, output type and the
+ * tile and k-tile counts to two significant bits.  No tuning while the
+ * stream is being captured; trial runs write the product's own output when
+ * beta = 0, else a scratch array from the library's allocator.  Every
+ * variant meets the same error bound.  Process-wide. */
+int aces_set_autotune(int mode);
+/* Shape classes tuned so far, how many of them chose a variant other than
+ * the built-in rule, and the device ms the timed trial runs took. */
+int aces_autotune_stats(long long *classes, long long *changed, double *tune_ms);
 
 /* ---- member programs ---------------------------------------------------- */
 

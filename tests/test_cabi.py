@@ -154,3 +154,15 @@ def test_header_is_c99_and_config_layout_matches_ctypes(tmp_path):
     assert int(out["sizeof"]) == ctypes.sizeof(ab.EOMConfig)
     for f in efields:
         assert int(out[f]) == getattr(ab.EOMConfig, f).offset, f
+
+
+def test_autotune_switch_and_stats_without_a_gpu(lib):
+    """aces_set_autotune takes modes 0/1/2 only; with nothing tuned the stats
+    are zero; the switch is left off (the default) for the other tests."""
+    assert lib.h.aces_set_autotune(3) == -1
+    assert lib.h.aces_set_autotune(-1) == -1
+    lib.set_autotune(2)
+    lib.set_autotune(1)
+    assert lib.autotune_stats() == (0, 0, 0.0)
+    lib.set_autotune(0)
+    assert lib.autotune_stats() == (0, 0, 0.0)
