@@ -264,3 +264,33 @@ def test_dipoles_match_reference_026():
 
     mu_ccsd = ham.nucdip[2] - five_point_derivative(e_total, 1e-3)
     assert abs(mu_ccsd - GOLD_026_DIPOLE_CCSD) < 3e-8, mu_ccsd - GOLD_026_DIPOLE_CCSD
+
+
+def test_zvector_relaxed_dipole_matches_reference_026():
+    """The orbital-relaxed density by the Z-vector method (oracle.relaxed:
+    the CC Lagrangian's orbital gradient X(a,i), the RHF response of the
+    Brillouin condition, Z^T A = -X; dens/vdens.F:1036-1137) gives the
+    reference's correlated dipole analytically, and its three terms add up
+    to the finite-field derivatives of the test above: the fixed-orbital
+    CC term Tr(D z) and the orbital-relaxation term sum Z_ai z_ai."""
+    from oracle.hamiltonian import MOHamiltonian, five_point_derivative
+    from oracle import relaxed
+    ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat026.npz"))
+    z = ham.dipole[2]
+    dens = relaxed.relaxed_density(ham, cc_conv=11)
+    p = relaxed.property_derivative(ham, dens, z)
+    mu = ham.nucdip[2] - p["total"]
+    assert abs(mu - GOLD_026_DIPOLE_CCSD) < 3e-8, mu - GOLD_026_DIPOLE_CCSD
+    assert abs(ham.nucdip[2] - p["scf"] - GOLD_026_DIPOLE_SCF) < 1e-8
+    # the fixed-orbital CC term against the finite difference of the energy
+    # with f -> f + x z (non-HF Fock, orbitals unchanged)
+    o = ham.nocc
+
+    def e_fixed(x):
+        h = MOHamiltonian(o, ham.fock + x * z, irrep=ham.irrep, eri=ham._eri,
+                          nirrep=ham.nirrep)
+        return ccsd.run_ccsd(h, cc_conv=12, maxcyc=200, exporder=8)["e_final"]
+
+    assert abs(p["cc"] - five_point_derivative(e_fixed, 1e-3)) < 1e-10
+    # the orbital relaxation moves the dipole by 2.53e-3 a.u. here
+    assert abs(p["relax"] + 2.5299e-3) < 1e-6
