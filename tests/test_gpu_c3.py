@@ -6,7 +6,8 @@ This is where the split contractions run their longest sums: the K = v^2 =
 72900 products (the T1-dressed <am|ef> tau and <mn|ef> tau terms) take the
 256-element FP32 accumulation chunks, and <ab|cd> (42.5 GB of FP64, built on
 the device by aces_intprc_df) feeds the packed ladder every cycle.  The
-|dE| <= 1e-6 Eh for the CCSD energy and for (T).
+accuracy target of the split path: |dE| <= 1e-6 Eh for the CCSD energy and
+for (T).
 """
 import pytest
 
