@@ -592,9 +592,6 @@ def run_ours(a, rank, world, local_rank):
     return line
 
 
-# DRAM bytes (read + write) of one packed ladder (its launches summed), from
-# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the grouped
-# ladder launch at c2
 # DRAM bytes of the grouped packed-ladder launch of the c2 cycle: an ncu
 # capture of its symmetric product alone (--kernel-case ladder-packed, M = K =
 # 16290, N = 400: 1161.2 MB read + 45.4 MB written) scaled by the units the
