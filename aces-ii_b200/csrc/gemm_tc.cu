@@ -1196,7 +1196,9 @@ namespace {
 // and the output tile counts and k tile count rounded to two significant
 // bits.  Each candidate runs once untimed and three times timed (CUDA events)
 // on the product's stream, into the product's own output when beta = 0 and
-// into a zeroed scratch array otherwise; batched launches with beta != 0 are
+// into a zeroed scratch array with unit m stride otherwise (the layout whose
+// epilogue stores coalesce, which the dispatcher gives real outputs);
+// batched launches with beta != 0 are
 // not tuned (they take a cached choice or the default).  Nothing is tuned
 // while the stream is being captured.  Every variant meets the same error
 // bound (same K order and FP32 chunks); one replaces the default only when at
@@ -1496,7 +1498,7 @@ int gemm_nt_bf16x3_multi(const SplitOperand *A, const SplitOperand *B, int nseg,
     CView Ct = C;
     if (scratch_out) {
       ACES_TRY(scr.get((size_t)M * N, st));
-      Ct = cview_rowmajor(scr.p, N);
+      Ct = cview_colmajor(scr.p, M);  // unit m stride, as the dispatcher arranges outputs
     }
     ACES_TRY(tune_pick(
         cands,
@@ -1552,7 +1554,7 @@ int gemm_nt_bf16x3_grouped(const GroupedProblem *probs, int nprob, double alpha,
       size_t off = 0;
       for (int g = 0; g < nprob; ++g) {
         if (tp[g].M <= 0 || tp[g].N <= 0) continue;
-        tp[g].C = cview_rowmajor(scr.p + off, tp[g].N);
+        tp[g].C = cview_colmajor(scr.p + off, tp[g].M);
         off += (size_t)tp[g].M * tp[g].N;
       }
     }
