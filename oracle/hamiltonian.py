@@ -108,6 +108,9 @@ def from_fixture(path):
     ham.dipole = d["dipole"]
     ham.nucdip = d["nucdip"]
     ham.hcore = d["hcore"]
+    if "second" in d.files:   # diagonal second moments x^2, y^2, z^2 (MO basis)
+        ham.second = d["second"]
+        ham.nucsecond = d["nucsecond"]
     return ham
 
 

@@ -226,12 +226,14 @@ class Basis:
         return m
 
     def one_electron(self, charges, centers):
-        """Overlap S, kinetic T, nuclear attraction V, and dipole moments (x,y,z) about origin."""
+        """Overlap S, kinetic T, nuclear attraction V, and dipole moments (x,y,z) about origin;
+        the diagonal second moments (x^2, y^2, z^2) are left in ``self.second_moments``."""
         groups = self._by_l()
         fidx = self._func_index()
         n = self.nprim
         S = np.zeros((n, n)); T = np.zeros((n, n)); V = np.zeros((n, n))
         M = np.zeros((3, n, n))
+        Q = np.zeros((3, n, n))
         for la, ia in groups.items():
             for lb, ib in groups.items():
                 pairs = list(itertools.product(ia, ib))
@@ -272,12 +274,18 @@ class Basis:
                                                 * Ex[2][az, bz, v] * R[(t, u, v)])
                             vval -= Zc * 2 * np.pi / p * acc
                         mvals = []
+                        qvals = []
                         for d in range(3):
                             i_, j_ = e[d]
                             # <x_C> about origin: E_1 + P_x E_0
                             m1 = (Ex[d][i_, j_, 1] if i_ + j_ >= 1 else 0.0) + P[:, d] * Ex[d][i_, j_, 0]
                             m1 = m1 * sq
                             mvals.append(m1 * s1[(d + 1) % 3] * s1[(d + 2) % 3])
+                            # <x^2> about origin: 2 E_2 + 2 P_x E_1 + (P_x^2 + 1/(2p)) E_0
+                            m2 = ((2.0 * Ex[d][i_, j_, 2] if i_ + j_ >= 2 else 0.0)
+                                  + (2.0 * P[:, d] * Ex[d][i_, j_, 1] if i_ + j_ >= 1 else 0.0)
+                                  + (P[:, d] ** 2 + 0.5 / p) * Ex[d][i_, j_, 0]) * sq
+                            qvals.append(m2 * s1[(d + 1) % 3] * s1[(d + 2) % 3])
                         for k, (sa, sb) in enumerate(pairs):
                             fa = fidx[sa][ci]
                             fb = fidx[sb][cj]
@@ -286,8 +294,11 @@ class Basis:
                             V[fa, fb] = vval[k]
                             for d in range(3):
                                 M[d, fa, fb] = mvals[d][k]
+                                Q[d, fa, fb] = qvals[d][k]
         D = self.D
         tr = lambda X: D.T @ X @ D
+        # diagonal second moments <x^2>, <y^2>, <z^2> about the origin
+        self.second_moments = np.array([tr(Q[d]) for d in range(3)])
         return tr(S), tr(T), tr(V), np.array([tr(M[d]) for d in range(3)])
 
     def eri(self):

@@ -27,7 +27,9 @@ inputs and for the cc-pVDZ benchmark system:
 Each file holds: orbital energies (occupied then virtual, each block sorted by
 irrep as the reference's DPD lists order them), the irrep populations
 (pop, vrt), the MO two-electron integrals (pq|rs) packed with 8-fold symmetry,
-the MO dipole integrals, E(SCF) and the nuclear repulsion energy.
+the MO dipole and diagonal second-moment (x^2, y^2, z^2) integrals about the
+origin (the centre of mass) with their nuclear counterparts, E(SCF) and the
+nuclear repulsion energy.
 
 Where the reference prints them, the SCF and nuclear repulsion energies must
 reproduce its records; the script asserts that.
@@ -231,13 +233,16 @@ def build(ref_root, tag):
     g = np.einsum("ijrs,rk->ijks", g, C, optimize=True)
     g = np.einsum("ijks,sl->ijkl", g, C, optimize=True)
     mu_mo = np.array([C.T @ Mu[d] @ C for d in range(3)])
+    q_mo = np.array([C.T @ basis.second_moments[d] @ C for d in range(3)])
+    nucsecond = sum(a[1] * a[2] ** 2 for a in atoms)
     charges = np.array([a[1] for a in atoms])
     nucdip = sum(a[1] * a[2] for a in atoms)
     h_mo = C.T @ (T + V) @ C
     np.savez_compressed(
         os.path.join(os.path.dirname(os.path.abspath(__file__)), fname),
         eps=eps, irrep=irr, pop=pop, vrt=vrt, eri8=pack8(g), nmo=basis.nao,
-        dipole=mu_mo, nucdip=nucdip, hcore=h_mo, e_scf=E_scf, e_nuc=enuc,
+        dipole=mu_mo, nucdip=nucdip, second=q_mo, nucsecond=nucsecond, hcore=h_mo,
+        e_scf=E_scf, e_nuc=enuc,
         charges=charges,
     )
     return eps, irr, pop, vrt, g

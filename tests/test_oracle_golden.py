@@ -239,6 +239,11 @@ def test_ccpvdz_config1_fixture():
 # z along the C2 axis, atomic units
 GOLD_026_DIPOLE_SCF = 0.8647256373
 GOLD_026_DIPOLE_CCSD = 0.8197061290
+# electronic second moments <sum r_a r_a> (XX, YY, ZZ) of the same densities
+# (:764-765, :796-797); the reference's molecular plane is yz, the fixture's
+# xz, so its XX is the fixture's y^2 and its YY the fixture's x^2
+GOLD_026_SECOND_SCF = {"x": 7.1867815660, "y": 5.4134779614, "z": 6.4335007706}
+GOLD_026_SECOND_CCSD = {"x": 7.3082722125, "y": 5.4731788028, "z": 6.5237129470}
 
 
 def test_dipoles_match_reference_026():
@@ -266,13 +271,14 @@ def test_dipoles_match_reference_026():
     assert abs(mu_ccsd - GOLD_026_DIPOLE_CCSD) < 3e-8, mu_ccsd - GOLD_026_DIPOLE_CCSD
 
 
-def test_zvector_relaxed_dipole_matches_reference_026():
+def test_zvector_relaxed_density_matches_reference_026():
     """The orbital-relaxed density by the Z-vector method (oracle.relaxed:
     the CC Lagrangian's orbital gradient X(a,i), the RHF response of the
     Brillouin condition, Z^T A = -X; dens/vdens.F:1036-1137) gives the
-    reference's correlated dipole analytically, and its three terms add up
-    to the finite-field derivatives of the test above: the fixed-orbital
-    CC term Tr(D z) and the orbital-relaxation term sum Z_ai z_ai."""
+    reference's correlated dipole and second moments analytically, and the
+    dipole's terms add up to the finite-field derivatives of the test above:
+    the fixed-orbital CC term Tr(D z) and the orbital-relaxation term
+    sum Z_ai z_ai."""
     from oracle.hamiltonian import MOHamiltonian, five_point_derivative
     from oracle import relaxed
     ham = from_fixture(os.path.join(GOLDEN, "h2o_dzp_zmat026.npz"))
@@ -294,3 +300,10 @@ def test_zvector_relaxed_dipole_matches_reference_026():
     assert abs(p["cc"] - five_point_derivative(e_fixed, 1e-3)) < 1e-10
     # the orbital relaxation moves the dipole by 2.53e-3 a.u. here
     assert abs(p["relax"] + 2.5299e-3) < 1e-6
+    # the second moments of the SCF and of the relaxed correlated density
+    # (the relaxation term is about 1e-2 bohr^2 of each)
+    for d, axis in enumerate("xyz"):
+        q = relaxed.property_derivative(ham, dens, ham.second[d])
+        assert abs(q["scf"] - GOLD_026_SECOND_SCF[axis]) < 1e-8, axis
+        assert abs(q["total"] - GOLD_026_SECOND_CCSD[axis]) < 5e-8, (axis, q)
+        assert abs(q["relax"]) > 5e-3
