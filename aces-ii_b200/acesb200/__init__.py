@@ -38,7 +38,7 @@ SYMBOLS = [
     "aces_putlst_dev", "aces_getall", "aces_putall", "aces_list_memset", "aces_list_devptr",
     "aces_intprc_df",
     "aces_putrec", "aces_getrec", "aces_reclen", "aces_xgemm", "aces_xgemm_static",
-    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "aces_set_tc_wide", "aces_set_autotune", "aces_autotune_stats", "xvcc_run", "xlambda_run", "xdens_1pdm",
+    "aces_set_wait_limit", "aces_debug_inject", "aces_set_tc_pairs", "aces_set_tc_wide", "aces_set_autotune", "aces_autotune_stats", "aces_autotune_save", "aces_autotune_load", "xvcc_run", "xlambda_run", "xdens_1pdm",
     "xvee_run",
 ]
 
@@ -264,6 +264,14 @@ class Lib:
         self._chk("aces_autotune_stats",
                   self.h.aces_autotune_stats(C.byref(n), C.byref(c), C.byref(ms)))
         return n.value, c.value, ms.value
+
+    def autotune_save(self, path):
+        """The current device's cached tile choices to a text file (aces_autotune_save)."""
+        self._chk("aces_autotune_save", self.h.aces_autotune_save(str(path).encode()))
+
+    def autotune_load(self, path):
+        """Tile choices from a file saved by autotune_save (aces_autotune_load)."""
+        self._chk("aces_autotune_load", self.h.aces_autotune_load(str(path).encode()))
 
     def debug_inject(self, mode):
         """Test hook: 1 = the tensor-core producer issues no copies (aces_debug_inject)."""

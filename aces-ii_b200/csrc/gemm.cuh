@@ -192,5 +192,8 @@ bool bf16x3_wide_applies(const SplitOperand *A, int nseg, int N);
 void tc_set_autotune(int on);
 void tc_autotune_reset();
 void tc_autotune_stats(long long *classes, long long *changed, double *ms);
+// the current device's cached choices to / from a text file
+int tc_autotune_save(const char *path);
+int tc_autotune_load(const char *path);
 
 }  // namespace acesb200

@@ -27,6 +27,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -1207,6 +1208,7 @@ struct TuneChoice {
   int cg = 1;       // CTAs per tile
   int bn = 0;       // batched FP32 output: tile width (0 = the default rule)
   int nosplit = 0;  // single products: 1 = no split K
+  int changed = 0;  // cached entries: the choice differs from the built-in rule
 };
 struct TuneKey {
   int dev, kind, nseg, flags, tm, tn, kt;
@@ -1255,7 +1257,9 @@ bool tune_lookup(const TuneKey &key, TuneChoice *out) {
 void tune_store(const TuneKey &key, const TuneChoice &ch, bool changed, double ms) {
   TuneState &s = tune_state();
   std::lock_guard<std::mutex> lk(s.mu);
-  if (s.cache.emplace(key, ch).second) {
+  TuneChoice c = ch;
+  c.changed = changed ? 1 : 0;
+  if (s.cache.emplace(key, c).second) {
     ++s.classes;
     if (changed) ++s.changed;
     s.ms += ms;
@@ -1662,6 +1666,109 @@ void tc_autotune_stats(long long *classes, long long *changed, double *ms) {
   if (classes) *classes = s.classes;
   if (changed) *changed = s.changed;
   if (ms) *ms = s.ms;
+}
+
+// Text form of the current device's cached choices: a header line, then one
+// line per class, "kind nseg flags tm tn kt cg bn nosplit changed", sorted.
+static const char kTuneHeader[] = "# aces-b200 tile choices v1";
+
+int tc_autotune_save(const char *path) {
+  if (!path) {
+    set_error("aces_autotune_save: null path");
+    return ACES_ERR_ARG;
+  }
+  const int dev = current_device();
+  std::vector<std::array<int, 10>> rows;
+  {
+    TuneState &s = tune_state();
+    std::lock_guard<std::mutex> lk(s.mu);
+    for (const auto &kv : s.cache)
+      if (kv.first.dev == dev)
+        rows.push_back({kv.first.kind, kv.first.nseg, kv.first.flags, kv.first.tm, kv.first.tn,
+                        kv.first.kt, kv.second.cg, kv.second.bn, kv.second.nosplit,
+                        kv.second.changed});
+  }
+  std::sort(rows.begin(), rows.end());
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    set_error("aces_autotune_save: cannot open %s for writing", path);
+    return ACES_ERR_ARG;
+  }
+  fprintf(f, "%s\n", kTuneHeader);
+  for (const auto &r : rows)
+    fprintf(f, "%d %d %d %d %d %d %d %d %d %d\n", r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7],
+            r[8], r[9]);
+  if (fclose(f) != 0) {
+    set_error("aces_autotune_save: write to %s failed", path);
+    return ACES_ERR_ARG;
+  }
+  return ACES_OK;
+}
+
+int tc_autotune_load(const char *path) {
+  if (!path) {
+    set_error("aces_autotune_load: null path");
+    return ACES_ERR_ARG;
+  }
+  FILE *f = fopen(path, "r");
+  if (!f) {
+    set_error("aces_autotune_load: cannot open %s", path);
+    return ACES_ERR_ARG;
+  }
+  char line[256];
+  int lineno = 0;
+  std::vector<std::pair<TuneKey, TuneChoice>> rows;
+  const int dev = current_device();
+  int rc = ACES_OK;
+  while (fgets(line, sizeof line, f)) {
+    ++lineno;
+    if (lineno == 1) {
+      if (strncmp(line, kTuneHeader, sizeof kTuneHeader - 1) != 0) {
+        set_error("aces_autotune_load: %s is not a tile-choice file", path);
+        rc = ACES_ERR_ARG;
+        break;
+      }
+      continue;
+    }
+    int v[10];
+    char extra;
+    const int n = sscanf(line, "%d %d %d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3],
+                         &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &extra);
+    const int kind = v[0], nseg = v[1], flags = v[2], cg = v[6], bn = v[7], nosplit = v[8],
+              changed = v[9];
+    // each choice must be one the tuner could have made for its class
+    const bool ok =
+        n == 10 && kind >= 0 && kind <= 2 && nseg >= 1 &&
+        nseg <= (kind == 1 ? kMaxProb : kMaxSeg) && flags >= 0 && flags <= 15 && v[3] >= 0 &&
+        v[4] >= 0 && v[5] >= 0 && (cg == 1 || (cg == 2 && (flags & 1))) &&
+        (bn == 0 || (kind == 2 && (flags & 2) && cg == 1 && (bn == TBN_1 || bn == TBN_WIDE))) &&
+        (nosplit == 0 || (nosplit == 1 && kind == 0 && cg == 1)) && (changed == 0 || changed == 1);
+    if (!ok) {
+      set_error("aces_autotune_load: %s line %d is not a valid tile choice", path, lineno);
+      rc = ACES_ERR_ARG;
+      break;
+    }
+    TuneChoice c;
+    c.cg = cg;
+    c.bn = bn;
+    c.nosplit = nosplit;
+    c.changed = changed;
+    rows.push_back({TuneKey{dev, kind, nseg, flags, v[3], v[4], v[5]}, c});
+  }
+  fclose(f);
+  if (rc == ACES_OK && lineno == 0) {
+    set_error("aces_autotune_load: %s is empty", path);
+    rc = ACES_ERR_ARG;
+  }
+  if (rc != ACES_OK) return rc;
+  // all lines valid: replace the classes they name, recount
+  TuneState &s = tune_state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  for (const auto &r : rows) s.cache[r.first] = r.second;
+  s.classes = (long long)s.cache.size();
+  s.changed = 0;
+  for (const auto &kv : s.cache) s.changed += kv.second.changed;
+  return ACES_OK;
 }
 
 SplitOperand split_view(const SplitOperand &p, int row0, int rows) {

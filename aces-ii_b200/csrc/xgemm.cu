@@ -133,6 +133,10 @@ extern "C" int aces_autotune_stats(long long *classes, long long *changed, doubl
   return ACES_OK;
 }
 
+extern "C" int aces_autotune_save(const char *path) { return tc_autotune_save(path); }
+
+extern "C" int aces_autotune_load(const char *path) { return tc_autotune_load(path); }
+
 extern "C" int aces_debug_inject(int mode) {
   if (mode != 0 && mode != 1) {
     set_error("aces_debug_inject: mode %d (0 or 1)", mode);

@@ -204,6 +204,15 @@ int aces_set_autotune(int mode);
 /* Shape classes tuned so far, how many of them chose a variant other than
  * the built-in rule, and the device ms the timed trial runs took. */
 int aces_autotune_stats(long long *classes, long long *changed, double *tune_ms);
+/* The current device's cached tile choices to a text file, and back (no
+ * counterpart in the reference).  Loading replaces the classes the file
+ * names (for the current device; later products of those classes launch
+ * the loaded choice without timing, whether or not tuning is on) and
+ * rejects a file with any line that is not a choice the tuner could make
+ * (ACES_ERR_ARG, nothing loaded).  A host that loads one saved tuning in
+ * every run gets the same tile variant per class in every run. */
+int aces_autotune_save(const char *path);
+int aces_autotune_load(const char *path);
 
 /* ---- member programs ---------------------------------------------------- */
 

@@ -166,3 +166,38 @@ def test_autotune_switch_and_stats_without_a_gpu(lib):
     assert lib.autotune_stats() == (0, 0, 0.0)
     lib.set_autotune(0)
     assert lib.autotune_stats() == (0, 0, 0.0)
+
+
+def test_autotune_choices_save_and_load_without_a_gpu(lib, tmp_path):
+    """Tile choices round-trip through their text file; a file with a choice
+    the tuner could not make for its class (CTA pairs without the >= 256-row
+    flag, a tile width on an unbatched product) is refused and loads
+    nothing."""
+    header = "# aces-b200 tile choices v1\n"
+    rows = ("0 1 0 2 2 24 1 0 1 1\n"       # single product: no split K
+            "0 1 1 8 2 10 2 0 0 1\n"       # single product >= 256 rows: CTA pairs
+            "1 2 1 30 0 12 1 0 0 0\n"      # grouped launch of two products
+            "2 4 7 40 2 20 1 256 0 0\n")   # batched FP32 output: 256-wide tiles
+    lib.set_autotune(2)
+    good = tmp_path / "choices.txt"
+    good.write_text(header + rows)
+    lib.autotune_load(good)
+    assert lib.autotune_stats() == (4, 2, 0.0)
+    out = tmp_path / "saved.txt"
+    lib.autotune_save(out)
+    assert out.read_text() == header + rows
+    for bad_row in ("0 1 0 2 2 24 2 0 0 1\n", "0 1 1 8 2 10 1 256 0 0\n", "3 1 0 1 1 1 1 0 0 0\n",
+                    "0 1 0 2 2 24 1 0 1\n"):
+        bad = tmp_path / "bad.txt"
+        bad.write_text(header + bad_row)
+        with pytest.raises(ab.AcesError):
+            lib.autotune_load(bad)
+        assert lib.autotune_stats()[0] == 4
+    notfile = tmp_path / "other.txt"
+    notfile.write_text("0 1 0 2 2 24 1 0 1 1\n")
+    with pytest.raises(ab.AcesError):
+        lib.autotune_load(notfile)
+    with pytest.raises(ab.AcesError):
+        lib.autotune_load(tmp_path / "missing.txt")
+    lib.set_autotune(2)
+    assert lib.autotune_stats() == (0, 0, 0.0)

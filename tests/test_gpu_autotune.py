@@ -117,3 +117,21 @@ def test_autotuned_triples_match_default_tiles(lib):
     assert abs(tuned.e_ccsd - plain.e_ccsd) < 1e-8
     assert abs(tuned.e_t4 - plain.e_t4) < 1e-13 + 1e-8 * abs(plain.e_t4)
     assert abs(tuned.e_st5 - plain.e_st5) < 1e-14 + 1e-8 * abs(plain.e_st5)
+
+
+def test_saved_choices_reload_without_timing(lib, tmp_path):
+    """Choices saved after tuning and loaded into an emptied cache serve the
+    same class with no trial runs (no device time added to the stats)."""
+    m, n, k, ta, tb, beta = SHAPES[0]
+    rel, ok = _xgemm(lib, m, n, k, ta, tb, beta, 41)
+    assert ok
+    classes, changed, ms = lib.autotune_stats()
+    assert classes >= 1 and ms > 0.0
+    path = tmp_path / "choices.txt"
+    lib.autotune_save(path)
+    lib.set_autotune(2)
+    lib.autotune_load(path)
+    assert lib.autotune_stats() == (classes, changed, 0.0)
+    rel, ok = _xgemm(lib, m, n, k, ta, tb, beta, 42)
+    assert ok and rel < 2e-5
+    assert lib.autotune_stats() == (classes, changed, 0.0)
